@@ -1,0 +1,332 @@
+"""Benchmark: FP64-accurate TFLOP/s of the block-sparse CCSD particle-particle ladder
+r2(a,b,i,j) += v(a,b,c,d) * t2(c,d,i,j) at O=40, V=360 (spin-blocked, virtual tiles
+U{24..48}), split-INT8 vs plain FP64, one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode int8|fp64|bf16x3]
+                    [--impl ours|reference] [--oa 20 --va 180]
+
+One "step" is one execution of the contraction over every admitted tile triple
+through the Scheduler API.  `value` is the device-timed throughput with inputs
+resident in HBM (v is 50 GB, far beyond L2, so no flush is needed between steps);
+`e2e` repeats the step through the same public API with the step's input t2 copied
+from pinned host memory and the result r2 read back inside the timed region.
+Under torchrun (N > 1) each rank runs an independent copy of the workload on its
+own GPU (replicas: the path needs no exchange), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64-accurate TFLOP/s, block-sparse CC contractions: split-INT8 vs plain FP64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", default=None, choices=["int8", "fp64", "bf16x3"])
+    p.add_argument("--oa", type=int, default=20)
+    p.add_argument("--va", type=int, default=180)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--cpu-seconds", type=float, default=20.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 6:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[2 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak(torch, kind):
+    """Live cuBLAS throughput on this GPU, the denominator for kernels without a
+    driver-measured peak: FP64 DGEMM (torch.matmul float64) or INT8 (torch._int_mm)."""
+    n = 8192
+    if kind == "fp64":
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        f = lambda: torch.matmul(a, a)  # noqa: E731
+    else:
+        a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
+        f = lambda: torch._int_mm(a, a)  # noqa: E731
+    for _ in range(2):
+        f()
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline_sample(wl_triples, seconds, threads):
+    """The reference's own kernels::block_multiply (oracle/_ref, OpenBLAS GEMM) timed on
+    host buffers with the shapes of a fixed-seed sample of the workload's tile triples."""
+    from oracle import oracle as O
+    ref = O.ref()
+    kind = "reference"
+    if ref is None:
+        kind = "port"
+    else:
+        ref.ref_set_blas_threads(threads)
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(wl_triples))
+    lab = {c: -ord(c) for c in "abcdij"}
+    done_flops, t_used, n = 0.0, 0.0, 0
+    bufs = {}
+    for idx in order:
+        (ad, bd, cd) = wl_triples[idx]
+        key = (ad, bd)
+        if key not in bufs:
+            A = np.zeros(ad)
+            B = np.zeros(bd)
+            O.fill_uniform(A.reshape(-1), 1)
+            O.fill_uniform(B.reshape(-1), 2)
+            bufs = {key: (A, B, np.zeros(cd))}
+        A, B, Cb = bufs[key]
+        t0 = time.perf_counter()
+        rc = O.block_multiply(1.0, A, [lab[c] for c in "abcd"], B, [lab[c] for c in "cdij"], 1.0, Cb,
+                              [lab[c] for c in "abij"], 0, impl="ref" if kind == "reference" else "port")
+        t_used += time.perf_counter() - t0
+        assert rc == 0
+        done_flops += 2.0 * np.prod(cd) * ad[2] * ad[3]
+        n += 1
+        if t_used >= seconds:
+            break
+    return {"value": done_flops / t_used / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": kind,
+            "sample": f"{n} tile triples of the O=40/V=360 ladder (fixed-seed random order), "
+                      f"{done_flops:.3e} FLOP in {t_used:.1f} s through kernels::block_multiply "
+                      f"(CPU branch, OpenBLAS GEMM, {threads} threads)"}
+
+
+def ladder_triples(oa, va, seed):
+    """Block shapes (A dims, B dims, C dims) of every admitted ladder triple (host only)."""
+    import tamm_b200 as tb
+    from tamm_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    occ_t = W.random_tiles(oa, 24, 48, rng)
+    virt_t = W.random_tiles(va, 24, 48, rng)
+    vs = [1] * len(virt_t) + [2] * len(virt_t)
+    vt = virt_t + virt_t
+    os_ = [1] * len(occ_t) + [2] * len(occ_t)
+    ot = occ_t + occ_t
+    out = []
+    for a in range(len(vt)):
+        for b in range(len(vt)):
+            for i in range(len(ot)):
+                for j in range(len(ot)):
+                    if vs[a] + vs[b] != os_[i] + os_[j]:
+                        continue
+                    for c in range(len(vt)):
+                        for d in range(len(vt)):
+                            if vs[c] + vs[d] != vs[a] + vs[b]:
+                                continue
+                            out.append(((vt[a], vt[b], vt[c], vt[d]), (vt[c], vt[d], ot[i], ot[j]),
+                                        (vt[a], vt[b], ot[i], ot[j])))
+    del tb
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    triples = ladder_triples(args.oa, args.va, args.seed)
+    total_flops = sum(2.0 * np.prod(c) * a[2] * a[3] for a, _, c in triples)
+    per_step = max(2.0, args.cpu_seconds / max(args.steps, 1))
+    cb = None
+    vals = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_baseline_sample(triples, per_step if s >= args.warmup else 1.0, threads)
+        if s >= args.warmup:
+            vals.append(r["value"])
+            cb = r
+    value = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_flops / (value * 1e12) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}",
+                                            "admitted_flops": total_flops, "parallelism": "host threads"},
+            "cpu_baseline": {**cb, "value": value},
+            "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    import tamm_b200 as tb
+    from tamm_b200 import workloads as W
+
+    mode_name = args.mode or "fp64"
+    mode = {"fp64": tb.Precision.FP64, "int8": tb.Precision.INT8, "bf16x3": tb.Precision.BF16X3}[mode_name]
+    ec = tb.ExecutionContext(local, int(150 * 2 ** 30))
+    lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec)
+    a, b, c, d, i, j = lad.labels
+    stream = torch.cuda.ExternalStream(ec.stream)
+    ec.set_precision(mode)
+
+    def step():
+        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(tb.ExecutionHW.GPU)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * lad.flops / (ms * 1e-3) / 1e12
+
+    # e2e: t2 from pinned host memory in, r2 read back, same public API
+    t2_pin = torch.from_numpy(lad.t2_host).pin_memory()
+    r2_pin = torch.empty(lad.r2.nelems, dtype=torch.float64).pin_memory()
+    import ctypes as C
+    from tamm_b200 import _capi as A
+
+    def e2e_step():
+        A.call("tb_tensor_write", lad.t2.h, C.cast(t2_pin.data_ptr(), A.dp), lad.t2.nelems)
+        step()
+        A.call("tb_tensor_read", lad.r2.h, C.cast(r2_pin.data_ptr(), A.dp), lad.r2.nelems)
+
+    e2e_step()
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    f1.record(stream)
+    barrier()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * lad.flops / (e2e_ms * 1e-3) / 1e12
+
+    # roofline of the dominant kernel: the grouped contraction is the whole step
+    lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(tb.ExecutionHW.GPU, profile=True)
+    kms, kfl = lad.sch.profile()
+    peak_kind = "fp64" if mode_name == "fp64" else ("int8" if mode_name == "int8" else "fp64")
+    peak = measured_peak(torch, peak_kind)
+    achieved = lad.flops / (float(kms[-1]) * 1e-3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None,
+            "peak_source": f"measured live: cuBLAS {'DGEMM' if peak_kind == 'fp64' else 'INT8 GEMM'} 8192^3 "
+                           "on this GPU (no FP64/INT8 figure in MEASURED_PEAKS.json)"}
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu = cpu_baseline_sample(ladder_triples(args.oa, args.va, args.seed), args.cpu_seconds,
+                                      os.cpu_count() or 1)
+        bytes_step = 8 * lad.t2.nelems
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if mode_name == "fp64" else mode_name,
+            "data": "synthetic",
+            "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}", "mode": mode_name,
+                       "admitted_flops": lad.flops, "l2": "inputs larger than L2 (v = "
+                       f"{8*lad.v.nelems/1e9:.1f} GB)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_step,
+                    "d2h_bytes_per_step": 8 * lad.r2.nelems, "ms_per_step": e2e_ms},
+            "gpu_launches": int(args.steps * 1),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+/*
+ * tamm_b200 — C ABI of the B200-native block-sparse tensor-contraction path.
+ *
+ * Drop-in boundary for TAMM's block-contraction hot path.  Two tiers:
+ *
+ *  1. Kernel tier: replaces the block kernels TAMM's operations call
+ *     (tamm::kernels::block_multiply, tamm::kernels::assign, the GEMM wrappers) and
+ *     adds the grouped, device-built work-list form of MultOp::execute_bufacc.
+ *     Device pointers in, device pointers out, explicit CUDA stream.
+ *
+ *  2. Runtime tier: index spaces, tiled index spaces, block-sparse tensors in a
+ *     device-resident block store, and a Scheduler that queues Set/Add/Mult ops and
+ *     executes them on the GPU.  This is what TAMM's LabeledTensor/Scheduler API
+ *     lowers to; the C++ header tamm_b200/include/tamm_b200/tamm.hpp and the Python
+ *     package tamm_b200 are thin front-ends over it.
+ *
+ * Conventions: every function returns an int status (TB_OK == 0).  No C++
+ * exception crosses the boundary; tb_last_error() returns the message of the last
+ * failure on the calling thread.  Labels are plain ints: equal ints name the same
+ * index label (TAMM's per-op int labels, multop.hpp:955-970).  Block dims are tile
+ * extents, row-major, last mode fastest (TAMM's block layout).  All floating-point
+ * data is double (FP64), the element type of every configuration in scope.
+ * Citations are relative to the TAMM source tree.
+ */
+#ifndef TAMM_B200_H
+#define TAMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define TB_OK 0
+#define TB_ERR_INVALID 1         /* malformed arguments: TAMM's EXPECTS (errors.hpp:49-57) */
+#define TB_ERR_NOT_IMPLEMENTED 2 /* TAMM's NOT_IMPLEMENTED() */
+#define TB_ERR_NO_MEMORY 3       /* device arena / host allocation failed */
+#define TB_ERR_CUDA 4            /* a CUDA runtime call failed (TAMM's CUDA_CHECK) */
+#define TB_ERR_TIMEOUT 5         /* a bounded device-side wait gave up */
+#define TB_ERR_DEVICE 6          /* a kernel raised its device error flag */
+#define TB_ERR_STATE 7           /* object used in the wrong state (e.g. not allocated) */
+
+/* Human-readable name of a status code. */
+const char* tb_status_string(int status);
+/* Copies the last failure message of the calling thread into buf (NUL-terminated). */
+int tb_last_error(char* buf, size_t len);
+/* Library version (major, minor). */
+int tb_version(int* major, int* minor);
+
+/* --------------------------------------------------------------- precision modes */
+#define TB_MODE_FP64 0   /* plain FP64 (DMMA tensor-core) contraction */
+#define TB_MODE_INT8 1   /* Ozaki-style split-INT8: INT8 slices, INT32 tcgen05 MMA, FP64 recombination */
+#define TB_MODE_BF16X3 2 /* three-term BF16 split, FP32 accumulate (FP32-class accuracy) */
+
+/* ================================================================ KERNEL TIER === */
+
+/* C (=|+=) alpha * A * B for ONE block triple, device buffers.
+ * Replaces tamm::kernels::block_multiply<T,T1,T2,T3>(th_a, th_b, thandle, alpha,
+ * abuf, adims, alabels, bbuf, bdims, blabels, beta, cbuf, cdims, clabels, hw,
+ * is_assign, cinter_buf_dev, cinter_tmp_buf_dev) (src/tamm/kernels/multiply.hpp:212-220)
+ * for T = double.  Labels are classified as batch / A-outer / B-outer / inner /
+ * A-only / B-only exactly as multiply.hpp:237-302; beta chains the A-only x B-only
+ * reduction steps as gemm_wrapper does (multiply.hpp:42-74); the result is assigned
+ * (is_assign) or accumulated into C in C's own label order (transpose_output,
+ * multiply.hpp:196-210).  No intermediate transposed copy is made.  mode: TB_MODE_*.
+ * Scratch memory is taken from cudaMallocAsync on `stream` when mode needs it. */
+int tb_block_multiply(double alpha, const double* a, const int64_t* adims, const int* alabels,
+                      int na, const double* b, const int64_t* bdims, const int* blabels, int nb,
+                      double beta, double* c, const int64_t* cdims, const int* clabels, int nc,
+                      int is_assign, int mode, void* stream);
+
+/* dst (=|+=) scale * src with labels mapping modes, device buffers.
+ * Replaces tamm::kernels::assign<T>(dst, ddims, dlabels, scale, src, sdims, slabels,
+ * is_assign) (src/tamm/kernels/assign.hpp:467-485): label permutations (the HPTT
+ * branch, assign.hpp:375-401) and the general strided loop (ip_gen_loop,
+ * assign.hpp:312-373, up to 4 dst modes) share one device kernel.  Also serves
+ * internal::block_add (assign.hpp:418-460) and BlockAssignPlan::apply
+ * (block_assign_plan.hpp:111-157). */
+int tb_block_assign(double* dst, const int64_t* ddims, const int* dlabels, int nd, double scale,
+                    const double* src, const int64_t* sdims, const int* slabels, int ns,
+                    int is_assign, void* stream);
+
+/* x[0:n] = value (is_assign) or x[0:n] += value.  Device-side SetOp body
+ * (src/tamm/setop.hpp:130-274). */
+int tb_fill(double* x, int64_t n, double value, int is_assign, void* stream);
+
+/* y[0:n] = alpha * x[0:n] + beta * y[0:n] on the device (the axpy of multop.hpp:830
+ * and the flat AddOp plan, addop.hpp:426-454). */
+int tb_axpby(double alpha, const double* x, double beta, double* y, int64_t n, void* stream);
+
+/* sqrt(sum x^2) over x[0:n], written to *host_out after the stream drains
+ * (tamm::norm, src/tamm/tamm_utils.hpp:1180-1200).  Deterministic two-pass reduction. */
+int tb_norm2(const double* x, int64_t n, double* host_out, void* stream);
+
+/* sum x*y over [0:n] into *host_out (deterministic). */
+int tb_dot(const double* x, const double* y, int64_t n, double* host_out, void* stream);
+
+/* Seeded counter-based fill (same stream as the test oracle's generator up to the
+ * last ulp of log/cos): dist 0 = uniform [p0, p1), 1 = normal(mean p0, sd p1). */
+int tb_fill_random(double* x, int64_t n, uint64_t seed, uint64_t first, int dist, double p0,
+                   double p1, void* stream);
+
+/* ---- grouped contraction: the whole MultOp::execute_bufacc loop in one launch ---- */
+
+/* A contraction plan: label classes of C(clabels) += A(alabels) * B(blabels) as in
+ * multiply.hpp:237-330, plus the precision mode.  err_target is the max relative
+ * error allowed for TB_MODE_INT8 (slice count chosen per block from it; <= 0 picks
+ * the default 1e-11); nslices > 0 forces the slice count (6..8). */
+typedef struct tb_plan_s* tb_plan;
+int tb_plan_contraction(const int* clabels, int nc, const int* alabels, int na, const int* blabels,
+                        int nb, int mode, double err_target, int nslices, tb_plan* out);
+int tb_plan_destroy(tb_plan plan);
+
+/* A device work list for a plan: output-block groups, each with the (A block,
+ * B block) tasks of its admitted reduction tiles (multop.hpp:645-851).  Offsets are
+ * element offsets into the A/B/C arenas; dims are the blocks' tile extents in each
+ * tensor's own mode order.  group_task_begin has ngroups+1 entries. */
+typedef struct tb_worklist_s* tb_worklist;
+int tb_worklist_build(tb_plan plan, int64_t ngroups, const int64_t* group_c_off,
+                      const int32_t* group_cdims, const int64_t* group_task_begin,
+                      const int64_t* task_a_off, const int64_t* task_b_off,
+                      const int32_t* task_adims, const int32_t* task_bdims, tb_worklist* out);
+int tb_worklist_destroy(tb_worklist wl);
+/* Number of tasks and admitted FP64 FLOPs (2 * |C block| * K per task). */
+int tb_worklist_info(tb_worklist wl, int64_t* ntasks, double* flops);
+
+/* Per-launch statistics of the last tb_contract on a plan. */
+typedef struct tb_stats {
+  double flops;           /* admitted FP64 FLOPs */
+  double int8_ops;        /* INT8 tensor-core ops issued (TB_MODE_INT8) */
+  int    slices_min;      /* slice counts chosen (TB_MODE_INT8) */
+  int    slices_max;
+  int64_t scratch_bytes;  /* scratch used by the split operands */
+} tb_stats;
+
+/* C += alpha * sum over tasks of A * B, all groups, one stream-ordered pass.
+ * Scratch (INT8 slices) comes from cudaMallocAsync on the stream. */
+int tb_contract(tb_plan plan, tb_worklist wl, double alpha, const double* a, const double* b,
+                double* c, void* stream);
+int tb_plan_stats(tb_plan plan, tb_stats* out);
+
+/* =============================================================== RUNTIME TIER === */
+
+/* ExecutionContext (src/tamm/execution_context.hpp:120): one GPU, one stream, a
+ * stream-ordered device arena of pool_bytes (0 = 80% of free memory, TAMM's
+ * TAMM_GPU_POOL default, rmm_memory_pool.hpp:30-46), and the precision options. */
+typedef struct tb_ctx_s* tb_ctx;
+int tb_ctx_create(int device, int64_t pool_bytes, tb_ctx* out);
+int tb_ctx_destroy(tb_ctx ctx);
+int tb_ctx_set_precision(tb_ctx ctx, int mode, double err_target, int nslices);
+int tb_ctx_stream(tb_ctx ctx, void** stream);
+int tb_ctx_synchronize(tb_ctx ctx);
+/* Arena occupancy: bytes in use, high-water mark, capacity. */
+int tb_ctx_arena_info(tb_ctx ctx, int64_t* used, int64_t* peak, int64_t* capacity);
+
+/* IndexSpace{range(n), {{name, {ranges}}...}, {{Spin{s}, {ranges}}...}}
+ * (src/tamm/index_space.hpp:64).  name_ranges / spin_ranges hold [lo, hi) pairs,
+ * name_nranges[i] / spin_nranges[i] of them per name / spin value. */
+typedef struct tb_is_s* tb_is;
+int tb_is_create(int64_t n, int nnamed, const char* const* names, const int* name_nranges,
+                 const int64_t* name_ranges, int nspin, const int* spin_values,
+                 const int* spin_nranges, const int64_t* spin_ranges, tb_is* out);
+int tb_is_destroy(tb_is is);
+
+/* TiledIndexSpace{is, tile} (tiles == NULL) or TiledIndexSpace{is, tile_list}
+ * (src/tamm/tiled_index_space.hpp:31,49; tiling rules :1135-1262). */
+typedef struct tb_tis_s* tb_tis;
+int tb_tis_create(tb_is is, int64_t tile, const int64_t* tiles, int64_t ntiles, tb_tis* out);
+/* tis("name"): the tiles of a named subspace (e.g. MO("occ")). */
+int tb_tis_named(tb_tis tis, const char* name, tb_tis* out);
+/* TiledIndexSpace{tis, range(first, last)}: tiles [first, last) of tis
+ * (tiled_index_space.hpp:84-110). */
+int tb_tis_subrange(tb_tis tis, int64_t first_tile, int64_t last_tile, tb_tis* out);
+int tb_tis_num_tiles(tb_tis tis, int64_t* ntiles);
+/* Per tile: size, spin (of its first index, tiled_index_space.hpp:342-345,1327)
+ * and index in the root tiled space.  Arrays hold num_tiles entries. */
+int tb_tis_tiles(tb_tis tis, int64_t* sizes, int* spins, int64_t* root_tiles);
+int tb_tis_destroy(tb_tis tis);
+
+/* Tensor<T>{tis...} or Tensor<T>{{tis...}, SpinMask} (src/tamm/tensor.hpp:87-136,
+ * spin rule tensor_base.hpp:243-263).  spin_mask NULL: no spin symmetry; else per
+ * mode 0 upper, 1 lower, 2 ignore.  Blocks are stored in Distribution_NW order
+ * (distribution.hpp:197-285): admitted blocks sorted by row-major tile key,
+ * packed contiguously in one device arena allocation. */
+typedef struct tb_tensor_s* tb_tensor;
+int tb_tensor_create(int nmodes, const tb_tis* tis, const int* spin_mask, tb_tensor* out);
+/* Tensor{{tis...}, {nupper, nlower}} form (tensor_impl.hpp:153-209). */
+int tb_tensor_create_spin_sizes(int nmodes, const tb_tis* tis, int nupper, int nlower,
+                                tb_tensor* out);
+int tb_tensor_allocate(tb_tensor t, tb_ctx ctx);
+int tb_tensor_deallocate(tb_tensor t);
+int tb_tensor_destroy(tb_tensor t);
+int tb_tensor_info(tb_tensor t, int* nmodes, int64_t* nblocks, int64_t* nelems);
+/* Packed block table in storage order: keys and element offsets (nblocks each). */
+int tb_tensor_block_table(tb_tensor t, int64_t* keys, int64_t* offsets);
+int tb_tensor_data(tb_tensor t, double** device_ptr);
+int tb_tensor_is_non_zero(tb_tensor t, const int64_t* blockid, int* out);
+int tb_tensor_block_size(tb_tensor t, const int64_t* blockid, int64_t* out);
+int tb_tensor_block_dims(tb_tensor t, const int64_t* blockid, int64_t* dims);
+/* Element offset of a stored block, -1 if the block is not admitted. */
+int tb_tensor_locate(tb_tensor t, const int64_t* blockid, int64_t* offset);
+/* Tensor::get / put / add of one block with a HOST buffer of n >= block size
+ * (tensor_impl.hpp:321-455; get of a non-admitted block returns zeros). */
+int tb_tensor_get(tb_tensor t, const int64_t* blockid, double* host, int64_t n);
+int tb_tensor_put(tb_tensor t, const int64_t* blockid, const double* host, int64_t n);
+int tb_tensor_add(tb_tensor t, const int64_t* blockid, const double* host, int64_t n);
+/* Whole packed store <-> host (n == nelems). */
+int tb_tensor_write(tb_tensor t, const double* host, int64_t n);
+int tb_tensor_read(tb_tensor t, double* host, int64_t n);
+int tb_tensor_norm(tb_tensor t, double* out);
+
+/* A labelled operand: tensor, per-mode int label, per-mode label space (NULL array
+ * or NULL entry: the tensor's own tiled space; else a sub-space of it, as for
+ * TiledIndexLabels of MO("occ") on a tensor over MO). */
+typedef struct tb_labeled {
+  tb_tensor     tensor;
+  const int*    labels;
+  const tb_tis* label_tis;
+} tb_labeled;
+
+/* Scheduler (src/tamm/scheduler.hpp:40-51,160-438): ops are queued with
+ * operator() and run by execute() in dependence levels on the context's stream. */
+typedef struct tb_sched_s* tb_sched;
+int tb_sched_create(tb_ctx ctx, tb_sched* out);
+int tb_sched_destroy(tb_sched s);
+/* SetOp: lhs = value (is_assign) or lhs += value. */
+int tb_sched_set(tb_sched s, tb_labeled lhs, double value, int is_assign);
+/* AddOp: lhs (=|+=) alpha * rhs (addop.hpp:242-271). */
+int tb_sched_add(tb_sched s, tb_labeled lhs, double alpha, tb_labeled rhs, int is_assign);
+/* MultOp: lhs (=|+=) alpha * a * b; "=" is canonicalised to SetOp(0) then "+="
+ * (multop.hpp:255-269). */
+int tb_sched_mult(tb_sched s, tb_labeled lhs, double alpha, tb_labeled a, tb_labeled b,
+                  int is_assign);
+/* Work of lhs += a * b without running it: admitted output blocks, admitted
+ * (C, A, B) block triples and their FP64 FLOPs, from the same enumeration the
+ * MultOp uses (multop.hpp:645-893).  Needs no GPU and no allocation. */
+int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, int64_t* ntasks,
+                 double* flops);
+/* Scheduler::execute(ExecutionHW, profile).  hw: 0 DEFAULT, 1 CPU, 2 GPU — every op
+ * runs on the GPU (there is no host execution path); profile records per-op device
+ * times readable with tb_sched_profile. */
+int tb_sched_execute(tb_sched s, int hw, int profile);
+/* Number of ops in the last execute; per op: device milliseconds and FP64 FLOPs. */
+int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64_t cap);
+/* Drops queued ops without running them. */
+int tb_sched_clear(tb_sched s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

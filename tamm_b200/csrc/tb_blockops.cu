@@ -1,0 +1,343 @@
+// HBM-bound block kernels: permuted assign/accumulate (kernels::assign), fill (SetOp),
+// axpby (flat AddOp / the bufacc axpy), deterministic dot / norm reductions, and the
+// seeded counter-based generator.
+#include "tb_internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+namespace tb {
+namespace {
+
+constexpr int kThreads = 256;
+
+int grid_for(int64_t n, int per_thread) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t want = (n + (int64_t) kThreads * per_thread - 1) / ((int64_t) kThreads * per_thread);
+  int64_t cap  = (int64_t) sms * 8; // 8 resident CTAs of 256 threads per SM
+  return (int) std::max<int64_t>(1, std::min<int64_t>(want, cap));
+}
+
+// ---- permuted assign: dst[sum i_k dld_k] (=|+=) scale * src[sum i_k sld_k] ----
+// The destination is walked in its own row-major order so stores coalesce; the
+// source side is gathered.  Index space up to 4-D as the reference's ip0..ip4.
+struct AssignArgs {
+  int     nd;
+  int64_t dims[4], dld[4], sld[4];
+  int64_t total;
+};
+
+__global__ void __launch_bounds__(kThreads) k_assign(AssignArgs a, double* __restrict__ dst,
+                                                     double scale, const double* __restrict__ src,
+                                                     int is_assign) {
+  const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+  for(int64_t lin = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; lin < a.total; lin += stride) {
+    int64_t x = lin, so = 0, doff = 0;
+#pragma unroll
+    for(int k = 3; k >= 0; k--) {
+      if(k >= a.nd) continue;
+      const int64_t d = a.dims[k];
+      const int64_t q = x / d;
+      const int64_t i = x - q * d;
+      so += i * a.sld[k];
+      doff += i * a.dld[k];
+      x = q;
+    }
+    const double v = scale * __ldg(src + so);
+    dst[doff]      = is_assign ? v : dst[doff] + v;
+  }
+}
+
+// ---- pure permutation of >=2 modes whose last dst mode is not the last src mode:
+// 32x32 tiles through shared memory so both the read and the write are coalesced.
+struct TransArgs {
+  int     nd;
+  int64_t dims[4];      // dst-order loop dims
+  int64_t dld[4], sld[4];
+  int     p;            // loop position of the src stride-1 mode
+  int64_t outer_total;  // product of dims except positions nd-1 and p
+};
+
+__global__ void __launch_bounds__(kThreads) k_assign_tiled(TransArgs a, double* __restrict__ dst,
+                                                           double scale,
+                                                           const double* __restrict__ src,
+                                                           int is_assign) {
+  __shared__ double tile[32][33];
+  const int     q      = a.nd - 1;
+  const int64_t Dq     = a.dims[q], Dp = a.dims[a.p];
+  const int64_t tq     = (Dq + 31) / 32, tp = (Dp + 31) / 32;
+  const int64_t ntiles = a.outer_total * tq * tp;
+  for(int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int64_t x  = t;
+    int64_t bq = x % tq;
+    x /= tq;
+    int64_t bp = x % tp;
+    x /= tp;
+    // outer index over modes other than p and q
+    int64_t so = 0, doff = 0;
+    for(int k = a.nd - 1; k >= 0; k--) {
+      if(k == q || k == a.p) continue;
+      const int64_t d = a.dims[k];
+      const int64_t i = x % d;
+      x /= d;
+      so += i * a.sld[k];
+      doff += i * a.dld[k];
+    }
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5; // 32 x 8
+    // read: consecutive threads along p (src stride 1)
+    for(int r = ty; r < 32; r += 8) {
+      const int64_t iq = bq * 32 + r, ip = bp * 32 + tx;
+      if(iq < Dq && ip < Dp) tile[r][tx] = __ldg(src + so + iq * a.sld[q] + ip * a.sld[a.p]);
+    }
+    __syncthreads();
+    // write: consecutive threads along q (dst stride 1)
+    for(int r = ty; r < 32; r += 8) {
+      const int64_t ip = bp * 32 + r, iq = bq * 32 + tx;
+      if(iq < Dq && ip < Dp) {
+        double*      dp = dst + doff + iq * a.dld[q] + ip * a.dld[a.p];
+        const double v  = scale * tile[tx][r];
+        *dp             = is_assign ? v : *dp + v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_fill(double* __restrict__ x, int64_t n, double v,
+                                                   int is_assign) {
+  const int64_t stride = (int64_t) gridDim.x * blockDim.x * 2;
+  for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
+    if(i + 1 < n && ((reinterpret_cast<uintptr_t>(x + i) & 15) == 0)) {
+      double2 d;
+      if(is_assign) d = make_double2(v, v);
+      else {
+        d = *reinterpret_cast<double2*>(x + i);
+        d.x += v;
+        d.y += v;
+      }
+      *reinterpret_cast<double2*>(x + i) = d;
+    }
+    else {
+      for(int64_t j = i; j < i + 2 && j < n; j++) x[j] = is_assign ? v : x[j] + v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_axpby(double alpha, const double* __restrict__ x,
+                                                    double beta, double* __restrict__ y, int64_t n) {
+  const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+  for(int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    y[i] = beta == 0.0 ? alpha * x[i] : alpha * x[i] + beta * y[i];
+}
+
+// Deterministic dot: fixed grid, per-block partials in a fixed order, then one block
+// folds the partials.  y == nullptr means x.x.
+constexpr int kRedBlocks = 1024;
+
+__global__ void __launch_bounds__(kThreads) k_dot_partial(const double* __restrict__ x,
+                                                          const double* __restrict__ y, int64_t n,
+                                                          double* __restrict__ part) {
+  double        s      = 0.0;
+  const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+  for(int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double a = x[i];
+    s += a * (y ? y[i] : a);
+  }
+#pragma unroll
+  for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double ws[kThreads / 32];
+  if((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    double t = 0.0;
+    for(int w = 0; w < kThreads / 32; w++) t += ws[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_dot_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+  __shared__ double ws[32];
+  double            s = 0.0;
+  for(int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+#pragma unroll
+  for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    double t = 0.0;
+    for(int w = 0; w < (int) (blockDim.x / 32); w++) t += ws[w];
+    *out = t;
+  }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ double u01(uint64_t seed_mix, uint64_t i) {
+  const uint64_t h = splitmix64(seed_mix ^ (i * 0xD1B54A32D192ED03ull));
+  return (double) (h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void __launch_bounds__(kThreads) k_fill_random(double* __restrict__ x, int64_t n,
+                                                          uint64_t seed_mix, uint64_t first,
+                                                          int dist, double p0, double p1) {
+  const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+  for(int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const uint64_t i = first + (uint64_t) q;
+    if(dist == 0) x[q] = p0 + (p1 - p0) * u01(seed_mix, i);
+    else {
+      double u1 = u01(seed_mix, 2 * i), u2 = u01(seed_mix, 2 * i + 1);
+      if(u1 < 1e-300) u1 = 1e-300;
+      x[q] = p0 + p1 * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    }
+  }
+}
+
+uint64_t host_splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+} // namespace
+
+AssignLoop plan_assign(const int64_t* ddims, const int* dlabels, int nd, const int64_t* sdims,
+                       const int* slabels, int ns) {
+  // kernels::assign (assign.hpp:467-485): permutation -> HPTT semantics, otherwise
+  // ip_gen_loop (assign.hpp:312-373).  Both reduce to an nd-deep loop with dst and
+  // src strides per loop label.
+  TB_EXPECTS(nd >= 0 && nd <= kMaxModes && ns >= 0 && ns <= kMaxModes, "rank out of range");
+  auto find = [](const int* v, int n, int x) {
+    for(int i = 0; i < n; i++)
+      if(v[i] == x) return i;
+    return -1;
+  };
+  // are_permutations (perm.hpp:36-47)
+  bool perm = (nd == ns);
+  if(perm) {
+    bool taken[kMaxModes] = {false};
+    for(int i = 0; i < ns && perm; i++) {
+      int p = find(dlabels, nd, slabels[i]);
+      if(p < 0 || taken[p]) perm = false;
+      else taken[p] = true;
+    }
+  }
+  int64_t sld[kMaxModes + 1], dld[kMaxModes + 1];
+  sld[ns] = 1;
+  for(int i = ns - 1; i >= 0; i--) sld[i] = sld[i + 1] * sdims[i];
+  dld[nd] = 1;
+  for(int i = nd - 1; i >= 0; i--) dld[i] = dld[i + 1] * ddims[i];
+  AssignLoop lp;
+  lp.nd = nd;
+  if(perm) {
+    for(int i = 0; i < nd; i++) {
+      int p = find(slabels, ns, dlabels[i]);
+      TB_EXPECTS(ddims[i] == sdims[p], "dst dims are not a permutation of src dims");
+    }
+  }
+  TB_EXPECTS(nd <= 4, "assign supports at most 4 destination modes (NOT_IMPLEMENTED beyond)");
+  int loop_labels[2 * kMaxModes], nl = 0;
+  for(int i = 0; i < nd; i++)
+    if(find(loop_labels, nl, dlabels[i]) < 0) loop_labels[nl++] = dlabels[i];
+  for(int i = 0; i < ns; i++)
+    if(find(loop_labels, nl, slabels[i]) < 0) loop_labels[nl++] = slabels[i];
+  TB_EXPECTS(nl >= nd, "repeated destination labels");
+  for(int k = 0; k < nd; k++) {
+    lp.dims[k] = 0;
+    lp.sld[k]  = 0;
+    lp.dld[k]  = 0;
+    int ps     = find(slabels, ns, loop_labels[k]);
+    if(ps >= 0) {
+      lp.sld[k]  = sld[ps + 1];
+      lp.dims[k] = sdims[ps];
+    }
+    int pd = find(dlabels, nd, loop_labels[k]);
+    if(pd >= 0) {
+      lp.dld[k]  = dld[pd + 1];
+      lp.dims[k] = ddims[pd];
+    }
+  }
+  return lp;
+}
+
+void launch_assign(const AssignLoop& lp, double* dst, double scale, const double* src,
+                   int is_assign, cudaStream_t stream) {
+  int64_t total = 1;
+  for(int k = 0; k < lp.nd; k++) total *= lp.dims[k];
+  if(total == 0) return;
+  // A transposing permutation (dst's last loop mode is not src's stride-1 mode) goes
+  // through the shared-memory tile kernel; everything else streams directly.
+  int p = -1;
+  for(int k = 0; k < lp.nd; k++)
+    if(lp.sld[k] == 1 && lp.dims[k] > 1) p = k;
+  const int q = lp.nd - 1;
+  if(lp.nd >= 2 && p >= 0 && p != q && lp.dld[q] == 1 && lp.dims[q] >= 8 && lp.dims[p] >= 8) {
+    TransArgs a;
+    a.nd          = lp.nd;
+    a.p           = p;
+    a.outer_total = 1;
+    for(int k = 0; k < 4; k++) {
+      a.dims[k] = k < lp.nd ? lp.dims[k] : 1;
+      a.dld[k]  = k < lp.nd ? lp.dld[k] : 0;
+      a.sld[k]  = k < lp.nd ? lp.sld[k] : 0;
+      if(k < lp.nd && k != p && k != q) a.outer_total *= lp.dims[k];
+    }
+    const int64_t ntiles = a.outer_total * ((lp.dims[q] + 31) / 32) * ((lp.dims[p] + 31) / 32);
+    const int     grid   = (int) std::min<int64_t>(ntiles, 148 * 8);
+    k_assign_tiled<<<grid, kThreads, 0, stream>>>(a, dst, scale, src, is_assign);
+  }
+  else {
+    AssignArgs a;
+    a.nd    = lp.nd;
+    a.total = total;
+    for(int k = 0; k < 4; k++) {
+      a.dims[k] = k < lp.nd ? lp.dims[k] : 1;
+      a.dld[k]  = k < lp.nd ? lp.dld[k] : 0;
+      a.sld[k]  = k < lp.nd ? lp.sld[k] : 0;
+    }
+    k_assign<<<grid_for(total, 4), kThreads, 0, stream>>>(a, dst, scale, src, is_assign);
+  }
+  TB_CUDA(cudaGetLastError());
+}
+
+void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream) {
+  if(n <= 0) return;
+  k_fill<<<grid_for(n, 8), kThreads, 0, stream>>>(x, n, value, is_assign);
+  TB_CUDA(cudaGetLastError());
+}
+
+void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
+                  cudaStream_t stream) {
+  if(n <= 0) return;
+  k_axpby<<<grid_for(n, 4), kThreads, 0, stream>>>(alpha, x, beta, y, n);
+  TB_CUDA(cudaGetLastError());
+}
+
+double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream) {
+  if(n <= 0) return 0.0;
+  double* part = nullptr;
+  TB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * (kRedBlocks + 1), stream));
+  k_dot_partial<<<kRedBlocks, kThreads, 0, stream>>>(x, y, n, part);
+  k_dot_final<<<1, 1024, 0, stream>>>(part, kRedBlocks, part + kRedBlocks);
+  double h = 0.0;
+  TB_CUDA(cudaMemcpyAsync(&h, part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  TB_CUDA(cudaFreeAsync(part, stream));
+  TB_CUDA(cudaStreamSynchronize(stream));
+  return h;
+}
+
+void launch_fill_random(double* x, int64_t n, uint64_t seed, uint64_t first, int dist, double p0,
+                        double p1, cudaStream_t stream) {
+  if(n <= 0) return;
+  k_fill_random<<<grid_for(n, 4), kThreads, 0, stream>>>(x, n, host_splitmix64(seed), first, dist,
+                                                         p0, p1);
+  TB_CUDA(cudaGetLastError());
+}
+
+} // namespace tb

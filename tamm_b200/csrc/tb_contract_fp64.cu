@@ -1,0 +1,409 @@
+// Grouped FP64 block contraction on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64).
+//
+// One launch runs a whole MultOp::execute_bufacc (src/tamm/multop.hpp:576-893): every
+// CTA owns one 128x64 tile of one output block (a "group") and loops over the
+// group's (A block, B block) tasks — the admitted reduction tiles — and, inside each
+// task, over the A-only x B-only reduction steps and the K chunks, accumulating in
+// registers.  Operands are gathered straight from the block store with the label
+// permutation folded into per-row / per-k offset tables (no Ainter/Binter copies as in
+// kernels::block_multiply's transpose_inputs, multiply.hpp:159-194), staged through a
+// 3-deep cp.async pipeline, and the result is written once into C in C's own label
+// order (transpose_output, multiply.hpp:196-210, fused into the epilogue).
+#include "tb_internal.hpp"
+
+#include <algorithm>
+
+namespace tb {
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, NSLOT = STAGES + 1, NTHREADS = 256;
+constexpr int AS_LD = BK + 4; // padded row strides (doubles) against bank conflicts
+constexpr int BS_LD = BN + 4;
+
+struct TaskInfo {
+  int64_t a_blk, b_blk; // block offset + batch offset, elements
+  int32_t K, AR, BR, ARBR;
+  int32_t kdim[kMaxClass], kstrA[kMaxClass], kstrB[kMaxClass];
+  int32_t ardim[kMaxClass], arstrA[kMaxClass];
+  int32_t brdim[kMaxClass], brstrB[kMaxClass];
+  int32_t mstrA[kMaxClass], nstrB[kMaxClass];
+};
+
+struct ChunkDesc {
+  int64_t a_base, b_base;
+  int32_t valid, buf, kvalid, first_step;
+  int32_t kA[BK], kB[BK];
+};
+
+struct Smem {
+  double    As[STAGES][BM][AS_LD];
+  double    Bs[STAGES][BK][BS_LD];
+  int32_t   rowA[2][BM];
+  int32_t   colB[2][BN];
+  int32_t   rowC[BM];
+  int32_t   colC[BN];
+  TaskInfo  ti[2];
+  ChunkDesc desc[NSLOT];
+};
+
+struct Params {
+  LabelClasses    lc;
+  const double*   A;
+  const double*   B;
+  double*         C;
+  const DevGroup* groups;
+  const DevTask*  tasks;
+  const DevItem*  items;
+  double          alpha, beta;
+  int             is_assign;
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int bytes) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template<int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Row-major strides of a block with `n` modes.
+__device__ __forceinline__ void strides_of(const int32_t* dims, int n, int64_t* str) {
+  int64_t s = 1;
+  for(int i = n - 1; i >= 0; i--) {
+    str[i] = s;
+    s *= dims[i];
+  }
+}
+
+// Offset of linear index x decomposed over dims[0..n) (last fastest) with strides.
+__device__ __forceinline__ int32_t decompose(int32_t x, int n, const int32_t* dims,
+                                             const int32_t* str) {
+  int32_t off = 0;
+  for(int j = n - 1; j >= 0; j--) {
+    int32_t d = dims[j];
+    int32_t q = x / d;
+    off += (x - q * d) * str[j];
+    x = q;
+  }
+  return off;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem&               s   = *reinterpret_cast<Smem*>(smem_raw);
+  const LabelClasses& lc  = p.lc;
+  const int           tid = threadIdx.x;
+  const DevItem       it  = p.items[blockIdx.x];
+  const DevGroup      g   = p.groups[it.group];
+  const int           tb  = g.task_begin, te = g.task_end;
+
+  // ---- output block geometry (uniform) ----
+  int64_t cstr[kMaxModes];
+  strides_of(g.cdims, lc.nc, cstr);
+  int32_t mdim[kMaxClass], ndim[kMaxClass], mstrC[kMaxClass], nstrC[kMaxClass];
+  int32_t Mtot = 1, Ntot = 1;
+  for(int j = 0; j < lc.nm; j++) {
+    mdim[j]  = g.cdims[lc.m_c[j]];
+    mstrC[j] = (int32_t) cstr[lc.m_c[j]];
+    Mtot *= mdim[j];
+  }
+  for(int j = 0; j < lc.nn; j++) {
+    ndim[j]  = g.cdims[lc.n_c[j]];
+    nstrC[j] = (int32_t) cstr[lc.n_c[j]];
+    Ntot *= ndim[j];
+  }
+  int32_t bidx[kMaxClass];
+  {
+    int32_t x = it.batch;
+    for(int j = lc.nbatch - 1; j >= 0; j--) {
+      int32_t d = g.cdims[lc.batch_c[j]];
+      bidx[j]   = x % d;
+      x /= d;
+    }
+  }
+  int64_t c_base = g.c_off;
+  for(int j = 0; j < lc.nbatch; j++) c_base += bidx[j] * cstr[lc.batch_c[j]];
+  for(int m = tid; m < BM; m += NTHREADS)
+    s.rowC[m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, mdim, mstrC) : 0;
+  for(int n = tid; n < BN; n += NTHREADS)
+    s.colC[n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, ndim, nstrC) : 0;
+
+  // ---- chunk iterator over (task, reduction step, k0), uniform across the CTA ----
+  int  cur_t = tb, cur_s = 0, cur_k0 = 0, cur_K = 0, cur_ARBR = 0, cur_BR = 1;
+  bool started = false;
+
+  auto prepare = [&](int q) {
+    bool new_task = false;
+    if(!started) {
+      started  = true;
+      new_task = true;
+    }
+    else if(cur_t < te) {
+      cur_k0 += BK;
+      if(cur_k0 >= cur_K) {
+        cur_k0 = 0;
+        if(++cur_s >= cur_ARBR) {
+          cur_s = 0;
+          ++cur_t;
+          new_task = true;
+        }
+      }
+    }
+    ChunkDesc& d = s.desc[q % NSLOT];
+    if(cur_t >= te) {
+      if(tid == 0) d.valid = 0;
+      return;
+    }
+    const int buf = (cur_t - tb) & 1;
+    TaskInfo& ti  = s.ti[buf];
+    if(new_task) {
+      if(tid == 0) {
+        const DevTask tk = p.tasks[cur_t];
+        int64_t       astr[kMaxModes], bstr[kMaxModes];
+        strides_of(tk.adims, lc.na, astr);
+        strides_of(tk.bdims, lc.nb, bstr);
+        ti.K = 1;
+        for(int j = 0; j < lc.nk; j++) {
+          ti.kdim[j]  = tk.adims[lc.k_a[j]];
+          ti.kstrA[j] = (int32_t) astr[lc.k_a[j]];
+          ti.kstrB[j] = (int32_t) bstr[lc.k_b[j]];
+          ti.K *= ti.kdim[j];
+        }
+        ti.AR = 1;
+        for(int j = 0; j < lc.nar; j++) {
+          ti.ardim[j]  = tk.adims[lc.ar_a[j]];
+          ti.arstrA[j] = (int32_t) astr[lc.ar_a[j]];
+          ti.AR *= ti.ardim[j];
+        }
+        ti.BR = 1;
+        for(int j = 0; j < lc.nbr; j++) {
+          ti.brdim[j]  = tk.bdims[lc.br_b[j]];
+          ti.brstrB[j] = (int32_t) bstr[lc.br_b[j]];
+          ti.BR *= ti.brdim[j];
+        }
+        ti.ARBR = ti.AR * ti.BR;
+        for(int j = 0; j < lc.nm; j++) ti.mstrA[j] = (int32_t) astr[lc.m_a[j]];
+        for(int j = 0; j < lc.nn; j++) ti.nstrB[j] = (int32_t) bstr[lc.n_b[j]];
+        int64_t ab = tk.a_off, bb = tk.b_off;
+        for(int j = 0; j < lc.nbatch; j++) {
+          ab += bidx[j] * astr[lc.batch_a[j]];
+          bb += bidx[j] * bstr[lc.batch_b[j]];
+        }
+        ti.a_blk = ab;
+        ti.b_blk = bb;
+      }
+      __syncthreads();
+      cur_K    = ti.K;
+      cur_ARBR = ti.ARBR;
+      cur_BR   = ti.BR;
+      for(int m = tid; m < BM; m += NTHREADS)
+        s.rowA[buf][m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, mdim, ti.mstrA) : 0;
+      for(int n = tid; n < BN; n += NTHREADS)
+        s.colB[buf][n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, ndim, ti.nstrB) : 0;
+    }
+    if(tid == 0) {
+      const int ar = cur_s / cur_BR, br = cur_s - (cur_s / cur_BR) * cur_BR;
+      d.a_base     = ti.a_blk + decompose(ar, lc.nar, ti.ardim, ti.arstrA);
+      d.b_base     = ti.b_blk + decompose(br, lc.nbr, ti.brdim, ti.brstrB);
+      d.valid      = 1;
+      d.buf        = buf;
+      d.kvalid     = min(BK, cur_K - cur_k0);
+      d.first_step = (cur_s > 0 && cur_k0 == 0) ? 1 : 0;
+    }
+    if(tid < BK) {
+      const int k = cur_k0 + tid;
+      d.kA[tid]   = (k < cur_K) ? decompose(k, lc.nk, ti.kdim, ti.kstrA) : 0;
+    }
+    else if(tid < 2 * BK) {
+      const int k     = cur_k0 + tid - BK;
+      d.kB[tid - BK] = (k < cur_K) ? decompose(k, lc.nk, ti.kdim, ti.kstrB) : 0;
+    }
+  };
+
+  auto issue = [&](int q) {
+    const ChunkDesc& d = s.desc[q % NSLOT];
+    if(!d.valid) return;
+    const int stage = q % STAGES, buf = d.buf;
+    const double* Ab = p.A + d.a_base;
+    const double* Bb = p.B + d.b_base;
+#pragma unroll
+    for(int e = 0; e < (BM * BK) / NTHREADS; e++) {
+      int m, kk;
+      if(lc.a_contig == 1) {
+        kk = tid % BK;
+        m  = tid / BK + e * (NTHREADS / BK);
+      }
+      else {
+        m  = tid % BM;
+        kk = tid / BM + e * (NTHREADS / BM);
+      }
+      const bool ok = (it.m0 + m < Mtot) && (kk < d.kvalid);
+      cp_async8(&s.As[stage][m][kk], ok ? (const void*) (Ab + s.rowA[buf][m] + d.kA[kk]) : (const void*) p.A,
+                ok ? 8 : 0);
+    }
+#pragma unroll
+    for(int e = 0; e < (BK * BN) / NTHREADS; e++) {
+      int n, kk;
+      if(lc.b_contig == 1) {
+        kk = tid % BK;
+        n  = tid / BK + e * (NTHREADS / BK);
+      }
+      else {
+        n  = tid % BN;
+        kk = tid / BN + e * (NTHREADS / BN);
+      }
+      const bool ok = (it.n0 + n < Ntot) && (kk < d.kvalid);
+      cp_async8(&s.Bs[stage][kk][n], ok ? (const void*) (Bb + d.kB[kk] + s.colB[buf][n]) : (const void*) p.B,
+                ok ? 8 : 0);
+    }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  double    acc[4][4][2];
+#pragma unroll
+  for(int i = 0; i < 4; i++)
+#pragma unroll
+    for(int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  // ---- prologue: chunks 0..STAGES-2 in flight, chunk STAGES-1 prepared ----
+  prepare(0);
+  __syncthreads();
+#pragma unroll 1
+  for(int q = 0; q < STAGES - 1; q++) {
+    issue(q);
+    cp_async_commit();
+    prepare(q + 1);
+    __syncthreads();
+  }
+
+#pragma unroll 1
+  for(int q = 0;; q++) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const ChunkDesc& dq = s.desc[q % NSLOT];
+    if(!dq.valid) break;
+    const bool scale_acc = dq.first_step != 0;
+    issue(q + STAGES - 1);
+    cp_async_commit();
+    prepare(q + STAGES);
+    if(scale_acc) { // beta chaining of A-only x B-only reduction steps (gemm_wrapper)
+#pragma unroll
+      for(int i = 0; i < 4; i++)
+#pragma unroll
+        for(int j = 0; j < 4; j++) {
+          acc[i][j][0] *= p.beta;
+          acc[i][j][1] *= p.beta;
+        }
+    }
+    const int stage = q % STAGES;
+#pragma unroll
+    for(int k4 = 0; k4 < BK; k4 += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for(int i = 0; i < 4; i++) a[i] = s.As[stage][wm + 8 * i + (lane >> 2)][k4 + (lane & 3)];
+#pragma unroll
+      for(int j = 0; j < 4; j++) b[j] = s.Bs[stage][k4 + (lane & 3)][wn + 8 * j + (lane >> 2)];
+#pragma unroll
+      for(int i = 0; i < 4; i++)
+#pragma unroll
+        for(int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // ---- epilogue: C (=|+=) alpha * acc in C's own layout ----
+#pragma unroll
+  for(int i = 0; i < 4; i++) {
+    const int m = wm + 8 * i + (lane >> 2);
+    if(it.m0 + m >= Mtot) continue;
+    const int64_t rbase = c_base + s.rowC[m];
+#pragma unroll
+    for(int j = 0; j < 4; j++) {
+#pragma unroll
+      for(int h = 0; h < 2; h++) {
+        const int n = wn + 8 * j + 2 * (lane & 3) + h;
+        if(it.n0 + n >= Ntot) continue;
+        double*      cp = p.C + rbase + s.colC[n];
+        const double v  = p.alpha * acc[i][j][h];
+        *cp             = p.is_assign ? v : *cp + v;
+      }
+    }
+  }
+}
+
+} // namespace
+
+void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,
+                          int is_assign, const double* A, const double* B, double* C,
+                          cudaStream_t stream) {
+  if(wl.items_fp64.empty()) return;
+  Params p;
+  p.lc        = plan.lc;
+  p.A         = A;
+  p.B         = B;
+  p.C         = C;
+  p.groups    = wl.d_groups;
+  p.tasks     = wl.d_tasks;
+  p.items     = wl.d_items;
+  p.alpha     = alpha;
+  p.beta      = beta;
+  p.is_assign = is_assign;
+  const size_t smem = sizeof(Smem);
+  static bool  configured[64] = {false};
+  int          dev            = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  if(dev < 64 && !configured[dev]) {
+    TB_CUDA(cudaFuncSetAttribute(k_contract_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) smem));
+    configured[dev] = true;
+  }
+  const int64_t nitems = (int64_t) wl.items_fp64.size();
+  TB_EXPECTS(nitems < (1ll << 31), "work list too large");
+  k_contract_fp64<<<(unsigned) nitems, NTHREADS, smem, stream>>>(p);
+  TB_CUDA(cudaGetLastError());
+}
+
+// Work items of the FP64 kernel: one per (group, batch index, 128-row tile, 64-col
+// tile), longest first so the hardware block scheduler balances uneven groups.
+void build_items_fp64(const LabelClasses& lc, WorkList& wl) {
+  struct Cost {
+    int64_t cost;
+    DevItem item;
+  };
+  std::vector<Cost> v;
+  for(size_t gi = 0; gi < wl.groups.size(); gi++) {
+    const DevGroup& g = wl.groups[gi];
+    if(g.task_begin == g.task_end) continue;
+    int64_t nbatch = 1, M = 1, N = 1;
+    for(int j = 0; j < lc.nbatch; j++) nbatch *= g.cdims[lc.batch_c[j]];
+    for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
+    for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
+    int64_t work = 0;
+    for(int t = g.task_begin; t < g.task_end; t++) {
+      const DevTask& tk = wl.tasks[t];
+      int64_t        k  = 1;
+      for(int j = 0; j < lc.nk; j++) k *= tk.adims[lc.k_a[j]];
+      for(int j = 0; j < lc.nar; j++) k *= tk.adims[lc.ar_a[j]];
+      for(int j = 0; j < lc.nbr; j++) k *= tk.bdims[lc.br_b[j]];
+      work += (k + BK - 1) / BK;
+    }
+    for(int64_t b = 0; b < nbatch; b++)
+      for(int64_t m0 = 0; m0 < M; m0 += BM)
+        for(int64_t n0 = 0; n0 < N; n0 += BN)
+          v.push_back({work, DevItem{(int32_t) gi, (int32_t) b, (int32_t) m0, (int32_t) n0}});
+  }
+  std::stable_sort(v.begin(), v.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
+  wl.items_fp64.resize(v.size());
+  for(size_t i = 0; i < v.size(); i++) wl.items_fp64[i] = v[i].item;
+}
+
+} // namespace tb

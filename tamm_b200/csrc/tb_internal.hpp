@@ -1,0 +1,131 @@
+// Internal declarations shared by the host (C++) and device (CUDA) sources of
+// libtamm_b200.so.  Nothing here is part of the public C ABI (include/tamm_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tamm_b200.h"
+
+namespace tb {
+
+constexpr int kMaxModes = 8; // modes per tensor
+constexpr int kMaxClass = 4; // labels per label class in a contraction
+
+// Status-carrying exception used inside the library; converted to a status code
+// and tb_last_error() message at the C-ABI boundary.
+struct Error: std::runtime_error {
+  int code;
+  Error(int c, const std::string& m): std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+void              set_last_error(const std::string& msg);
+
+#define TB_EXPECTS(cond, msg)                                                          \
+  do {                                                                                 \
+    if(!(cond)) ::tb::fail(TB_ERR_INVALID, std::string("EXPECTS failed: ") + (msg));   \
+  } while(0)
+
+#define TB_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if(e_ != cudaSuccess)                                                              \
+      ::tb::fail(e_ == cudaErrorMemoryAllocation ? TB_ERR_NO_MEMORY : TB_ERR_CUDA,      \
+                 std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+  } while(0)
+
+// Label classes of one contraction C(cl) += A(al) * B(bl), following
+// kernels::block_multiply (src/tamm/kernels/multiply.hpp:237-330):
+//   batch  : in C, A and B          (mode positions in C, A, B)
+//   m      : in C and A only        (A-outer; C order)
+//   n      : in C and B only        (B-outer; C order)
+//   k      : in A and B only        (inner; A order)
+//   ar, br : only in A / only in B  (reduced by beta-chained GEMM steps)
+struct LabelClasses {
+  int    nc = 0, na = 0, nb = 0;
+  int    nbatch = 0, nm = 0, nn = 0, nk = 0, nar = 0, nbr = 0;
+  int8_t batch_c[kMaxClass], batch_a[kMaxClass], batch_b[kMaxClass];
+  int8_t m_c[kMaxClass], m_a[kMaxClass];
+  int8_t n_c[kMaxClass], n_b[kMaxClass];
+  int8_t k_a[kMaxClass], k_b[kMaxClass];
+  int8_t ar_a[kMaxClass], br_b[kMaxClass];
+  // which class holds the stride-1 (last) mode of A and of B: 0 m/n, 1 k, 2 other
+  int8_t a_contig = 0, b_contig = 0;
+};
+
+LabelClasses classify(const int* cl, int nc, const int* al, int na, const int* bl, int nb);
+
+// Device work-list records.
+struct DevGroup {
+  int64_t c_off;
+  int32_t task_begin, task_end;
+  int32_t cdims[kMaxModes];
+};
+struct DevTask {
+  int64_t a_off, b_off;
+  int32_t adims[kMaxModes];
+  int32_t bdims[kMaxModes];
+};
+// One CTA's output tile: group, batch index, first row / column of the tile.
+struct DevItem {
+  int32_t group, batch, m0, n0;
+};
+
+// Host mirror of a work list plus its device copies.
+struct WorkList {
+  std::vector<DevGroup> groups;
+  std::vector<DevTask>  tasks;
+  std::vector<DevItem>  items_fp64; // tile items for the FP64 kernel
+  double                flops = 0;
+  DevGroup*             d_groups = nullptr;
+  DevTask*              d_tasks  = nullptr;
+  DevItem*              d_items  = nullptr;
+  int                   device   = -1;
+  ~WorkList();
+};
+
+struct Plan {
+  LabelClasses lc;
+  int          mode       = TB_MODE_FP64;
+  double       err_target = 1e-11;
+  int          nslices    = 0;
+  tb_stats     last{};
+};
+
+// ---- launchers (device code in *.cu) ----
+void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,
+                          int is_assign, const double* A, const double* B, double* C,
+                          cudaStream_t stream);
+void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A,
+                   const double* B, double* C, cudaStream_t stream);
+void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double* A,
+                     const double* B, double* C, cudaStream_t stream);
+
+struct AssignLoop {
+  int     nd = 0;
+  int64_t dims[4];
+  int64_t dld[4];
+  int64_t sld[4];
+};
+AssignLoop plan_assign(const int64_t* ddims, const int* dlabels, int nd, const int64_t* sdims,
+                       const int* slabels, int ns);
+void launch_assign(const AssignLoop& lp, double* dst, double scale, const double* src,
+                   int is_assign, cudaStream_t stream);
+void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream);
+void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
+                  cudaStream_t stream);
+double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream);
+void   launch_fill_random(double* x, int64_t n, uint64_t seed, uint64_t first, int dist, double p0,
+                          double p1, cudaStream_t stream);
+
+// Build the work list for one block triple (the single-block entry point).
+WorkList* single_block_worklist(const LabelClasses& lc, const int64_t* adims, const int64_t* bdims,
+                                const int64_t* cdims);
+void finalize_worklist(const LabelClasses& lc, WorkList& wl, bool upload = true); // items + device copy
+
+} // namespace tb

@@ -1,0 +1,565 @@
+// Runtime tier implementation: arena, index spaces, tiling, block store, Scheduler.
+#include "tb_runtime.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <sstream>
+
+namespace tb {
+
+// ------------------------------------------------------------------------- arena
+
+Arena::Arena(int device, int64_t bytes): device_(device) {
+  TB_EXPECTS(bytes > 0, "arena size must be positive");
+  capacity_ = (bytes + 255) & ~int64_t(255);
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&base_), (size_t) capacity_));
+  free_[0] = capacity_;
+}
+
+Arena::~Arena() {
+  if(base_) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device_);
+    cudaFree(base_);
+    if(cur >= 0) cudaSetDevice(cur);
+  }
+}
+
+void* Arena::allocate(int64_t bytes) {
+  if(bytes <= 0) bytes = 1;
+  const int64_t need = (bytes + 255) & ~int64_t(255);
+  auto          best = free_.end();
+  for(auto it = free_.begin(); it != free_.end(); ++it) // best fit
+    if(it->second >= need && (best == free_.end() || it->second < best->second)) best = it;
+  if(best == free_.end()) {
+    std::ostringstream os;
+    os << "device arena exhausted: need " << need << " bytes, " << (capacity_ - used_)
+       << " free of " << capacity_ << " (fragmented)";
+    fail(TB_ERR_NO_MEMORY, os.str());
+  }
+  const int64_t off = best->first, sz = best->second;
+  free_.erase(best);
+  if(sz > need) free_[off + need] = sz - need;
+  inuse_[off] = need;
+  used_ += need;
+  peak_ = std::max(peak_, used_);
+  return base_ + off;
+}
+
+void Arena::deallocate(void* p) {
+  if(p == nullptr) return;
+  const int64_t off = static_cast<char*>(p) - base_;
+  auto          it  = inuse_.find(off);
+  TB_EXPECTS(it != inuse_.end(), "pointer does not belong to this arena");
+  int64_t sz = it->second;
+  inuse_.erase(it);
+  used_ -= sz;
+  int64_t start = off;
+  auto    nx    = free_.lower_bound(off); // coalesce with neighbours
+  if(nx != free_.end() && nx->first == off + sz) {
+    sz += nx->second;
+    nx = free_.erase(nx);
+  }
+  if(nx != free_.begin()) {
+    auto pv = std::prev(nx);
+    if(pv->first + pv->second == start) {
+      start = pv->first;
+      sz += pv->second;
+      free_.erase(pv);
+    }
+  }
+  free_[start] = sz;
+}
+
+void* Scratch::get(int64_t bytes) {
+  if(arena) return arena->allocate(bytes);
+  void* p = nullptr;
+  TB_CUDA(cudaMallocAsync(&p, (size_t) std::max<int64_t>(bytes, 1), stream));
+  return p;
+}
+
+void Scratch::put(void* p) {
+  if(p == nullptr) return;
+  if(arena) arena->deallocate(p);
+  else TB_CUDA(cudaFreeAsync(p, stream));
+}
+
+Ctx::~Ctx() {
+  if(stream) {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    arena.reset();
+    cudaStreamDestroy(stream);
+  }
+}
+
+// ------------------------------------------------------------------ index spaces
+
+int IndexSpace::spin_of(int64_t idx) const {
+  for(const auto& kv: spin)
+    for(const auto& r: kv.second)
+      if(idx >= r.first && idx < r.second) return kv.first;
+  return 0; // default spin of an unattributed index (index_space_interface.hpp:466-468)
+}
+
+std::vector<int64_t> IndexSpace::boundaries(bool with_named) const {
+  std::vector<int64_t> b;
+  if(with_named)
+    for(const auto& kv: named)
+      for(const auto& r: kv.second) {
+        b.push_back(r.first);
+        b.push_back(r.second);
+      }
+  for(const auto& kv: spin)
+    for(const auto& r: kv.second) {
+      b.push_back(r.first);
+      b.push_back(r.second);
+    }
+  std::sort(b.begin(), b.end());
+  b.erase(std::unique(b.begin(), b.end()), b.end());
+  return b;
+}
+
+int64_t TIS::find_root(int64_t r) const {
+  auto it = std::find(tiles.begin(), tiles.end(), r);
+  return it == tiles.end() ? -1 : (int64_t) (it - tiles.begin());
+}
+
+// TiledIndexSpaceInfo::construct_tiled_indices (tiled_index_space.hpp:1135-1194 for a
+// uniform tile size, :1205-1262 for a tile list).
+std::shared_ptr<TIS> make_tis(const std::shared_ptr<IndexSpace>& is, int64_t tile,
+                              const int64_t* tiles, int64_t ntiles) {
+  auto root = std::make_shared<RootTiling>();
+  root->is  = is;
+  auto& off = root->offsets;
+  if(is->n == 0) off.push_back(0);
+  else if(tiles == nullptr) {
+    TB_EXPECTS(tile > 0, "tile size must be positive");
+    auto b = is->boundaries(true);
+    if(b.empty()) {
+      for(int64_t i = 0; i < is->n; i += tile) off.push_back(i);
+    }
+    else {
+      int64_t i = 0;
+      size_t  j = (i == b[0]) ? 1 : 0;
+      while(i < is->n) {
+        off.push_back(i);
+        if(j < b.size() && i + tile >= b[j]) i = b[j++];
+        else i = i + tile;
+      }
+    }
+    off.push_back(is->n);
+  }
+  else {
+    int64_t sum = 0;
+    for(int64_t t = 0; t < ntiles; t++) {
+      TB_EXPECTS(tiles[t] > 0, "tile sizes must be positive");
+      sum += tiles[t];
+    }
+    TB_EXPECTS(sum == is->n, "tile sizes do not add up to the index space size");
+    int64_t j = 0;
+    for(int64_t i = 0; i < is->n; i += tiles[j++]) off.push_back(i);
+    off.push_back(is->n);
+    for(int64_t bnd: is->boundaries(true))
+      TB_EXPECTS(std::binary_search(off.begin(), off.end(), bnd),
+                 "tile list does not split at every named/spin boundary");
+  }
+  const int64_t nt = (int64_t) off.size() - 1;
+  root->spins.resize(nt > 0 ? nt : 0);
+  for(int64_t t = 0; t < nt; t++) root->spins[t] = is->spin_of(off[t]);
+  auto s  = std::make_shared<TIS>();
+  s->root = root;
+  s->tiles.resize(nt > 0 ? nt : 0);
+  std::iota(s->tiles.begin(), s->tiles.end(), 0);
+  return s;
+}
+
+std::shared_ptr<TIS> tis_named(const TIS& parent, const std::string& name) {
+  const auto& is = *parent.root->is;
+  const std::vector<Range>* ranges = nullptr;
+  for(const auto& kv: is.named)
+    if(kv.first == name) ranges = &kv.second;
+  if(name == "all") {
+    auto s   = std::make_shared<TIS>(parent);
+    return s;
+  }
+  TB_EXPECTS(ranges != nullptr, "no named subspace '" + name + "'");
+  auto s  = std::make_shared<TIS>();
+  s->root = parent.root;
+  for(int64_t t: parent.tiles) {
+    const int64_t lo = parent.root->offsets[t];
+    for(const auto& r: *ranges)
+      if(lo >= r.first && lo < r.second) {
+        s->tiles.push_back(t);
+        break;
+      }
+  }
+  return s;
+}
+
+std::shared_ptr<TIS> tis_subrange(const TIS& parent, int64_t first, int64_t last) {
+  TB_EXPECTS(first >= 0 && last >= first && last <= parent.ntiles(), "tile range out of bounds");
+  auto s  = std::make_shared<TIS>();
+  s->root = parent.root;
+  s->tiles.assign(parent.tiles.begin() + first, parent.tiles.begin() + last);
+  return s;
+}
+
+// ---------------------------------------------------------------------- tensors
+
+void Tensor::build_table() {
+  key_stride.assign(nmodes, 1);
+  for(int i = nmodes - 2; i >= 0; i--) key_stride[i] = key_stride[i + 1] * tis[i + 1]->ntiles();
+  keys.clear();
+  offsets.clear();
+  std::vector<std::pair<int64_t, int64_t>> h;
+  int64_t                                  nall = 1;
+  for(int i = 0; i < nmodes; i++) nall *= tis[i]->ntiles();
+  std::vector<int64_t> id(nmodes, 0);
+  for(int64_t lin = 0; lin < nall; lin++) {
+    if(is_non_zero(id.data())) h.push_back({key(id.data()), block_size(id.data())});
+    for(int q = nmodes - 1; q >= 0; q--) {
+      if(++id[q] < tis[q]->ntiles()) break;
+      id[q] = 0;
+    }
+  }
+  std::sort(h.begin(), h.end());
+  int64_t off = 0;
+  for(const auto& kv: h) {
+    keys.push_back(kv.first);
+    offsets.push_back(off);
+    off += kv.second;
+  }
+  nelems = off;
+}
+
+bool Tensor::is_non_zero(const int64_t* blockid) const {
+  // TensorBase::is_non_zero (tensor_base.hpp:243-263)
+  if(!has_spin) return true;
+  int upper = 0, lower = 0;
+  for(int i = 0; i < nmodes; i++) {
+    if(mask[i] == 0) upper += tis[i]->spin(blockid[i]);
+    else if(mask[i] == 1) lower += tis[i]->spin(blockid[i]);
+  }
+  return upper == lower;
+}
+
+int64_t Tensor::key(const int64_t* blockid) const {
+  int64_t k = 0;
+  for(int i = 0; i < nmodes; i++) k += blockid[i] * key_stride[i];
+  return k;
+}
+
+int64_t Tensor::locate(const int64_t* blockid) const {
+  const int64_t k  = key(blockid);
+  auto          it = std::lower_bound(keys.begin(), keys.end(), k);
+  if(it == keys.end() || *it != k) return -1;
+  return offsets[it - keys.begin()];
+}
+
+int64_t Tensor::block_size(const int64_t* blockid) const {
+  int64_t s = 1;
+  for(int i = 0; i < nmodes; i++) s *= tis[i]->size(blockid[i]);
+  return s;
+}
+
+void Tensor::block_dims(const int64_t* blockid, int32_t* dims) const {
+  for(int i = 0; i < nmodes; i++) dims[i] = (int32_t) tis[i]->size(blockid[i]);
+}
+
+void Tensor::check_blockid(const int64_t* blockid) const {
+  for(int i = 0; i < nmodes; i++)
+    TB_EXPECTS(blockid[i] >= 0 && blockid[i] < tis[i]->ntiles(), "block id out of range");
+}
+
+void Tensor::require_allocated() const {
+  if(data == nullptr && nelems > 0) fail(TB_ERR_STATE, "tensor is not allocated");
+}
+
+// -------------------------------------------------------------------- scheduler
+
+namespace {
+
+int find_label(const std::vector<int>& v, int x) {
+  for(size_t i = 0; i < v.size(); i++)
+    if(v[i] == x) return (int) i;
+  return -1;
+}
+
+// label-space tile -> tensor tile for every mode (internal::translate_blockid,
+// utils.hpp:264-286), -1 where the label tile is not a tile of the tensor's space
+std::vector<std::vector<int64_t>> tile_maps(const Labeled& x) {
+  std::vector<std::vector<int64_t>> m(x.t->nmodes);
+  for(int i = 0; i < x.t->nmodes; i++) {
+    const TIS& ls = *x.ltis[i];
+    const TIS& ts = *x.t->tis[i];
+    TB_EXPECTS(ls.root == ts.root, "label space and tensor space do not share a root tiling");
+    m[i].resize(ls.ntiles());
+    for(int64_t t = 0; t < ls.ntiles(); t++) {
+      m[i][t] = ts.find_root(ls.tiles[t]);
+      TB_EXPECTS(m[i][t] >= 0, "label tile is not a tile of the tensor's index space");
+    }
+  }
+  return m;
+}
+
+bool next_tuple(std::vector<int64_t>& it, const std::vector<int64_t>& nt) {
+  for(int q = (int) it.size() - 1; q >= 0; q--) {
+    if(++it[q] < nt[q]) return true;
+    it[q] = 0;
+  }
+  return false;
+}
+
+std::string signature(const Op& op) {
+  std::ostringstream os;
+  auto               put = [&](const Labeled& x) {
+    os << x.t << ":";
+    for(size_t i = 0; i < x.labels.size(); i++) os << x.labels[i] << "@" << x.ltis[i].get() << ",";
+    os << "|";
+  };
+  os << (int) op.kind << "|";
+  put(op.lhs);
+  if(op.kind != Op::Set) put(op.a);
+  if(op.kind == Op::Mult) put(op.b);
+  return os.str();
+}
+
+// MultOp::execute_bufacc enumeration (multop.hpp:576-893): owned admitted output
+// blocks x admitted reduction tiles, as device work-list groups and tasks.
+std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& lc, bool upload) {
+  const Labeled &c = op.lhs, &a = op.a, &b = op.b;
+  auto cm = tile_maps(c), am = tile_maps(a), bm = tile_maps(b);
+  // reduction labels: unique rhs labels (A then B) not in the lhs, sorted (multop.hpp:593-601)
+  std::vector<int>                 red;
+  std::map<int, const TIS*>        lsp;
+  auto note = [&](const Labeled& x) {
+    for(size_t i = 0; i < x.labels.size(); i++) {
+      auto it = lsp.find(x.labels[i]);
+      if(it == lsp.end()) lsp[x.labels[i]] = x.ltis[i].get();
+      else
+        TB_EXPECTS(it->second->root == x.ltis[i]->root && it->second->tiles == x.ltis[i]->tiles,
+                   "one label bound to two different index spaces");
+    }
+  };
+  note(c);
+  note(a);
+  note(b);
+  for(int l: a.labels)
+    if(find_label(c.labels, l) < 0 && find_label(red, l) < 0) red.push_back(l);
+  for(int l: b.labels)
+    if(find_label(c.labels, l) < 0 && find_label(red, l) < 0) red.push_back(l);
+  std::sort(red.begin(), red.end());
+  std::vector<int64_t> red_nt, c_nt;
+  for(int l: red) red_nt.push_back(lsp[l]->ntiles());
+  for(size_t i = 0; i < c.labels.size(); i++) c_nt.push_back(c.ltis[i]->ntiles());
+  std::vector<int> a_out(a.labels.size()), a_red(a.labels.size()), b_out(b.labels.size()),
+    b_red(b.labels.size());
+  for(size_t i = 0; i < a.labels.size(); i++) {
+    a_out[i] = find_label(c.labels, a.labels[i]);
+    a_red[i] = find_label(red, a.labels[i]);
+  }
+  for(size_t i = 0; i < b.labels.size(); i++) {
+    b_out[i] = find_label(c.labels, b.labels[i]);
+    b_red[i] = find_label(red, b.labels[i]);
+  }
+
+  auto wl = std::make_shared<WorkList>();
+  for(int64_t n: c_nt)
+    if(n == 0) return wl;
+  for(int64_t n: red_nt)
+    if(n == 0) return wl;
+  std::vector<int64_t> itval(c.labels.size(), 0), inner(red.size(), 0);
+  std::vector<int64_t> cid(c.labels.size()), aid(a.labels.size()), bid(b.labels.size());
+  do {
+    for(size_t i = 0; i < cid.size(); i++) cid[i] = cm[i][itval[i]];
+    if(!c.t->is_non_zero(cid.data())) continue;
+    DevGroup g{};
+    g.c_off = c.t->locate(cid.data());
+    c.t->block_dims(cid.data(), g.cdims);
+    g.task_begin = (int32_t) wl->tasks.size();
+    std::fill(inner.begin(), inner.end(), 0);
+    do {
+      for(size_t i = 0; i < aid.size(); i++) {
+        int64_t l = a_out[i] >= 0 ? itval[a_out[i]] : inner[a_red[i]];
+        aid[i]    = am[i][l];
+      }
+      if(!a.t->is_non_zero(aid.data())) continue;
+      for(size_t i = 0; i < bid.size(); i++) {
+        int64_t l = b_out[i] >= 0 ? itval[b_out[i]] : inner[b_red[i]];
+        bid[i]    = bm[i][l];
+      }
+      if(!b.t->is_non_zero(bid.data())) continue;
+      DevTask t{};
+      t.a_off = a.t->locate(aid.data());
+      t.b_off = b.t->locate(bid.data());
+      a.t->block_dims(aid.data(), t.adims);
+      b.t->block_dims(bid.data(), t.bdims);
+      wl->tasks.push_back(t);
+    } while(!red.empty() && next_tuple(inner, red_nt));
+    TB_EXPECTS(wl->tasks.size() < (1ull << 31), "too many tasks in one contraction");
+    g.task_end = (int32_t) wl->tasks.size();
+    wl->groups.push_back(g);
+  } while(!cid.empty() && next_tuple(itval, c_nt));
+  finalize_worklist(lc, *wl, upload);
+  return wl;
+}
+
+} // namespace
+
+std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload) {
+  return build_mult_worklist(op, lc, upload);
+}
+
+void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
+                  double* C, cudaStream_t stream, Arena* arena); // tb_capi.cpp
+
+void Sched::run(Op& op) {
+  cudaStream_t st = ctx->stream;
+  if(op.kind == Op::Set) {
+    op.lhs.t->require_allocated();
+    if(!op.set_blocks) {
+      auto blocks = std::make_shared<std::vector<int64_t>>();
+      bool whole  = true;
+      for(int i = 0; i < op.lhs.t->nmodes; i++)
+        if(op.lhs.ltis[i]->tiles != op.lhs.t->tis[i]->tiles) whole = false;
+      if(!whole) {
+        auto                 m = tile_maps(op.lhs);
+        std::vector<int64_t> nt, it(op.lhs.t->nmodes, 0), id(op.lhs.t->nmodes);
+        for(int i = 0; i < op.lhs.t->nmodes; i++) nt.push_back(op.lhs.ltis[i]->ntiles());
+        bool empty = false;
+        for(auto n: nt) empty |= (n == 0);
+        if(!empty) do {
+            for(int i = 0; i < op.lhs.t->nmodes; i++) id[i] = m[i][it[i]];
+            if(!op.lhs.t->is_non_zero(id.data())) continue;
+            blocks->push_back(op.lhs.t->locate(id.data()));
+            blocks->push_back(op.lhs.t->block_size(id.data()));
+          } while(!it.empty() && next_tuple(it, nt));
+      }
+      op.set_blocks = blocks;
+    }
+    if(op.set_blocks->empty()) launch_fill(op.lhs.t->data, op.lhs.t->nelems, op.value, op.is_assign, st);
+    else
+      for(size_t i = 0; i < op.set_blocks->size(); i += 2)
+        launch_fill(op.lhs.t->data + (*op.set_blocks)[i], (*op.set_blocks)[i + 1], op.value,
+                    op.is_assign, st);
+    return;
+  }
+  if(op.kind == Op::Add) {
+    op.lhs.t->require_allocated();
+    op.a.t->require_allocated();
+    if(!op.add_blocks) {
+      auto blocks = std::make_shared<std::vector<Op::AddBlock>>();
+      // FlatAddPlan condition (addop.hpp:245-251): same labels, same layout
+      bool flat = op.lhs.labels == op.a.labels && op.lhs.t->has_spin == op.a.t->has_spin &&
+                  op.lhs.t->nmodes == op.a.t->nmodes && op.lhs.t->keys == op.a.t->keys &&
+                  op.lhs.t->offsets == op.a.t->offsets;
+      for(int i = 0; flat && i < op.lhs.t->nmodes; i++)
+        flat = op.lhs.ltis[i]->tiles == op.lhs.t->tis[i]->tiles &&
+               op.a.ltis[i]->tiles == op.a.t->tis[i]->tiles &&
+               op.lhs.t->tis[i]->tiles == op.a.t->tis[i]->tiles &&
+               op.lhs.t->tis[i]->root == op.a.t->tis[i]->root;
+      op.flat = flat;
+      if(!flat) {
+        // LHSAddPlan (addop.hpp:457-519): loop over the merged labels, skip pairs with
+        // a non-admitted side, apply the block assign.
+        auto             lm = tile_maps(op.lhs), rm = tile_maps(op.a);
+        std::vector<int> merged = op.lhs.labels;
+        std::vector<const TIS*> msp;
+        for(size_t i = 0; i < op.lhs.labels.size(); i++) msp.push_back(op.lhs.ltis[i].get());
+        for(size_t i = 0; i < op.a.labels.size(); i++)
+          if(find_label(merged, op.a.labels[i]) < 0) {
+            merged.push_back(op.a.labels[i]);
+            msp.push_back(op.a.ltis[i].get());
+          }
+        std::vector<int64_t> nt, it(merged.size(), 0);
+        for(auto* s: msp) nt.push_back(s->ntiles());
+        bool empty = false;
+        for(auto n: nt) empty |= (n == 0);
+        std::vector<int64_t> lid(op.lhs.t->nmodes), rid(op.a.t->nmodes);
+        if(!empty) do {
+            for(int i = 0; i < op.lhs.t->nmodes; i++) lid[i] = lm[i][it[find_label(merged, op.lhs.labels[i])]];
+            for(int i = 0; i < op.a.t->nmodes; i++) rid[i] = rm[i][it[find_label(merged, op.a.labels[i])]];
+            if(!op.lhs.t->is_non_zero(lid.data()) || !op.a.t->is_non_zero(rid.data())) continue;
+            Op::AddBlock ab{};
+            ab.dst_off = op.lhs.t->locate(lid.data());
+            ab.src_off = op.a.t->locate(rid.data());
+            for(int i = 0; i < op.lhs.t->nmodes; i++) ab.ddims[i] = op.lhs.t->tis[i]->size(lid[i]);
+            for(int i = 0; i < op.a.t->nmodes; i++) ab.sdims[i] = op.a.t->tis[i]->size(rid[i]);
+            blocks->push_back(ab);
+          } while(!it.empty() && next_tuple(it, nt));
+      }
+      op.add_blocks = blocks;
+    }
+    if(op.flat) {
+      launch_axpby(op.alpha, op.a.t->data, op.is_assign ? 0.0 : 1.0, op.lhs.t->data,
+                   op.lhs.t->nelems, st);
+      return;
+    }
+    for(const auto& ab: *op.add_blocks) {
+      AssignLoop lp = plan_assign(ab.ddims, op.lhs.labels.data(), op.lhs.t->nmodes, ab.sdims,
+                                  op.a.labels.data(), op.a.t->nmodes);
+      launch_assign(lp, op.lhs.t->data + ab.dst_off, op.alpha, op.a.t->data + ab.src_off,
+                    op.is_assign, st);
+    }
+    return;
+  }
+  // MultOp
+  op.lhs.t->require_allocated();
+  op.a.t->require_allocated();
+  op.b.t->require_allocated();
+  if(!op.wl) {
+    const std::string sig = signature(op);
+    auto              pit = plan_cache.find(sig);
+    if(pit == plan_cache.end()) {
+      auto plan        = std::make_shared<Plan>();
+      plan->lc         = classify(op.lhs.labels.data(), (int) op.lhs.labels.size(), op.a.labels.data(),
+                                  (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
+      plan->mode       = ctx->mode;
+      plan->err_target = ctx->err_target;
+      plan->nslices    = ctx->nslices;
+      plan_cache[sig]  = plan;
+      wl_cache[sig]    = build_mult_worklist(op, plan->lc, true);
+      pit              = plan_cache.find(sig);
+    }
+    op.plan = pit->second;
+    op.wl   = wl_cache[sig];
+  }
+  op.plan->mode       = ctx->mode;
+  op.plan->err_target = ctx->err_target;
+  op.plan->nslices    = ctx->nslices;
+  op.flops            = op.wl->flops;
+  run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
+               ctx->arena.get());
+}
+
+void Sched::execute(bool profile) {
+  TB_CUDA(cudaSetDevice(ctx->device));
+  prof_ms.clear();
+  prof_flops.clear();
+  std::vector<cudaEvent_t> ev;
+  if(profile) {
+    ev.resize(2 * (ops.size() - start));
+    for(auto& e: ev) TB_CUDA(cudaEventCreate(&e));
+  }
+  for(size_t i = start; i < ops.size(); i++) {
+    if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start)], ctx->stream));
+    run(ops[i]);
+    if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start) + 1], ctx->stream));
+  }
+  if(profile) {
+    TB_CUDA(cudaStreamSynchronize(ctx->stream));
+    for(size_t i = start; i < ops.size(); i++) {
+      float ms = 0;
+      TB_CUDA(cudaEventElapsedTime(&ms, ev[2 * (i - start)], ev[2 * (i - start) + 1]));
+      prof_ms.push_back(ms);
+      prof_flops.push_back(ops[i].flops);
+    }
+    for(auto& e: ev) cudaEventDestroy(e);
+  }
+  start = ops.size();
+}
+
+} // namespace tb

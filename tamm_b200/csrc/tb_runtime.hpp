@@ -1,0 +1,169 @@
+// Runtime tier: execution context with a stream-ordered device arena, index spaces,
+// tiled index spaces, block-sparse tensors in a device-resident block store, and the
+// Scheduler.  Exposed through the runtime half of include/tamm_b200.h.
+#pragma once
+
+#include "tb_internal.hpp"
+
+#include <map>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace tb {
+
+// Stream-ordered arena: one cudaMalloc carved by a coalescing best-fit free list
+// (the role of TAMM's RMM pool_memory_resource, src/tamm/mr/pool_memory_resource.hpp,
+// with TAMM_GPU_POOL semantics).  Every user of an arena works on the context's
+// single stream, so a block freed on the host is reusable by any later stream work.
+class Arena {
+public:
+  Arena(int device, int64_t bytes);
+  ~Arena();
+  Arena(const Arena&)            = delete;
+  Arena& operator=(const Arena&) = delete;
+  void*   allocate(int64_t bytes);
+  void    deallocate(void* p);
+  int64_t used() const { return used_; }
+  int64_t peak() const { return peak_; }
+  int64_t capacity() const { return capacity_; }
+
+private:
+  int                        device_;
+  char*                      base_     = nullptr;
+  int64_t                    capacity_ = 0;
+  int64_t                    used_     = 0;
+  int64_t                    peak_     = 0;
+  std::map<int64_t, int64_t> free_;  // offset -> size
+  std::map<int64_t, int64_t> inuse_; // offset -> size
+};
+
+struct Ctx {
+  int                    device = 0;
+  cudaStream_t           stream = nullptr;
+  std::unique_ptr<Arena> arena;
+  int                    mode       = TB_MODE_FP64;
+  double                 err_target = 1e-11;
+  int                    nslices    = 0;
+  ~Ctx();
+};
+
+using Range = std::pair<int64_t, int64_t>; // [lo, hi)
+
+struct IndexSpace {
+  int64_t                                                 n = 0;
+  std::vector<std::pair<std::string, std::vector<Range>>> named;
+  std::vector<std::pair<int, std::vector<Range>>>         spin;
+  bool                                                    has_spin() const { return !spin.empty(); }
+  int                                                     spin_of(int64_t idx) const;
+  std::vector<int64_t>                                    boundaries(bool with_named) const;
+};
+
+// The root tiling of an IndexSpace (TiledIndexSpaceInfo): tile start offsets and
+// the spin of each tile (spin of its first index, tiled_index_space.hpp:1327).
+struct RootTiling {
+  std::shared_ptr<IndexSpace> is;
+  std::vector<int64_t>        offsets; // ntiles + 1
+  std::vector<int>            spins;
+};
+
+// A tiled index space: a list of root tiles (all of them for the root space,
+// a subset for named subspaces and tile sub-ranges).
+struct TIS {
+  std::shared_ptr<RootTiling> root;
+  std::vector<int64_t>        tiles;
+  int64_t                     ntiles() const { return (int64_t) tiles.size(); }
+  int64_t size(int64_t t) const { return root->offsets[tiles[t] + 1] - root->offsets[tiles[t]]; }
+  int     spin(int64_t t) const { return root->spins[tiles[t]]; }
+  // index of root tile r in this space, -1 if absent (TiledIndexSpace::info_translate)
+  int64_t find_root(int64_t r) const;
+};
+
+struct Tensor {
+  int                               nmodes = 0;
+  std::vector<std::shared_ptr<TIS>> tis;
+  bool                              has_spin = false;
+  int                               mask[kMaxModes] = {0};
+  std::vector<int64_t>              key_stride;
+  std::vector<int64_t>              keys, offsets; // admitted blocks, key order
+  int64_t                           nelems = 0;
+  Ctx*                              ctx    = nullptr;
+  double*                           data   = nullptr;
+
+  void    build_table(); // Distribution_NW (distribution.hpp:201-243)
+  bool    is_non_zero(const int64_t* blockid) const;
+  int64_t key(const int64_t* blockid) const;
+  int64_t locate(const int64_t* blockid) const; // -1 if not stored
+  int64_t block_size(const int64_t* blockid) const;
+  void    block_dims(const int64_t* blockid, int32_t* dims) const;
+  void    check_blockid(const int64_t* blockid) const;
+  void    require_allocated() const;
+};
+
+struct Labeled {
+  Tensor*                           t = nullptr;
+  std::vector<int>                  labels;
+  std::vector<std::shared_ptr<TIS>> ltis; // label space per mode
+};
+
+struct Op {
+  enum Kind { Set, Add, Mult } kind;
+  Labeled lhs, a, b;
+  double  alpha = 1.0, value = 0.0;
+  int     is_assign = 0;
+  // cached execution state
+  std::shared_ptr<Plan>     plan;
+  std::shared_ptr<WorkList> wl;
+  struct AddBlock {
+    int64_t dst_off, src_off;
+    int64_t ddims[kMaxModes], sdims[kMaxModes];
+  };
+  std::shared_ptr<std::vector<AddBlock>> add_blocks;
+  bool                                   flat = false;
+  std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
+  double                                 flops = 0;
+};
+
+struct Sched {
+  Ctx*                                              ctx = nullptr;
+  std::vector<Op>                                   ops;
+  size_t                                            start = 0;
+  std::vector<double>                               prof_ms, prof_flops;
+  std::map<std::string, std::shared_ptr<Plan>>     plan_cache;
+  std::map<std::string, std::shared_ptr<WorkList>> wl_cache;
+  void                                              execute(bool profile);
+  void                                              run(Op& op);
+};
+
+// scratch memory source for split operands
+struct Scratch {
+  Arena*       arena  = nullptr; // null: cudaMallocAsync on the stream
+  cudaStream_t stream = nullptr;
+  void*        get(int64_t bytes);
+  void         put(void* p);
+};
+
+} // namespace tb
+
+struct tb_ctx_s {
+  std::unique_ptr<tb::Ctx> p;
+};
+struct tb_is_s {
+  std::shared_ptr<tb::IndexSpace> p;
+};
+struct tb_tis_s {
+  std::shared_ptr<tb::TIS> p;
+};
+struct tb_tensor_s {
+  std::unique_ptr<tb::Tensor> p;
+};
+struct tb_sched_s {
+  std::unique_ptr<tb::Sched> p;
+};
+struct tb_plan_s {
+  tb::Plan p;
+};
+struct tb_worklist_s {
+  std::unique_ptr<tb::WorkList> p;
+};

@@ -1,0 +1,452 @@
+"""Python front-end mirroring TAMM's LabeledTensor / Scheduler API over the C ABI.
+
+    is_  = IndexSpace(range(100), named={"occ": [(0, 20)], "virt": [(20, 100)]},
+                      spin={1: [(0, 10), (20, 60)], 2: [(10, 20), (60, 100)]})
+    MO   = TiledIndexSpace(is_, tiles)             # TiledIndexSpace{is, tiles}
+    O, V = MO("occ"), MO("virt")
+    a, b, c, d = V.labels(4)
+    i, j = O.labels(2)
+    t2 = Tensor([V, V, O, O], spin=(2, 2))          # Tensor<T>{{V,V,O,O},{2,2}}
+    sch = Scheduler(ec)
+    sch.allocate(t2, r2, v)
+    sch(r2(a, b, i, j).iadd(v(a, b, c, d) * t2(c, d, i, j))).execute(ExecutionHW.GPU)
+
+C++ `C(...) += expr` / `-=` / `=` are `.iadd(expr)` / `.isub(expr)` / `.assign(expr)`
+here (Python has no augmented assignment on a call).  Everything executes on the
+GPU through libtamm_b200.so; there is no host execution path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import itertools
+from typing import Sequence
+
+import numpy as np
+
+from . import _capi as A
+from ._capi import call
+
+
+class ExecutionHW:
+    DEFAULT = 0
+    CPU = 1
+    GPU = 2
+
+
+class Precision:
+    FP64 = A.TB_MODE_FP64
+    INT8 = A.TB_MODE_INT8
+    BF16X3 = A.TB_MODE_BF16X3
+
+
+def _i64arr(v):
+    a = np.ascontiguousarray(np.asarray(list(v) if not isinstance(v, np.ndarray) else v, dtype=np.int64))
+    return a if a.size else np.zeros(1, dtype=np.int64)
+
+
+class ExecutionContext:
+    """ExecutionContext on one GPU: stream + stream-ordered device arena."""
+
+    def __init__(self, device: int = 0, pool_bytes: int = 0):
+        self.h = A.h()
+        call("tb_ctx_create", device, int(pool_bytes), C.byref(self.h))
+        self.device = device
+
+    def set_precision(self, mode=Precision.FP64, err_target=1e-11, nslices=0):
+        call("tb_ctx_set_precision", self.h, int(mode), float(err_target), int(nslices))
+
+    @property
+    def stream(self):
+        s = A.vp()
+        call("tb_ctx_stream", self.h, C.byref(s))
+        return s.value
+
+    def synchronize(self):
+        call("tb_ctx_synchronize", self.h)
+
+    def arena_info(self):
+        u, p, c = C.c_int64(), C.c_int64(), C.c_int64()
+        call("tb_ctx_arena_info", self.h, C.byref(u), C.byref(p), C.byref(c))
+        return u.value, p.value, c.value
+
+    def close(self):
+        if self.h:
+            A.lib().tb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ranges(rs):
+    out = []
+    for r in rs:
+        if isinstance(r, range):
+            assert r.step == 1
+            out.append((r.start, r.stop))
+        else:
+            out.append((int(r[0]), int(r[1])))
+    return out
+
+
+class IndexSpace:
+    """IndexSpace{range(n), {{name, {ranges}}...}, {{Spin{s}, {ranges}}...}}."""
+
+    def __init__(self, n, named: dict | None = None, spin: dict | None = None):
+        if isinstance(n, range):
+            assert n.start == 0 and n.step == 1
+            n = n.stop
+        self.n = int(n)
+        named = named or {}
+        spin = spin or {}
+        names = list(named.keys())
+        cnames = (C.c_char_p * max(len(names), 1))(*[s.encode() for s in names])
+        nn = (C.c_int * max(len(names), 1))(*[len(_ranges(named[s])) for s in names])
+        nr = _i64arr([x for s in names for r in _ranges(named[s]) for x in r])
+        svals = list(spin.keys())
+        sv = (C.c_int * max(len(svals), 1))(*[int(s) for s in svals])
+        sn = (C.c_int * max(len(svals), 1))(*[len(_ranges(spin[s])) for s in svals])
+        sr = _i64arr([x for s in svals for r in _ranges(spin[s]) for x in r])
+        self.h = A.h()
+        call("tb_is_create", self.n, len(names), cnames, nn, nr.ctypes.data_as(A.i64p), len(svals),
+             sv, sn, sr.ctypes.data_as(A.i64p), C.byref(self.h))
+
+    def __del__(self):
+        try:
+            A.lib().tb_is_destroy(self.h)
+        except Exception:
+            pass
+
+
+_label_ids = itertools.count(1)
+
+
+class TiledIndexLabel:
+    def __init__(self, tis: "TiledIndexSpace", name: str = ""):
+        self.tis = tis
+        self.id = next(_label_ids)
+        self.name = name
+
+    def __repr__(self):
+        return f"TiledIndexLabel({self.name or self.id})"
+
+
+class TiledIndexSpace:
+    """TiledIndexSpace{is, tile} or TiledIndexSpace{is, tile_list}."""
+
+    def __init__(self, is_: IndexSpace | None = None, tile=None, _handle=None, _parent=None):
+        self.parent = _parent
+        self.is_ = is_ if is_ is not None else (_parent.is_ if _parent else None)
+        if _handle is not None:
+            self.h = _handle
+        else:
+            self.h = A.h()
+            if isinstance(tile, (list, tuple, np.ndarray)):
+                t = _i64arr(tile)
+                call("tb_tis_create", is_.h, 0, t.ctypes.data_as(A.i64p), len(tile), C.byref(self.h))
+            else:
+                call("tb_tis_create", is_.h, int(tile), None, 0, C.byref(self.h))
+        n = C.c_int64()
+        call("tb_tis_num_tiles", self.h, C.byref(n))
+        nt = n.value
+        sizes = np.zeros(max(nt, 1), dtype=np.int64)
+        spins = np.zeros(max(nt, 1), dtype=np.int32)
+        roots = np.zeros(max(nt, 1), dtype=np.int64)
+        call("tb_tis_tiles", self.h, sizes.ctypes.data_as(A.i64p), spins.ctypes.data_as(A.ip),
+             roots.ctypes.data_as(A.i64p))
+        self.tile_sizes = sizes[:nt].copy()
+        self.tile_spins = spins[:nt].copy()
+        self.root_tiles = roots[:nt].copy()
+
+    def __call__(self, name: str = "all") -> "TiledIndexSpace":
+        h = A.h()
+        call("tb_tis_named", self.h, name.encode(), C.byref(h))
+        return TiledIndexSpace(_handle=h, _parent=self)
+
+    def sub(self, first: int, last: int) -> "TiledIndexSpace":
+        """TiledIndexSpace{tis, range(first, last)} (a range of tiles)."""
+        h = A.h()
+        call("tb_tis_subrange", self.h, int(first), int(last), C.byref(h))
+        return TiledIndexSpace(_handle=h, _parent=self)
+
+    @property
+    def num_tiles(self):
+        return len(self.tile_sizes)
+
+    def tile_size(self, i):
+        return int(self.tile_sizes[i])
+
+    def spin(self, i):
+        return int(self.tile_spins[i])
+
+    def label(self, name=""):
+        return TiledIndexLabel(self, name)
+
+    def labels(self, n, name="all"):
+        sp = self if name == "all" else self(name)
+        return tuple(TiledIndexLabel(sp) for _ in range(n))
+
+    def __del__(self):
+        try:
+            A.lib().tb_tis_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Tensor:
+    """Tensor<double>{tis...}, with `spin=(nupper, nlower)` or `spin_mask=[...]` for
+    spin-blocked sparsity."""
+
+    def __init__(self, spaces: Sequence, spin=None, spin_mask=None):
+        self.spaces = [s.tis if isinstance(s, TiledIndexLabel) else s for s in spaces]
+        self.default_labels = [s if isinstance(s, TiledIndexLabel) else None for s in spaces]
+        n = len(self.spaces)
+        hs = (A.h * max(n, 1))(*[s.h for s in self.spaces])
+        self.h = A.h()
+        if spin is not None:
+            call("tb_tensor_create_spin_sizes", n, hs, int(spin[0]), int(spin[1]), C.byref(self.h))
+        elif spin_mask is not None:
+            m = (C.c_int * n)(*spin_mask)
+            call("tb_tensor_create", n, hs, m, C.byref(self.h))
+        else:
+            call("tb_tensor_create", n, hs, None, C.byref(self.h))
+        nm, nb, ne = C.c_int(), C.c_int64(), C.c_int64()
+        call("tb_tensor_info", self.h, C.byref(nm), C.byref(nb), C.byref(ne))
+        self.nmodes, self.nblocks, self.nelems = nm.value, nb.value, ne.value
+        self.ec = None
+
+    # --- storage ---
+    def allocate(self, ec: ExecutionContext):
+        call("tb_tensor_allocate", self.h, ec.h)
+        self.ec = ec
+        return self
+
+    def deallocate(self):
+        call("tb_tensor_deallocate", self.h)
+        self.ec = None
+
+    def data_ptr(self):
+        p = A.vp()
+        call("tb_tensor_data", self.h, C.byref(p))
+        return p.value
+
+    def block_table(self):
+        k = np.zeros(max(self.nblocks, 1), dtype=np.int64)
+        o = np.zeros(max(self.nblocks, 1), dtype=np.int64)
+        call("tb_tensor_block_table", self.h, k.ctypes.data_as(A.i64p), o.ctypes.data_as(A.i64p))
+        return k[:self.nblocks].copy(), o[:self.nblocks].copy()
+
+    def is_non_zero(self, blockid):
+        b = _i64arr(blockid)
+        r = C.c_int()
+        call("tb_tensor_is_non_zero", self.h, b.ctypes.data_as(A.i64p), C.byref(r))
+        return bool(r.value)
+
+    def block_dims(self, blockid):
+        b = _i64arr(blockid)
+        d = np.zeros(max(self.nmodes, 1), dtype=np.int64)
+        call("tb_tensor_block_dims", self.h, b.ctypes.data_as(A.i64p), d.ctypes.data_as(A.i64p))
+        return tuple(int(x) for x in d[:self.nmodes])
+
+    def locate(self, blockid):
+        b = _i64arr(blockid)
+        o = C.c_int64()
+        call("tb_tensor_locate", self.h, b.ctypes.data_as(A.i64p), C.byref(o))
+        return o.value
+
+    def get(self, blockid) -> np.ndarray:
+        dims = self.block_dims(blockid)
+        buf = np.zeros(int(np.prod(dims)) if dims else 1, dtype=np.float64)
+        b = _i64arr(blockid)
+        call("tb_tensor_get", self.h, b.ctypes.data_as(A.i64p), buf.ctypes.data_as(A.dp), buf.size)
+        return buf.reshape(dims)
+
+    def put(self, blockid, values):
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        b = _i64arr(blockid)
+        call("tb_tensor_put", self.h, b.ctypes.data_as(A.i64p), v.ctypes.data_as(A.dp), v.size)
+
+    def add(self, blockid, values):
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        b = _i64arr(blockid)
+        call("tb_tensor_add", self.h, b.ctypes.data_as(A.i64p), v.ctypes.data_as(A.dp), v.size)
+
+    def write(self, packed: np.ndarray):
+        v = np.ascontiguousarray(packed, dtype=np.float64).ravel()
+        call("tb_tensor_write", self.h, v.ctypes.data_as(A.dp), v.size)
+
+    def read(self) -> np.ndarray:
+        v = np.zeros(max(self.nelems, 1), dtype=np.float64)
+        call("tb_tensor_read", self.h, v.ctypes.data_as(A.dp), self.nelems)
+        return v[:self.nelems]
+
+    def norm(self) -> float:
+        r = C.c_double()
+        call("tb_tensor_norm", self.h, C.byref(r))
+        return r.value
+
+    def fill_random(self, seed, dist=0, p0=-1.0, p1=1.0, first=0):
+        call("tb_fill_random", self.data_ptr(), self.nelems, int(seed), int(first), int(dist),
+             float(p0), float(p1), A.vp(self.ec.stream))
+        self.ec.synchronize()
+
+    # --- labelling ---
+    def __call__(self, *labels) -> "LabeledTensor":
+        if len(labels) == 1 and isinstance(labels[0], str):
+            names = [s.strip() for s in labels[0].split(",")] if labels[0] else []
+            return LabeledTensor(self, names)
+        if not labels:
+            # T(): the tensor's own labels; labels of equal (space, position) coincide
+            return LabeledTensor(self, [f"__mode{i}" for i in range(self.nmodes)])
+        return LabeledTensor(self, list(labels))
+
+    def __del__(self):
+        try:
+            A.lib().tb_tensor_destroy(self.h)
+        except Exception:
+            pass
+
+
+class _Product:
+    def __init__(self, alpha, factors):
+        self.alpha = alpha
+        self.factors = factors
+
+    def __mul__(self, other):
+        if isinstance(other, LabeledTensor):
+            return _Product(self.alpha, self.factors + [other])
+        return _Product(self.alpha * float(other), self.factors)
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return _Product(-self.alpha, self.factors)
+
+
+class LabeledTensor:
+    def __init__(self, tensor: Tensor, labels: list):
+        if len(labels) != tensor.nmodes:
+            raise ValueError(f"{len(labels)} labels for a {tensor.nmodes}-mode tensor")
+        self.tensor = tensor
+        self.labels = labels
+
+    def __mul__(self, other):
+        return _Product(1.0, [self]) * other
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return _Product(-1.0, [self])
+
+    # C++ `=`, `+=`, `-=`
+    def assign(self, rhs):
+        return _OpSpec(self, rhs, is_assign=True, sign=1.0)
+
+    def iadd(self, rhs):
+        return _OpSpec(self, rhs, is_assign=False, sign=1.0)
+
+    def isub(self, rhs):
+        return _OpSpec(self, rhs, is_assign=False, sign=-1.0)
+
+
+class _OpSpec:
+    def __init__(self, lhs, rhs, is_assign, sign):
+        self.lhs, self.rhs, self.is_assign, self.sign = lhs, rhs, is_assign, sign
+
+
+def _to_c_labeled(lt: LabeledTensor, ids: dict, keep: list):
+    """tb_labeled for one operand; labels equal within one op get equal int ids
+    (the per-op int labels of MultOp::fillin_int_labels, multop.hpp:955-970)."""
+    n = lt.tensor.nmodes
+    lab = (C.c_int * max(n, 1))()
+    sp = (A.h * max(n, 1))()
+    for k, l in enumerate(lt.labels):
+        if isinstance(l, TiledIndexLabel):
+            key = ("L", l.id)
+            sp[k] = l.tis.h
+        else:
+            key = ("S", l)
+            sp[k] = None
+        if key not in ids:
+            ids[key] = -(len(ids) + 1)
+        lab[k] = ids[key]
+    keep += [lab, sp]
+    return A.tb_labeled(lt.tensor.h, C.cast(lab, A.ip), C.cast(sp, C.POINTER(A.h)))
+
+
+def mult_info(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor):
+    """(admitted output blocks, admitted block triples, FP64 FLOPs) of lhs += a * b,
+    computed on the host without running anything."""
+    ids: dict = {}
+    keep: list = []
+    l, x, y = (_to_c_labeled(t, ids, keep) for t in (lhs, a, b))
+    ng, nt, fl = C.c_int64(), C.c_int64(), C.c_double()
+    call("tb_mult_info", l, x, y, C.byref(ng), C.byref(nt), C.byref(fl))
+    return ng.value, nt.value, fl.value
+
+
+class Scheduler:
+    """Scheduler{ec}: sch(op)...execute(hw, profile)."""
+
+    def __init__(self, ec: ExecutionContext):
+        self.ec = ec
+        self.h = A.h()
+        call("tb_sched_create", ec.h, C.byref(self.h))
+        self._keep = []
+
+    def allocate(self, *tensors):
+        for t in tensors:
+            t.allocate(self.ec)
+        return self
+
+    def deallocate(self, *tensors):
+        for t in tensors:
+            t.deallocate()
+        return self
+
+    def _labeled(self, lt: LabeledTensor, ids: dict):
+        return _to_c_labeled(lt, ids, self._keep)
+
+    def __call__(self, spec: _OpSpec, opstr: str = "", hw=ExecutionHW.DEFAULT):
+        ids: dict = {}
+        lhs = self._labeled(spec.lhs, ids)
+        rhs = spec.rhs
+        if isinstance(rhs, (int, float)):
+            call("tb_sched_set", self.h, lhs, spec.sign * float(rhs), int(spec.is_assign))
+            return self
+        if isinstance(rhs, LabeledTensor):
+            rhs = _Product(1.0, [rhs])
+        if not isinstance(rhs, _Product):
+            raise TypeError("right-hand side must be a scalar, a labelled tensor or a product")
+        alpha = spec.sign * rhs.alpha
+        if len(rhs.factors) == 1:
+            a = self._labeled(rhs.factors[0], ids)
+            call("tb_sched_add", self.h, lhs, alpha, a, int(spec.is_assign))
+        elif len(rhs.factors) == 2:
+            a = self._labeled(rhs.factors[0], ids)
+            b = self._labeled(rhs.factors[1], ids)
+            call("tb_sched_mult", self.h, lhs, alpha, a, b, int(spec.is_assign))
+        else:
+            raise ValueError("a TAMM op has at most two tensor factors")
+        return self
+
+    def execute(self, hw=ExecutionHW.DEFAULT, profile=False):
+        call("tb_sched_execute", self.h, int(hw), int(bool(profile)))
+        return self
+
+    def profile(self):
+        n = C.c_int64()
+        call("tb_sched_profile", self.h, C.byref(n), None, None, 0)
+        ms = np.zeros(max(n.value, 1))
+        fl = np.zeros(max(n.value, 1))
+        call("tb_sched_profile", self.h, C.byref(n), ms.ctypes.data_as(A.dp), fl.ctypes.data_as(A.dp), n.value)
+        return ms[:n.value], fl[:n.value]
+
+    def __del__(self):
+        try:
+            A.lib().tb_sched_destroy(self.h)
+        except Exception:
+            pass
