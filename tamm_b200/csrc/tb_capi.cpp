@@ -456,7 +456,7 @@ int tb_tensor_allocate(tb_tensor t, tb_ctx ctx) {
   if(t->p->data != nullptr) fail(TB_ERR_STATE, "tensor already allocated");
   TB_CUDA(cudaSetDevice(ctx->p->device));
   t->p->data = static_cast<double*>(ctx->p->arena->allocate(sizeof(double) * std::max<int64_t>(t->p->nelems, 1)));
-  t->p->ctx  = ctx->p.get();
+  t->p->ctx  = ctx->p;
   TB_API_END
 }
 
@@ -465,7 +465,7 @@ int tb_tensor_deallocate(tb_tensor t) {
   REQUIRE_ARG(t != nullptr);
   if(t->p->data && t->p->ctx) t->p->ctx->arena->deallocate(t->p->data);
   t->p->data = nullptr;
-  t->p->ctx  = nullptr;
+  t->p->ctx.reset();
   TB_API_END
 }
 
@@ -628,7 +628,7 @@ int tb_sched_create(tb_ctx ctx, tb_sched* out) {
   REQUIRE_ARG(ctx != nullptr && out != nullptr);
   auto* h   = new tb_sched_s();
   h->p      = std::make_unique<Sched>();
-  h->p->ctx = ctx->p.get();
+  h->p->ctx = ctx->p;
   *out      = h;
   TB_API_END
 }

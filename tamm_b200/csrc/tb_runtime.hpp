@@ -88,7 +88,7 @@ struct Tensor {
   std::vector<int64_t>              key_stride;
   std::vector<int64_t>              keys, offsets; // admitted blocks, key order
   int64_t                           nelems = 0;
-  Ctx*                              ctx    = nullptr;
+  std::shared_ptr<Ctx>              ctx;
   double*                           data   = nullptr;
 
   void    build_table(); // Distribution_NW (distribution.hpp:201-243)
@@ -126,7 +126,7 @@ struct Op {
 };
 
 struct Sched {
-  Ctx*                                              ctx = nullptr;
+  std::shared_ptr<Ctx>                              ctx;
   std::vector<Op>                                   ops;
   size_t                                            start = 0;
   std::vector<double>                               prof_ms, prof_flops;
@@ -147,7 +147,7 @@ struct Scratch {
 } // namespace tb
 
 struct tb_ctx_s {
-  std::unique_ptr<tb::Ctx> p;
+  std::shared_ptr<tb::Ctx> p;
 };
 struct tb_is_s {
   std::shared_ptr<tb::IndexSpace> p;

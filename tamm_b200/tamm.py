@@ -176,6 +176,16 @@ class TiledIndexSpace:
     def num_tiles(self):
         return len(self.tile_sizes)
 
+    @property
+    def tile_offsets(self):
+        """Index-space offset of the first index of each tile."""
+        root = self
+        while root.parent is not None:
+            root = root.parent
+        starts = np.zeros(root.num_tiles + 1, dtype=np.int64)
+        starts[1:] = np.cumsum(root.tile_sizes)
+        return starts[self.root_tiles]
+
     def tile_size(self, i):
         return int(self.tile_sizes[i])
 

@@ -54,15 +54,12 @@ def mo_tiled(oa: int, va: int, occ_tiles: list, virt_tiles: list) -> TiledIndexS
 
 def fill_blocks(t: Tensor, fn) -> np.ndarray:
     """Packed host buffer of t: fn(blockid, dims, index ranges per mode) -> block array,
-    called for every admitted block in storage order."""
+    called for every admitted block in storage order.  Ranges are absolute positions
+    in the root index space (e.g. MO orbital indices)."""
     keys, offs = t.block_table()
     out = np.empty(max(t.nelems, 1), dtype=np.float64)
     nts = [s.num_tiles for s in t.spaces]
-    starts = []
-    for s in t.spaces:
-        st = np.zeros(s.num_tiles + 1, dtype=np.int64)
-        st[1:] = np.cumsum(s.tile_sizes)
-        starts.append(st)
+    starts = [s.tile_offsets for s in t.spaces]
     for key, off in zip(keys, offs):
         bid, k = [], int(key)
         for n in reversed(nts):
