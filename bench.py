@@ -213,95 +213,134 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     import tamm_b200 as tb
+    from tamm_b200 import _capi as A
     from tamm_b200 import workloads as W
 
-    mode_name = args.mode or "fp64"
-    mode = {"fp64": tb.Precision.FP64, "int8": tb.Precision.INT8, "bf16x3": tb.Precision.BF16X3}[mode_name]
+    headline = args.mode or "int8"
+    modes = {"fp64": tb.Precision.FP64, "int8": tb.Precision.INT8, "bf16x3": tb.Precision.BF16X3}
     ec = tb.ExecutionContext(local, int(150 * 2 ** 30))
     lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec)
     a, b, c, d, i, j = lad.labels
     stream = torch.cuda.ExternalStream(ec.stream)
-    ec.set_precision(mode)
 
-    def step():
-        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(tb.ExecutionHW.GPU)
+    def step(profile=False):
+        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(
+            tb.ExecutionHW.GPU, profile)
+
+    def reset():
+        lad.sch(lad.r2().assign(0.0)).execute()
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        step()
-    barrier()
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+    # plain FP64 path: reference result + throughput
+    ec.set_precision(tb.Precision.FP64)
+    reset()
+    step()
+    r2_fp64 = lad.r2.read().copy()
+    fp64_ms = timed(step, max(1, min(args.steps, 3))) if headline != "fp64" else None
+
+    # headline mode: accuracy against the FP64 path, then the timed steps
+    ec.set_precision(modes[headline], 1e-11)
+    reset()
+    step()
+    r2_h = lad.r2.read()
+    scale = float(np.max(np.abs(r2_fp64)))
+    max_rel_err = float(np.max(np.abs(r2_h - r2_fp64)) / scale) if headline != "fp64" else 0.0
     clk = ClockSampler(local)
     clk.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    barrier()
+    ms = timed(step, args.steps)
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    if fp64_ms is None:
+        fp64_ms = ms
     value = world * lad.flops / (ms * 1e-3) / 1e12
 
-    # e2e: t2 from pinned host memory in, r2 read back, same public API
+    # e2e through the public API: t2 in from pinned host memory, r2 read back
     t2_pin = torch.from_numpy(lad.t2_host).pin_memory()
     r2_pin = torch.empty(lad.r2.nelems, dtype=torch.float64).pin_memory()
-    import ctypes as C
-    from tamm_b200 import _capi as A
 
     def e2e_step():
         A.call("tb_tensor_write", lad.t2.h, C.cast(t2_pin.data_ptr(), A.dp), lad.t2.nelems)
         step()
         A.call("tb_tensor_read", lad.r2.h, C.cast(r2_pin.data_ptr(), A.dp), lad.r2.nelems)
 
-    e2e_step()
-    barrier()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, min(args.steps, 3))
-    f0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    f1.record(stream)
-    barrier()
-    e2e_ms = f0.elapsed_time(f1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = timed(e2e_step, max(1, min(args.steps, 3)))
     e2e_val = world * lad.flops / (e2e_ms * 1e-3) / 1e12
 
-    # roofline of the dominant kernel: the grouped contraction is the whole step
-    lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(tb.ExecutionHW.GPU, profile=True)
-    kms, kfl = lad.sch.profile()
-    peak_kind = "fp64" if mode_name == "fp64" else ("int8" if mode_name == "int8" else "fp64")
-    peak = measured_peak(torch, peak_kind)
-    achieved = lad.flops / (float(kms[-1]) * 1e-3) / 1e12
-    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None,
-            "peak_source": f"measured live: cuBLAS {'DGEMM' if peak_kind == 'fp64' else 'INT8 GEMM'} 8192^3 "
-                           "on this GPU (no FP64/INT8 figure in MEASURED_PEAKS.json)"}
+    # roofline of the dominant kernel from a profiled step (CUDA events on the stream)
+    step(profile=True)
+    st = lad.sch.op_stats(-1)
+    peaks = load_peaks()
+    if headline == "int8":
+        S = st["slices_max"]
+        peak = measured_peak(torch, "int8")
+        achieved = st["int8_ops"] / (st["gemm_ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": f"k_contract_i8<S={S}> (tcgen05 kind::i8)",
+                "ops": "INT8 tensor ops (2 per multiply-add) incl. padding to 128x80x32 tiles",
+                "peak_source": "measured live: cuBLASLt INT8 GEMM (torch._int_mm) 8192^3 on this GPU; "
+                               "MEASURED_PEAKS.json has no INT8 figure",
+                "gemm_ms": st["gemm_ms"], "split_ms": st["split_ms"]}
+        # the split pass is HBM-bound: FP64 read + S digit bytes written per operand element
+        nsplit = lad.v.nelems + lad.t2.nelems
+        split_bytes = nsplit * (8 + S) + 0.0
+        hbm = peaks.get("hbm_gbs")
+        roof["split"] = {"bound": "hbm", "achieved": split_bytes / (st["split_ms"] * 1e-3) / 1e9,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": (split_bytes / (st["split_ms"] * 1e-3) / 1e9 / hbm) if hbm else None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+    else:
+        peak = measured_peak(torch, "fp64")
+        achieved = lad.flops / (st["gemm_ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_contract_fp64 (DMMA m8n8k4)",
+                "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU; "
+                               "MEASURED_PEAKS.json has no FP64 figure"}
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -309,18 +348,23 @@ def main():
         if not args.no_cpu_baseline and world == 1:
             cpu = cpu_baseline_sample(ladder_triples(args.oa, args.va, args.seed), args.cpu_seconds,
                                       os.cpu_count() or 1)
-        bytes_step = 8 * lad.t2.nelems
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if mode_name == "fp64" else mode_name,
-            "data": "synthetic",
-            "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}", "mode": mode_name,
-                       "admitted_flops": lad.flops, "l2": "inputs larger than L2 (v = "
-                       f"{8*lad.v.nelems/1e9:.1f} GB)", "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_step,
+            "vs_baseline": None, "dtype": {"fp64": "f64", "int8": "s8/u8 digits, s32 accumulate, f64 recombination",
+                                           "bf16x3": "bf16x3"}[headline],
+            "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}", "mode": headline,
+                       "contraction": "r2(a,b,i,j) += v(a,b,c,d) * t2(c,d,i,j), spin-blocked, virt tiles U{24..48}",
+                       "admitted_flops": lad.flops, "slices": st.get("slices_max"),
+                       "l2": f"inputs larger than L2 (v = {8*lad.v.nelems/1e9:.1f} GB), no flush",
+                       "parallelism": f"replicas x{world}"},
+            "fp64_path": {"value": world * lad.flops / (fp64_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": fp64_ms},
+            "speedup_vs_fp64_path": fp64_ms / ms,
+            "max_rel_err_vs_fp64": max_rel_err,
+            "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * lad.t2.nelems,
                     "d2h_bytes_per_step": 8 * lad.r2.nelems, "ms_per_step": e2e_ms},
-            "gpu_launches": int(args.steps * 1),
+            "gpu_launches": args.steps * (3 if headline == "int8" else 1),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -133,6 +133,8 @@ typedef struct tb_stats {
   int    slices_min;      /* slice counts chosen (TB_MODE_INT8) */
   int    slices_max;
   int64_t scratch_bytes;  /* scratch used by the split operands */
+  double split_ms;        /* device time of the operand splitting (profiled runs) */
+  double gemm_ms;         /* device time of the tensor-core contraction kernel (profiled runs) */
 } tb_stats;
 
 /* C += alpha * sum over tasks of A * B, all groups, one stream-ordered pass.
@@ -244,6 +246,8 @@ int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, i
 int tb_sched_execute(tb_sched s, int hw, int profile);
 /* Number of ops in the last execute; per op: device milliseconds and FP64 FLOPs. */
 int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64_t cap);
+/* Kernel statistics of op `index` of the last profiled execute (zeros for Set/Add ops). */
+int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out);
 /* Drops queued ops without running them. */
 int tb_sched_clear(tb_sched s);
 

@@ -34,7 +34,8 @@ h = C.c_void_p  # opaque handles
 
 class tb_stats(C.Structure):
     _fields_ = [("flops", C.c_double), ("int8_ops", C.c_double), ("slices_min", C.c_int),
-                ("slices_max", C.c_int), ("scratch_bytes", C.c_int64)]
+                ("slices_max", C.c_int), ("scratch_bytes", C.c_int64), ("split_ms", C.c_double),
+                ("gemm_ms", C.c_double)]
 
 
 class tb_labeled(C.Structure):
@@ -103,6 +104,7 @@ PROTOS = {
     "tb_sched_execute": [h, C.c_int, C.c_int],
     "tb_sched_profile": [h, i64p, dp, dp, C.c_int64],
     "tb_sched_clear": [h],
+    "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
 }
 
 _lib = None

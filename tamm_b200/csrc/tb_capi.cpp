@@ -19,14 +19,30 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
                   double* C, cudaStream_t stream, Arena* arena) {
   plan.last       = tb_stats{};
   plan.last.flops = wl.flops;
+  plan.arena      = arena;
   if(wl.tasks.empty()) return;
   switch(plan.mode) {
-    case TB_MODE_FP64: launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream); break;
+    case TB_MODE_FP64:
+      if(plan.profile) {
+        cudaEvent_t e0, e1;
+        TB_CUDA(cudaEventCreate(&e0));
+        TB_CUDA(cudaEventCreate(&e1));
+        TB_CUDA(cudaEventRecord(e0, stream));
+        launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+        TB_CUDA(cudaEventRecord(e1, stream));
+        TB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        plan.last.gemm_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+      }
+      else launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+      break;
     case TB_MODE_INT8: contract_int8(plan, wl, alpha, A, B, C, stream); break;
     case TB_MODE_BF16X3: contract_bf16x3(plan, wl, alpha, A, B, C, stream); break;
     default: fail(TB_ERR_INVALID, "unknown precision mode");
   }
-  (void) arena;
 }
 } // namespace tb
 
@@ -723,6 +739,15 @@ int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64
     if(ms) ms[i] = s->p->prof_ms[i];
     if(flops) flops[i] = s->p->prof_flops[i];
   }
+  TB_API_END
+}
+
+int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && out != nullptr);
+  TB_EXPECTS(index >= 0 && index < (int64_t) s->p->prof_stats.size(),
+             "op index out of range (profile the execute first)");
+  *out = s->p->prof_stats[index];
   TB_API_END
 }
 

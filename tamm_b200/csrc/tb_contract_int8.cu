@@ -1,15 +1,646 @@
-// Split-INT8 (Ozaki-style) contraction on the tcgen05 INT8 tensor cores.
+// Split-INT8 (Ozaki-style) block contraction on the tcgen05 INT8 tensor cores.
+//
+// Every operand block of a contraction is viewed as its GEMM matrix (A: M x K with
+// the A-outer labels as rows, B: N x K with the B-outer labels as rows, K = the inner
+// labels in A's order — the Ainter / Binter views of kernels::block_multiply,
+// multiply.hpp:304-330, without materialising them in FP64).  Each row is scaled by
+// a power of two 2^-e (e = exponent of the row's max |x|, per block) and cut into S
+// base-256 digits of the two's-complement integer X = trunc(x * 2^(8S-1-e)):
+//     X = d_0 * 256^(S-1) + d_1 * 256^(S-2) + ... + d_(S-1),
+// d_0 signed (s8), d_1.. unsigned (u8).  A * B is then the sum over digit pairs of
+// exact INT8 x INT8 -> INT32 tensor-core products; pairs (i, j) with equal i + j share
+// one power of two, so the S(S+1)/2 products with i + j <= S - 1 accumulate into S
+// INT32 TMEM accumulators ("diagonals").  After each (A block, B block) task the
+// diagonals are recombined in FP64, rescaled by 2^(e_row + e_col - 14 - 8d) and added
+// to FP64 register accumulators; the output block is written once, in C's own label
+// order, when the group's tasks are done.
+//
+// Truncation: each operand is exact to 2^-(8S-1) of its row maximum and the dropped
+// pairs (i + j >= S) weigh at most ~S * 2^(2-8S) of row-max x col-max x K, so
+// S = 6 (21 INT8 products) gives ~1e-13 relative accuracy on this scale.  This is the
+// error-free splitting of Ozaki, Ogita, Oishi and Rump with the INT8 tensor-core
+// digit layout of Ootomo / Ozaki / Uchino-Imamura style DGEMM emulation.
 #include "tb_internal.hpp"
+#include "tb_runtime.hpp"
+#include "tb_sm100.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
 
 namespace tb {
 
-void contract_int8(Plan&, const WorkList&, double, const double*, const double*, double*,
-                   cudaStream_t) {
-  fail(TB_ERR_NOT_IMPLEMENTED, "split-INT8 contraction is not built yet");
+void launch_contract_fp64(const Plan&, const WorkList&, double, double, int, const double*,
+                          const double*, double*, cudaStream_t);
+
+namespace {
+using namespace sm100;
+
+constexpr int MT = 128; // UMMA M: output rows of a tile
+constexpr int KC = 32;  // bytes of K per pipeline stage (one INT8 MMA k-step)
+constexpr int STAGES = 4;
+constexpr int NTHREADS = 192; // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
+
+// One operand block to split into digit slices.
+struct SplitBlock {
+  int64_t src_off; // element offset in the FP64 arena
+  int64_t dst_off; // byte offset of the block's slices in the scratch
+  int32_t exp_off; // first exponent (int32 per padded row)
+  int32_t rows, K, rows_pad, K_pad, tile_rows;
+  int32_t nr, nk;
+  int32_t rdim[kMaxClass], rstr[kMaxClass];
+  int32_t kdim[kMaxClass], kstr[kMaxClass];
+};
+
+struct I8Task {
+  int64_t a_off, b_off; // byte offsets of the A / B block slices
+  int32_t a_exp, b_exp; // exponent index bases
+  int32_t nkc;          // K_pad / KC
+  int32_t pad;
+};
+
+struct I8Item {
+  int32_t group, mt, nt, pad;
+};
+
+__device__ __forceinline__ int32_t decomp(int32_t x, int n, const int32_t* dims, const int32_t* str) {
+  int32_t off = 0;
+  for(int j = n - 1; j >= 0; j--) {
+    const int32_t d = dims[j], q = x / d;
+    off += (x - q * d) * str[j];
+    x = q;
+  }
+  return off;
 }
 
-void contract_bf16x3(Plan&, const WorkList&, double, const double*, const double*, double*,
-                     cudaStream_t) {
+// Byte position of (row r, k) inside one K chunk of one digit slice of a row tile of
+// `tile_rows` rows: UMMA canonical K-major layout without swizzle (8 x 16-byte core
+// matrices; the two 16-byte K halves tile_rows * 16 bytes apart; 8-row groups 128
+// bytes apart).
+__device__ __forceinline__ int32_t canon_off(int r, int kk, int tile_rows) {
+  return (kk >> 4) * (tile_rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kk & 15);
+}
+
+// One warp per (block, row): row max -> exponent, then the S digit slices of the row
+// (zero for padding rows / columns).  chunk table: (block, first row) per 8 rows.
+template<int S>
+__global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ blocks,
+                                               const int2* __restrict__ chunks, int nchunks,
+                                               const double* __restrict__ src,
+                                               uint8_t* __restrict__ dst, int32_t* __restrict__ exps) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int2       ch  = chunks[c];
+    const SplitBlock b   = blocks[ch.x];
+    const int        row = ch.y + warp;
+    if(row >= b.rows_pad) continue;
+    const bool    live   = row < b.rows;
+    const int32_t rowoff = live ? decomp(row, b.nr, b.rdim, b.rstr) : 0;
+    const double* s      = src + b.src_off + rowoff;
+    double        mx     = 0.0;
+    if(live)
+      for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + decomp(k, b.nk, b.kdim, b.kstr))));
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int e = 0;
+    if(mx > 0.0) frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1): |x| < 2^e
+    const int    sh    = 8 * S - 1 - e;
+    const int    tile = row / b.tile_rows, r = row - tile * b.tile_rows;
+    const int    nkc  = b.K_pad / KC;
+    uint8_t*     out  = dst + b.dst_off + (int64_t) tile * nkc * S * b.tile_rows * KC;
+    for(int k = lane; k < b.K_pad; k += 32) {
+      long long X = 0;
+      if(live && k < b.K) X = __double2ll_rz(ldexp(__ldg(s + decomp(k, b.nk, b.kdim, b.kstr)), sh));
+      const int kc = k / KC, kk = k - kc * KC;
+      uint8_t*  o  = out + (int64_t) kc * S * b.tile_rows * KC + canon_off(r, kk, b.tile_rows);
+#pragma unroll
+      for(int i = 0; i < S; i++) {
+        const int ds = 8 * (S - 1 - i);
+        o[(int64_t) i * b.tile_rows * KC] = (uint8_t) ((X >> ds) & 0xFF); // d_0 keeps the sign bits
+      }
+    }
+    if(lane == 0) exps[b.exp_off + row] = e;
+  }
+}
+
+struct I8Params {
+  const uint8_t*  slices;
+  const int32_t*  exps;
+  const I8Task*   tasks;
+  const DevGroup* groups;
+  const I8Item*   items;
+  int             nitems;
+  double*         C;
+  double          alpha;
+  LabelClasses    lc;
+  int*            err;
+};
+
+template<int S, int NT>
+constexpr uint32_t stage_bytes() {
+  return (uint32_t) S * (MT + NT) * KC;
+}
+
+template<int S, int NT>
+constexpr size_t smem_bytes() {
+  return (size_t) STAGES * stage_bytes<S, NT>() + 1024;
+}
+
+template<int S, int NT>
+__global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
+  static_assert(S * NT <= 512, "TMEM holds 512 columns");
+  extern __shared__ __align__(1024) uint8_t smem[];
+  constexpr uint32_t A_BYTES = S * MT * KC, B_BYTES = S * NT * KC, STAGE = A_BYTES + B_BYTES;
+  uint64_t*          full   = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE);
+  uint64_t*          empty  = full + STAGES;
+  uint64_t*          tfull  = empty + STAGES;
+  uint64_t*          tempty = tfull + 1;
+  uint32_t*          tslot  = reinterpret_cast<uint32_t*>(tempty + 1);
+  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if(threadIdx.x == 0) {
+    for(int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, 128);
+    fence_mbarrier_init();
+  }
+  if(warp == 1) tmem_alloc(tslot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if(warp == 0) {
+    // ---------------- producer: one bulk copy of all S digit slices per operand ----
+    if(elect_one()) {
+      int      stage = 0;
+      uint32_t phase = 0;
+      for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+        const I8Item   item = p.items[it];
+        const DevGroup g    = p.groups[item.group];
+        for(int t = g.task_begin; t < g.task_end; t++) {
+          const I8Task   tk = p.tasks[t];
+          const uint8_t* ga = p.slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
+          const uint8_t* gb = p.slices + tk.b_off + (int64_t) item.nt * tk.nkc * B_BYTES;
+          for(int kc = 0; kc < tk.nkc; kc++) {
+            if(!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) goto done_producer;
+            mbar_arrive_expect_tx(&full[stage], STAGE);
+            bulk_g2s(smem + stage * STAGE, ga + (int64_t) kc * A_BYTES, A_BYTES, &full[stage]);
+            bulk_g2s(smem + stage * STAGE + A_BYTES, gb + (int64_t) kc * B_BYTES, B_BYTES, &full[stage]);
+            if(++stage == STAGES) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+      }
+    done_producer:;
+    }
+  }
+  else if(warp == 1) {
+    // ---------------- MMA issuer: S(S+1)/2 digit products per K step --------------
+    if(elect_one()) {
+      int      stage = 0;
+      uint32_t phase = 0, tphase = 0;
+      for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+        const I8Item   item = p.items[it];
+        const DevGroup g    = p.groups[item.group];
+        for(int t = g.task_begin; t < g.task_end; t++) {
+          const int nkc = p.tasks[t].nkc;
+          if(!mbar_wait(tempty, tphase ^ 1, p.err, 2)) goto done_mma;
+          tc_fence_after();
+          for(int kc = 0; kc < nkc; kc++) {
+            if(!mbar_wait(&full[stage], phase, p.err, 3)) goto done_mma;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(smem + stage * STAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+            for(int d = 0; d < S; d++) {
+#pragma unroll
+              for(int i = 0; i <= d; i++) {
+                const int      j  = d - i;
+                const uint64_t ad = umma_desc_kmajor(a0 + i * MT * KC, MT * 16, 128);
+                const uint64_t bd = umma_desc_kmajor(b0 + j * NT * KC, NT * 16, 128);
+                mma_i8(tmem + d * NT, ad, bd, idesc_i8(MT, NT, i == 0, j == 0), kc > 0 || i > 0);
+              }
+            }
+            umma_commit(&empty[stage]); // stage free once these MMAs have read it
+            if(++stage == STAGES) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+          umma_commit(tfull); // the task's diagonals are complete
+          tphase ^= 1;
+        }
+      }
+    done_mma:;
+    }
+  }
+  else {
+    // ---------------- epilogue: FP64 recombination of the diagonals ----------------
+    const int q = warp & 3, row = q * 32 + lane;
+    uint32_t  tphase = 0;
+    double    racc[NT];
+    for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+      const I8Item   item = p.items[it];
+      const DevGroup g    = p.groups[item.group];
+#pragma unroll
+      for(int x = 0; x < NT; x++) racc[x] = 0.0;
+      bool ok = true;
+      for(int t = g.task_begin; t < g.task_end; t++) {
+        if(!mbar_wait(tfull, tphase, p.err, 4)) {
+          ok = false;
+          break;
+        }
+        tphase ^= 1;
+        tc_fence_after();
+        const I8Task tk = p.tasks[t];
+        const int    er = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
+        const double sr = ldexp(1.0, er - 7);
+#pragma unroll
+        for(int c0 = 0; c0 < NT; c0 += 16) {
+          double tacc[16];
+#pragma unroll
+          for(int x = 0; x < 16; x++) tacc[x] = 0.0;
+#pragma unroll
+          for(int d = 0; d < S; d++) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + d * NT + c0, v);
+            tmem_wait_ld();
+            const double w = pow2i(-8 * d);
+#pragma unroll
+            for(int x = 0; x < 16; x++) tacc[x] += (double) (int32_t) v[x] * w;
+          }
+          const int32_t* ec = p.exps + tk.b_exp + item.nt * NT + c0;
+#pragma unroll
+          for(int x = 0; x < 16; x++) racc[c0 + x] += tacc[x] * sr * ldexp(1.0, __ldg(ec + x) - 7);
+        }
+        tc_fence_before();
+        mbar_arrive(tempty);
+      }
+      if(!ok) break;
+      // C (+)= alpha * result, in C's own layout (transpose_output fused here)
+      int64_t cstr[kMaxModes];
+      {
+        int64_t s = 1;
+        for(int i = p.lc.nc - 1; i >= 0; i--) {
+          cstr[i] = s;
+          s *= g.cdims[i];
+        }
+      }
+      int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
+      int32_t M = 1, N = 1;
+      for(int j = 0; j < p.lc.nm; j++) {
+        mdim[j] = g.cdims[p.lc.m_c[j]];
+        mstr[j] = (int32_t) cstr[p.lc.m_c[j]];
+        M *= mdim[j];
+      }
+      for(int j = 0; j < p.lc.nn; j++) {
+        ndim[j] = g.cdims[p.lc.n_c[j]];
+        nstr[j] = (int32_t) cstr[p.lc.n_c[j]];
+        N *= ndim[j];
+      }
+      const int m = item.mt * MT + row;
+      if(m < M) {
+        double* crow = p.C + g.c_off + decomp(m, p.lc.nm, mdim, mstr);
+#pragma unroll
+        for(int x = 0; x < NT; x++) {
+          const int n = item.nt * NT + x;
+          if(n < N) {
+            double* cp = crow + decomp(n, p.lc.nn, ndim, nstr);
+            *cp += p.alpha * racc[x];
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if(warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// ---------------------------------------------------------------- host side
+
+struct I8Layout {
+  int                     S = 0, NT = 0;
+  std::vector<SplitBlock> a_blocks, b_blocks;
+  std::vector<int2>       a_chunks, b_chunks;
+  std::vector<I8Task>     tasks;
+  std::vector<I8Item>     items;
+  int64_t                 slice_bytes = 0, a_bytes = 0;
+  int64_t                 nexp = 0, a_nexp = 0;
+  double                  int8_ops = 0;
+  SplitBlock*             d_ablocks = nullptr;
+  SplitBlock*             d_bblocks = nullptr;
+  int2*                   d_achunks = nullptr;
+  int2*                   d_bchunks = nullptr;
+  I8Task*                 d_tasks   = nullptr;
+  I8Item*                 d_items   = nullptr;
+  int*                    d_err     = nullptr;
+  int                     device    = -1;
+  ~I8Layout() {
+    if(device >= 0) {
+      cudaSetDevice(device);
+      cudaFree(d_ablocks);
+      cudaFree(d_bblocks);
+      cudaFree(d_achunks);
+      cudaFree(d_bchunks);
+      cudaFree(d_tasks);
+      cudaFree(d_items);
+      cudaFree(d_err);
+    }
+  }
+};
+
+int nt_for(int S) { return S <= 6 ? 80 : 64; }
+
+int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S) {
+  auto L = std::make_shared<I8Layout>();
+  L->S   = S;
+  L->NT  = nt_for(S);
+  std::map<int64_t, int> amap, bmap;
+  int64_t                aexp = 0, bexp = 0, abytes = 0, bbytes = 0;
+  auto                   strides = [](const int32_t* dims, int n, int64_t* str) {
+    int64_t s = 1;
+    for(int i = n - 1; i >= 0; i--) {
+      str[i] = s;
+      s *= dims[i];
+    }
+  };
+  L->tasks.resize(wl.tasks.size());
+  for(const auto& g: wl.groups) {
+    for(int t = g.task_begin; t < g.task_end; t++) {
+      const DevTask& tk = wl.tasks[t];
+      int64_t        astr[kMaxModes], bstr[kMaxModes];
+      strides(tk.adims, lc.na, astr);
+      strides(tk.bdims, lc.nb, bstr);
+      int32_t K = 1;
+      for(int j = 0; j < lc.nk; j++) K *= tk.adims[lc.k_a[j]];
+      auto ia = amap.find(tk.a_off);
+      if(ia == amap.end()) {
+        SplitBlock b{};
+        b.src_off = tk.a_off;
+        b.nr      = lc.nm;
+        b.nk      = lc.nk;
+        b.rows    = 1;
+        for(int j = 0; j < lc.nm; j++) {
+          b.rdim[j] = tk.adims[lc.m_a[j]];
+          b.rstr[j] = (int32_t) astr[lc.m_a[j]];
+          b.rows *= b.rdim[j];
+        }
+        for(int j = 0; j < lc.nk; j++) {
+          b.kdim[j] = tk.adims[lc.k_a[j]];
+          b.kstr[j] = (int32_t) astr[lc.k_a[j]];
+        }
+        b.K         = K;
+        b.tile_rows = MT;
+        b.rows_pad  = (int32_t) rup(b.rows, MT);
+        b.K_pad     = (int32_t) rup(K, KC);
+        b.dst_off   = abytes;
+        b.exp_off   = (int32_t) aexp;
+        abytes += (int64_t) b.rows_pad * b.K_pad * S;
+        aexp += b.rows_pad;
+        ia = amap.emplace(tk.a_off, (int) L->a_blocks.size()).first;
+        L->a_blocks.push_back(b);
+      }
+      auto ib = bmap.find(tk.b_off);
+      if(ib == bmap.end()) {
+        SplitBlock b{};
+        b.src_off = tk.b_off;
+        b.nr      = lc.nn;
+        b.nk      = lc.nk;
+        b.rows    = 1;
+        for(int j = 0; j < lc.nn; j++) {
+          b.rdim[j] = tk.bdims[lc.n_b[j]];
+          b.rstr[j] = (int32_t) bstr[lc.n_b[j]];
+          b.rows *= b.rdim[j];
+        }
+        for(int j = 0; j < lc.nk; j++) {
+          b.kdim[j] = tk.bdims[lc.k_b[j]];
+          b.kstr[j] = (int32_t) bstr[lc.k_b[j]];
+        }
+        b.K         = K;
+        b.tile_rows = L->NT;
+        b.rows_pad  = (int32_t) rup(b.rows, L->NT);
+        b.K_pad     = (int32_t) rup(K, KC);
+        b.dst_off   = bbytes;
+        b.exp_off   = (int32_t) bexp;
+        bbytes += (int64_t) b.rows_pad * b.K_pad * S;
+        bexp += b.rows_pad;
+        ib = bmap.emplace(tk.b_off, (int) L->b_blocks.size()).first;
+        L->b_blocks.push_back(b);
+      }
+      const SplitBlock& A = L->a_blocks[ia->second];
+      const SplitBlock& B = L->b_blocks[ib->second];
+      I8Task            it{};
+      it.a_off     = A.dst_off;
+      it.b_off     = B.dst_off; // rebased below
+      it.a_exp     = A.exp_off;
+      it.b_exp     = B.exp_off;
+      it.nkc       = A.K_pad / KC;
+      L->tasks[t]  = it;
+    }
+  }
+  TB_EXPECTS(aexp + bexp < (1ll << 31), "too many split rows");
+  for(auto& b: L->b_blocks) {
+    b.dst_off += abytes;
+    b.exp_off += (int32_t) aexp;
+  }
+  for(auto& t: L->tasks) {
+    t.b_off += abytes;
+    t.b_exp += (int32_t) aexp;
+  }
+  L->a_bytes     = abytes;
+  L->slice_bytes = abytes + bbytes;
+  L->a_nexp      = aexp;
+  L->nexp        = aexp + bexp;
+  auto chunks    = [](const std::vector<SplitBlock>& bl, std::vector<int2>& out) {
+    for(size_t i = 0; i < bl.size(); i++)
+      for(int r = 0; r < bl[i].rows_pad; r += 8) out.push_back(make_int2((int) i, r));
+  };
+  chunks(L->a_blocks, L->a_chunks);
+  chunks(L->b_blocks, L->b_chunks);
+  // output tiles, longest first
+  std::vector<std::pair<int64_t, I8Item>> v;
+  for(size_t gi = 0; gi < wl.groups.size(); gi++) {
+    const DevGroup& g = wl.groups[gi];
+    if(g.task_begin == g.task_end) continue;
+    int64_t M = 1, N = 1, work = 0;
+    for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
+    for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
+    for(int t = g.task_begin; t < g.task_end; t++) work += L->tasks[t].nkc;
+    for(int64_t mt = 0; mt < (M + MT - 1) / MT; mt++)
+      for(int64_t nt = 0; nt < (N + L->NT - 1) / L->NT; nt++) {
+        v.push_back({work, I8Item{(int32_t) gi, (int32_t) mt, (int32_t) nt, 0}});
+        L->int8_ops += 2.0 * MT * L->NT * KC * work * (S * (S + 1) / 2);
+      }
+  }
+  std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  for(auto& x: v) L->items.push_back(x.second);
+  TB_CUDA(cudaGetDevice(&L->device));
+  auto up = [](auto*& dptr, const auto& vec) {
+    using T = std::remove_reference_t<decltype(vec[0])>;
+    if(vec.empty()) return;
+    TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&dptr), sizeof(T) * vec.size()));
+    TB_CUDA(cudaMemcpy(dptr, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice));
+  };
+  up(L->d_ablocks, L->a_blocks);
+  up(L->d_bblocks, L->b_blocks);
+  up(L->d_achunks, L->a_chunks);
+  up(L->d_bchunks, L->b_chunks);
+  up(L->d_tasks, L->tasks);
+  up(L->d_items, L->items);
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_err), sizeof(int)));
+  TB_CUDA(cudaMemset(L->d_err, 0, sizeof(int)));
+  return L;
+}
+
+int sm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+template<int S>
+void launch_split(const I8Layout& L, const double* A, const double* B, uint8_t* slices, int32_t* exps,
+                  cudaStream_t st) {
+  const int grid_cap = sm_count() * 8;
+  if(!L.a_chunks.empty())
+    k_split<S><<<std::min<int64_t>((int64_t) L.a_chunks.size(), grid_cap), 256, 0, st>>>(
+      L.d_ablocks, L.d_achunks, (int) L.a_chunks.size(), A, slices, exps);
+  if(!L.b_chunks.empty())
+    k_split<S><<<std::min<int64_t>((int64_t) L.b_chunks.size(), grid_cap), 256, 0, st>>>(
+      L.d_bblocks, L.d_bchunks, (int) L.b_chunks.size(), B, slices, exps);
+  TB_CUDA(cudaGetLastError());
+}
+
+template<int S, int NT>
+void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha,
+                 const uint8_t* slices, const int32_t* exps, double* C, cudaStream_t st) {
+  if(L.items.empty()) return;
+  I8Params p;
+  p.slices = slices;
+  p.exps   = exps;
+  p.tasks  = L.d_tasks;
+  p.groups = wl.d_groups;
+  p.items  = L.d_items;
+  p.nitems = (int) L.items.size();
+  p.C      = C;
+  p.alpha  = alpha;
+  p.lc     = lc;
+  p.err    = L.d_err;
+  const size_t smem = smem_bytes<S, NT>();
+  static bool  configured[64] = {false};
+  int          dev            = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  if(dev < 64 && !configured[dev]) {
+    TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    configured[dev] = true;
+  }
+  const int grid = (int) std::min<int64_t>((int64_t) L.items.size(), sm_count());
+  k_contract_i8<S, NT><<<grid, NTHREADS, smem, st>>>(p);
+  TB_CUDA(cudaGetLastError());
+}
+
+template<int S>
+void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha, const double* A,
+           const double* B, double* C, uint8_t* slices, int32_t* exps, cudaStream_t st,
+           cudaEvent_t* ev) {
+  if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
+  launch_split<S>(L, A, B, slices, exps, st);
+  if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
+  launch_gemm<S, (S <= 6 ? 80 : 64)>(L, wl, lc, alpha, slices, exps, C, st);
+  if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
+}
+
+// slice count for an error target: smallest S with S * 2^(2 - 8S) * 16 <= target
+int slices_for(double err_target) {
+  for(int S = 3; S <= 8; S++)
+    if(S * std::ldexp(1.0, 2 - 8 * S) * 16.0 <= err_target) return S;
+  return 8;
+}
+
+std::map<const WorkList*, std::shared_ptr<I8Layout>> g_layouts; // per work list, keyed by S below
+
+} // namespace
+
+void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
+                   double* C, cudaStream_t stream) {
+  const LabelClasses& lc = plan.lc;
+  if(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0) {
+    // Hadamard / one-sided reduction labels and outer products run on the FP64 path.
+    launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+    return;
+  }
+  const int S = plan.nslices > 0 ? std::min(std::max(plan.nslices, 3), 8) : slices_for(plan.err_target);
+  auto&     L = g_layouts[&wl];
+  if(!L || L->S != S) L = build_layout(lc, wl, S);
+  Scratch sc;
+  sc.stream = stream;
+  sc.arena  = plan.arena;
+  auto* slices = static_cast<uint8_t*>(sc.get(L->slice_bytes));
+  auto* exps   = static_cast<int32_t*>(sc.get(sizeof(int32_t) * std::max<int64_t>(L->nexp, 1)));
+  cudaEvent_t  evs[3];
+  cudaEvent_t* ev = nullptr;
+  if(plan.profile) {
+    for(auto& e: evs) TB_CUDA(cudaEventCreate(&e));
+    ev = evs;
+  }
+  switch(S) {
+    case 3: run_s<3>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    case 4: run_s<4>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    case 5: run_s<5>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    case 6: run_s<6>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    case 7: run_s<7>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    default: run_s<8>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+  }
+  sc.put(exps);
+  sc.put(slices);
+  if(ev) {
+    float a = 0, b = 0;
+    TB_CUDA(cudaEventSynchronize(evs[2]));
+    TB_CUDA(cudaEventElapsedTime(&a, evs[0], evs[1]));
+    TB_CUDA(cudaEventElapsedTime(&b, evs[1], evs[2]));
+    plan.last.split_ms = a;
+    plan.last.gemm_ms  = b;
+    for(auto& e: evs) cudaEventDestroy(e);
+  }
+  plan.last.int8_ops      = L->int8_ops;
+  plan.last.slices_min    = S;
+  plan.last.slices_max    = S;
+  plan.last.scratch_bytes = L->slice_bytes + 4 * L->nexp;
+  if(plan.check_errors) {
+    int h = 0;
+    TB_CUDA(cudaMemcpyAsync(&h, L->d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    TB_CUDA(cudaStreamSynchronize(stream));
+    if(h != 0) {
+      cudaMemsetAsync(L->d_err, 0, sizeof(int), stream);
+      fail(TB_ERR_TIMEOUT, "split-INT8 contraction: a device-side wait gave up (code " + std::to_string(h) + ")");
+    }
+  }
+}
+
+void forget_int8_layout(const WorkList* wl) { g_layouts.erase(wl); }
+
+void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
+                     double* C, cudaStream_t stream) {
+  (void) plan;
+  (void) wl;
+  (void) alpha;
+  (void) A;
+  (void) B;
+  (void) C;
+  (void) stream;
   fail(TB_ERR_NOT_IMPLEMENTED, "BF16x3 contraction is not built yet");
 }
 

@@ -89,13 +89,20 @@ struct WorkList {
   ~WorkList();
 };
 
+class Arena;
+
 struct Plan {
   LabelClasses lc;
   int          mode       = TB_MODE_FP64;
   double       err_target = 1e-11;
   int          nslices    = 0;
   tb_stats     last{};
+  Arena*       arena        = nullptr; // scratch source (null: cudaMallocAsync)
+  bool         check_errors = true;    // read the device error word after a launch
+  bool         profile      = false;   // time the phases with CUDA events (synchronises)
 };
+
+void forget_int8_layout(const WorkList* wl);
 
 // ---- launchers (device code in *.cu) ----
 void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,

@@ -107,6 +107,7 @@ LabelClasses classify(const int* cl, int nc, const int* al, int na, const int* b
 }
 
 WorkList::~WorkList() {
+  forget_int8_layout(this);
   if(d_groups || d_tasks || d_items) {
     int cur = -1;
     cudaGetDevice(&cur);

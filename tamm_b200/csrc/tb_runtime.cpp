@@ -530,15 +530,19 @@ void Sched::run(Op& op) {
   op.plan->mode       = ctx->mode;
   op.plan->err_target = ctx->err_target;
   op.plan->nslices    = ctx->nslices;
+  op.plan->profile    = profiling;
   op.flops            = op.wl->flops;
   run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
                ctx->arena.get());
+  op.plan->profile = false;
 }
 
 void Sched::execute(bool profile) {
   TB_CUDA(cudaSetDevice(ctx->device));
   prof_ms.clear();
   prof_flops.clear();
+  prof_stats.clear();
+  profiling = profile;
   std::vector<cudaEvent_t> ev;
   if(profile) {
     ev.resize(2 * (ops.size() - start));
@@ -547,8 +551,12 @@ void Sched::execute(bool profile) {
   for(size_t i = start; i < ops.size(); i++) {
     if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start)], ctx->stream));
     run(ops[i]);
-    if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start) + 1], ctx->stream));
+    if(profile) {
+      TB_CUDA(cudaEventRecord(ev[2 * (i - start) + 1], ctx->stream));
+      prof_stats.push_back(ops[i].kind == Op::Mult && ops[i].plan ? ops[i].plan->last : tb_stats{});
+    }
   }
+  profiling = false;
   if(profile) {
     TB_CUDA(cudaStreamSynchronize(ctx->stream));
     for(size_t i = start; i < ops.size(); i++) {

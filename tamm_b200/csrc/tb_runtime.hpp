@@ -130,6 +130,8 @@ struct Sched {
   std::vector<Op>                                   ops;
   size_t                                            start = 0;
   std::vector<double>                               prof_ms, prof_flops;
+  std::vector<tb_stats>                             prof_stats;
+  bool                                              profiling = false;
   std::map<std::string, std::shared_ptr<Plan>>     plan_cache;
   std::map<std::string, std::shared_ptr<WorkList>> wl_cache;
   void                                              execute(bool profile);

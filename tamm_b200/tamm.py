@@ -455,6 +455,16 @@ class Scheduler:
         call("tb_sched_profile", self.h, C.byref(n), ms.ctypes.data_as(A.dp), fl.ctypes.data_as(A.dp), n.value)
         return ms[:n.value], fl[:n.value]
 
+    def op_stats(self, index=-1):
+        """Kernel statistics (dict) of one op of the last profiled execute."""
+        n = C.c_int64()
+        call("tb_sched_profile", self.h, C.byref(n), None, None, 0)
+        if index < 0:
+            index += n.value
+        st = A.tb_stats()
+        call("tb_sched_op_stats", self.h, int(index), C.byref(st))
+        return {k: getattr(st, k) for k, _ in A.tb_stats._fields_}
+
     def __del__(self):
         try:
             A.lib().tb_sched_destroy(self.h)
