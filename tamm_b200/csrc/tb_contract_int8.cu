@@ -16,10 +16,12 @@
 // order, when the group's tasks are done.
 //
 // Truncation: each operand is exact to 2^-(8S-1) of its row maximum and the dropped
-// pairs (i + j >= S) weigh at most ~S * 2^(2-8S) of row-max x col-max x K, so
-// S = 6 (21 INT8 products) gives ~1e-13 relative accuracy on this scale.  This is the
-// error-free splitting of Ozaki, Ogita, Oishi and Rump with the INT8 tensor-core
-// digit layout of Ootomo / Ozaki / Uchino-Imamura style DGEMM emulation.
+// pairs (i + j >= S) weigh at most ~S * 2^(2-8S) of row-max x col-max x K.  The slice
+// count is chosen per task: the largest task of an output block gets the S the error
+// target needs (S = 7, 28 INT8 products, for 1e-11), tasks 2^(8m) smaller get S - m,
+// numerically zero blocks one digit.  This is the error-free splitting of Ozaki,
+// Ogita, Oishi and Rump with the INT8 tensor-core digit layout of Ozaki / Uchino /
+// Imamura's DGEMM emulation.
 #include "tb_internal.hpp"
 #include "tb_runtime.hpp"
 #include "tb_sm100.cuh"
@@ -47,8 +49,9 @@ struct SplitBlock {
   int64_t src_off; // element offset in the FP64 arena
   int64_t dst_off; // byte offset of the block's slices in the scratch
   int32_t exp_off; // first exponent (int32 per padded row)
+  int32_t id;      // index into the per-block max-exponent array
   int32_t rows, K, rows_pad, K_pad, tile_rows;
-  int32_t nr, nk;
+  int32_t nr, nk, kcontig;
   int32_t rdim[kMaxClass], rstr[kMaxClass];
   int32_t kdim[kMaxClass], kstr[kMaxClass];
 };
@@ -58,6 +61,11 @@ struct I8Task {
   int32_t a_exp, b_exp; // exponent index bases
   int32_t nkc;          // K_pad / KC
   int32_t pad;
+};
+
+struct I8TaskMeta {
+  int32_t a_block, b_block; // max-exponent slots (B blocks after the A blocks)
+  int32_t log2k;            // ceil(log2 K) of the task
 };
 
 struct I8Item {
@@ -82,13 +90,23 @@ __device__ __forceinline__ int32_t canon_off(int r, int kk, int tile_rows) {
   return (kk >> 4) * (tile_rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kk & 15);
 }
 
-// One warp per (block, row): row max -> exponent, then the S digit slices of the row
-// (zero for padding rows / columns).  chunk table: (block, first row) per 8 rows.
+// Offset of the k-th K element of a row: contiguous K (the inner labels are the
+// trailing modes, last one stride 1) needs no index arithmetic.
+__device__ __forceinline__ int32_t koff(const SplitBlock& b, int32_t k) {
+  return b.kcontig ? k : decomp(k, b.nk, b.kdim, b.kstr);
+}
+
+// One warp per (block, row): row max -> exponent e, then the S base-256 digit
+// slices of X = trunc(x * 2^(8S-1-e)) for 16 consecutive k per thread, stored as one
+// 16-byte vector per slice (the k-run of one row inside one 16-byte core-matrix
+// row).  Padding rows / columns get zero digits.  chunk table: (block, first row)
+// per 8 rows.  blockmax[b] collects the largest row exponent of each block (rows
+// that are entirely zero do not count).
 template<int S>
 __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ blocks,
                                                const int2* __restrict__ chunks, int nchunks,
-                                               const double* __restrict__ src,
-                                               uint8_t* __restrict__ dst, int32_t* __restrict__ exps) {
+                                               const double* __restrict__ src, uint8_t* __restrict__ dst,
+                                               int32_t* __restrict__ exps, int32_t* __restrict__ blockmax) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int2       ch  = chunks[c];
@@ -100,27 +118,64 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
     const double* s      = src + b.src_off + rowoff;
     double        mx     = 0.0;
     if(live)
-      for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + decomp(k, b.nk, b.kdim, b.kstr))));
+      for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + koff(b, k))));
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     int e = 0;
     if(mx > 0.0) frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1): |x| < 2^e
-    const int    sh    = 8 * S - 1 - e;
-    const int    tile = row / b.tile_rows, r = row - tile * b.tile_rows;
-    const int    nkc  = b.K_pad / KC;
-    uint8_t*     out  = dst + b.dst_off + (int64_t) tile * nkc * S * b.tile_rows * KC;
-    for(int k = lane; k < b.K_pad; k += 32) {
-      long long X = 0;
-      if(live && k < b.K) X = __double2ll_rz(ldexp(__ldg(s + decomp(k, b.nk, b.kdim, b.kstr)), sh));
-      const int kc = k / KC, kk = k - kc * KC;
-      uint8_t*  o  = out + (int64_t) kc * S * b.tile_rows * KC + canon_off(r, kk, b.tile_rows);
+    const int sh   = 8 * S - 1 - e;
+    const int tile = row / b.tile_rows, r = row - tile * b.tile_rows;
+    const int nkc  = b.K_pad / KC;
+    uint8_t*  out  = dst + b.dst_off + (int64_t) tile * nkc * S * b.tile_rows * KC;
+    for(int g = lane; g < b.K_pad / 16; g += 32) {
+      const int k0 = g * 16;
+      long long X[16];
+#pragma unroll
+      for(int x = 0; x < 16; x++) {
+        const int k = k0 + x;
+        X[x]        = (live && k < b.K) ? __double2ll_rz(ldexp(__ldg(s + koff(b, k)), sh)) : 0ll;
+      }
+      const int kc = k0 / KC;
+      uint8_t*  o  = out + (int64_t) kc * S * b.tile_rows * KC + canon_off(r, k0 - kc * KC, b.tile_rows);
 #pragma unroll
       for(int i = 0; i < S; i++) {
-        const int ds = 8 * (S - 1 - i);
-        o[(int64_t) i * b.tile_rows * KC] = (uint8_t) ((X >> ds) & 0xFF); // d_0 keeps the sign bits
+        const int ds = 8 * (S - 1 - i); // digit i; d_0 keeps the sign bits
+        uint32_t  w[4];
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          w[q] = (uint32_t) ((X[4 * q] >> ds) & 0xFF) | ((uint32_t) ((X[4 * q + 1] >> ds) & 0xFF) << 8) |
+                 ((uint32_t) ((X[4 * q + 2] >> ds) & 0xFF) << 16) |
+                 ((uint32_t) ((X[4 * q + 3] >> ds) & 0xFF) << 24);
+        *reinterpret_cast<uint4*>(o + (int64_t) i * b.tile_rows * KC) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
-    if(lane == 0) exps[b.exp_off + row] = e;
+    if(lane == 0) {
+      exps[b.exp_off + row] = e;
+      if(mx > 0.0) atomicMax(blockmax + b.id, e);
+    }
+  }
+}
+
+// Slice count per task: a task whose largest possible product (2^(maxexp A + maxexp
+// B) * K) is 2^(8m) below the largest of its output group needs m fewer digits for
+// the same absolute truncation error; numerically zero blocks keep one digit.
+__global__ void k_task_slices(const I8TaskMeta* __restrict__ meta, const DevGroup* __restrict__ groups,
+                              int ngroups, const int32_t* __restrict__ blockmax, int smax,
+                              uint8_t* __restrict__ tslices) {
+  for(int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ngroups; gi += gridDim.x * blockDim.x) {
+    constexpr int  kNone = -1000000; // blockmax slots start at 0x80808080 (no nonzero row)
+    const DevGroup g     = groups[gi];
+    int            eg    = kNone;
+    for(int t = g.task_begin; t < g.task_end; t++) {
+      const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
+      if(ea > kNone && eb > kNone) eg = max(eg, ea + eb + meta[t].log2k);
+    }
+    for(int t = g.task_begin; t < g.task_end; t++) {
+      const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
+      int       s  = 1;
+      if(ea > kNone && eb > kNone) s = max(1, smax - (eg - (ea + eb + meta[t].log2k)) / 8);
+      tslices[t] = (uint8_t) s;
+    }
   }
 }
 
@@ -135,6 +190,7 @@ struct I8Params {
   double          alpha;
   LabelClasses    lc;
   int*            err;
+  const uint8_t*  tslices; // digit count of each task (1..S)
 };
 
 template<int S, int NT>
@@ -186,11 +242,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           const I8Task   tk = p.tasks[t];
           const uint8_t* ga = p.slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
           const uint8_t* gb = p.slices + tk.b_off + (int64_t) item.nt * tk.nkc * B_BYTES;
+          const uint32_t st = p.tslices[t]; // only the task's leading digits travel
+          const uint32_t ab = st * MT * KC, bb = st * NT * KC;
           for(int kc = 0; kc < tk.nkc; kc++) {
             if(!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) goto done_producer;
-            mbar_arrive_expect_tx(&full[stage], STAGE);
-            bulk_g2s(smem + stage * STAGE, ga + (int64_t) kc * A_BYTES, A_BYTES, &full[stage]);
-            bulk_g2s(smem + stage * STAGE + A_BYTES, gb + (int64_t) kc * B_BYTES, B_BYTES, &full[stage]);
+            mbar_arrive_expect_tx(&full[stage], ab + bb);
+            bulk_g2s(smem + stage * STAGE, ga + (int64_t) kc * A_BYTES, ab, &full[stage]);
+            bulk_g2s(smem + stage * STAGE + A_BYTES, gb + (int64_t) kc * B_BYTES, bb, &full[stage]);
             if(++stage == STAGES) {
               stage = 0;
               phase ^= 1;
@@ -211,6 +269,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         const DevGroup g    = p.groups[item.group];
         for(int t = g.task_begin; t < g.task_end; t++) {
           const int nkc = p.tasks[t].nkc;
+          const int st  = p.tslices[t];
           if(!mbar_wait(tempty, tphase ^ 1, p.err, 2)) goto done_mma;
           tc_fence_after();
           for(int kc = 0; kc < nkc; kc++) {
@@ -219,6 +278,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
             const uint32_t a0 = smem_u32(smem + stage * STAGE), b0 = a0 + A_BYTES;
 #pragma unroll
             for(int d = 0; d < S; d++) {
+              if(d >= st) break;
 #pragma unroll
               for(int i = 0; i <= d; i++) {
                 const int      j  = d - i;
@@ -259,6 +319,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         tphase ^= 1;
         tc_fence_after();
         const I8Task tk = p.tasks[t];
+        const int    st = p.tslices[t];
         const int    er = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
         const double sr = ldexp(1.0, er - 7);
 #pragma unroll
@@ -268,6 +329,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           for(int x = 0; x < 16; x++) tacc[x] = 0.0;
 #pragma unroll
           for(int d = 0; d < S; d++) {
+            if(d >= st) break;
             uint32_t v[16];
             tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + d * NT + c0, v);
             tmem_wait_ld();
@@ -333,6 +395,7 @@ struct I8Layout {
   std::vector<SplitBlock> a_blocks, b_blocks;
   std::vector<int2>       a_chunks, b_chunks;
   std::vector<I8Task>     tasks;
+  std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
   int64_t                 slice_bytes = 0, a_bytes = 0;
   int64_t                 nexp = 0, a_nexp = 0;
@@ -343,6 +406,9 @@ struct I8Layout {
   int2*                   d_bchunks = nullptr;
   I8Task*                 d_tasks   = nullptr;
   I8Item*                 d_items   = nullptr;
+  I8TaskMeta*             d_meta    = nullptr;
+  int32_t*                d_blockmax = nullptr;
+  uint8_t*                d_tslices  = nullptr;
   int*                    d_err     = nullptr;
   int                     device    = -1;
   ~I8Layout() {
@@ -354,6 +420,9 @@ struct I8Layout {
       cudaFree(d_bchunks);
       cudaFree(d_tasks);
       cudaFree(d_items);
+      cudaFree(d_meta);
+      cudaFree(d_blockmax);
+      cudaFree(d_tslices);
       cudaFree(d_err);
     }
   }
@@ -377,6 +446,7 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
     }
   };
   L->tasks.resize(wl.tasks.size());
+  L->meta.resize(wl.tasks.size());
   for(const auto& g: wl.groups) {
     for(int t = g.task_begin; t < g.task_end; t++) {
       const DevTask& tk = wl.tasks[t];
@@ -402,6 +472,9 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
           b.kstr[j] = (int32_t) astr[lc.k_a[j]];
         }
         b.K         = K;
+        b.kcontig   = 1;
+        for(int j = 0; j < lc.nk; j++) b.kcontig &= (lc.k_a[j] == lc.na - lc.nk + j) ? 1 : 0;
+        b.id        = (int32_t) L->a_blocks.size();
         b.tile_rows = MT;
         b.rows_pad  = (int32_t) rup(b.rows, MT);
         b.K_pad     = (int32_t) rup(K, KC);
@@ -429,6 +502,9 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
           b.kstr[j] = (int32_t) bstr[lc.k_b[j]];
         }
         b.K         = K;
+        b.kcontig   = 1;
+        for(int j = 0; j < lc.nk; j++) b.kcontig &= (lc.k_b[j] == lc.nb - lc.nk + j) ? 1 : 0;
+        b.id        = (int32_t) L->b_blocks.size(); // rebased after the A blocks below
         b.tile_rows = L->NT;
         b.rows_pad  = (int32_t) rup(b.rows, L->NT);
         b.K_pad     = (int32_t) rup(K, KC);
@@ -448,13 +524,22 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
       it.b_exp     = B.exp_off;
       it.nkc       = A.K_pad / KC;
       L->tasks[t]  = it;
+      I8TaskMeta mt{};
+      mt.a_block = A.id;
+      mt.b_block = B.id; // rebased below
+      int lk = 0;
+      while((1ll << lk) < K) lk++;
+      mt.log2k    = lk;
+      L->meta[t]  = mt;
     }
   }
   TB_EXPECTS(aexp + bexp < (1ll << 31), "too many split rows");
   for(auto& b: L->b_blocks) {
     b.dst_off += abytes;
     b.exp_off += (int32_t) aexp;
+    b.id += (int32_t) L->a_blocks.size();
   }
+  for(auto& m: L->meta) m.b_block += (int32_t) L->a_blocks.size();
   for(auto& t: L->tasks) {
     t.b_off += abytes;
     t.b_exp += (int32_t) aexp;
@@ -499,6 +584,10 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   up(L->d_bchunks, L->b_chunks);
   up(L->d_tasks, L->tasks);
   up(L->d_items, L->items);
+  up(L->d_meta, L->meta);
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_blockmax),
+                     sizeof(int32_t) * std::max<size_t>(1, L->a_blocks.size() + L->b_blocks.size())));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_tslices), std::max<size_t>(1, L->tasks.size())));
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_err), sizeof(int)));
   TB_CUDA(cudaMemset(L->d_err, 0, sizeof(int)));
   return L;
@@ -512,15 +601,20 @@ int sm_count() {
 }
 
 template<int S>
-void launch_split(const I8Layout& L, const double* A, const double* B, uint8_t* slices, int32_t* exps,
-                  cudaStream_t st) {
+void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const double* B, uint8_t* slices,
+                  int32_t* exps, cudaStream_t st) {
   const int grid_cap = sm_count() * 8;
+  // 0x80808080: below every exponent sum, marks blocks without a nonzero row
+  TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
   if(!L.a_chunks.empty())
     k_split<S><<<std::min<int64_t>((int64_t) L.a_chunks.size(), grid_cap), 256, 0, st>>>(
-      L.d_ablocks, L.d_achunks, (int) L.a_chunks.size(), A, slices, exps);
+      L.d_ablocks, L.d_achunks, (int) L.a_chunks.size(), A, slices, exps, L.d_blockmax);
   if(!L.b_chunks.empty())
     k_split<S><<<std::min<int64_t>((int64_t) L.b_chunks.size(), grid_cap), 256, 0, st>>>(
-      L.d_bblocks, L.d_bchunks, (int) L.b_chunks.size(), B, slices, exps);
+      L.d_bblocks, L.d_bchunks, (int) L.b_chunks.size(), B, slices, exps, L.d_blockmax);
+  const int ng = (int) wl.groups.size();
+  if(ng > 0)
+    k_task_slices<<<(ng + 255) / 256, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -538,7 +632,8 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   p.C      = C;
   p.alpha  = alpha;
   p.lc     = lc;
-  p.err    = L.d_err;
+  p.err     = L.d_err;
+  p.tslices = L.d_tslices;
   const size_t smem = smem_bytes<S, NT>();
   static bool  configured[64] = {false};
   int          dev            = 0;
@@ -557,16 +652,19 @@ void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double
            const double* B, double* C, uint8_t* slices, int32_t* exps, cudaStream_t st,
            cudaEvent_t* ev) {
   if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
-  launch_split<S>(L, A, B, slices, exps, st);
+  launch_split<S>(L, wl, A, B, slices, exps, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
   launch_gemm<S, (S <= 6 ? 80 : 64)>(L, wl, lc, alpha, slices, exps, C, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
 }
 
-// slice count for an error target: smallest S with S * 2^(2 - 8S) * 16 <= target
+// Largest slice count for an error target: the truncation bound S * 2^(2 - 8S) of
+// row-max x col-max x K, times 2^10 for the cancellation between that scale and the
+// largest |C| seen on coupled-cluster data (O=40/V=360 ladder: S = 6 -> 1.1e-10,
+// S = 7 -> 4e-13 measured); smallest S meeting the target.
 int slices_for(double err_target) {
   for(int S = 3; S <= 8; S++)
-    if(S * std::ldexp(1.0, 2 - 8 * S) * 16.0 <= err_target) return S;
+    if(S * std::ldexp(1.0, 2 - 8 * S) * 1024.0 <= err_target) return S;
   return 8;
 }
 
@@ -615,9 +713,29 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
     plan.last.gemm_ms  = b;
     for(auto& e: evs) cudaEventDestroy(e);
   }
-  plan.last.int8_ops      = L->int8_ops;
-  plan.last.slices_min    = S;
-  plan.last.slices_max    = S;
+  plan.last.int8_ops   = L->int8_ops;
+  plan.last.slices_min = S;
+  plan.last.slices_max = S;
+  if(plan.profile && !L->tasks.empty()) {
+    // exact INT8 work of this launch: per output tile, per task, St(St+1)/2 products
+    std::vector<uint8_t> ts(L->tasks.size());
+    TB_CUDA(cudaMemcpyAsync(ts.data(), L->d_tslices, ts.size(), cudaMemcpyDeviceToHost, stream));
+    TB_CUDA(cudaStreamSynchronize(stream));
+    double ops = 0;
+    int    smin = S, smax = 1;
+    for(const auto& it: L->items) {
+      const DevGroup& g = wl.groups[it.group];
+      for(int t = g.task_begin; t < g.task_end; t++) {
+        const int st = ts[t];
+        ops += 2.0 * MT * L->NT * KC * L->tasks[t].nkc * (st * (st + 1) / 2);
+        smin = std::min(smin, st);
+        smax = std::max(smax, st);
+      }
+    }
+    plan.last.int8_ops   = ops;
+    plan.last.slices_min = smin;
+    plan.last.slices_max = smax;
+  }
   plan.last.scratch_bytes = L->slice_bytes + 4 * L->nexp;
   if(plan.check_errors) {
     int h = 0;

@@ -79,6 +79,30 @@ def test_int8_spin_ladder_default_target(ec):
     assert rel_err(lad.r2.read(), want) <= INT8_TOL
 
 
+def test_int8_cholesky_ladder_with_zero_spin_blocks(ec):
+    """v built on the device from Cholesky vectors (its (ab|ba)-type spin blocks are
+    exactly zero, its off-diagonal blocks damped): per-task digit counts must keep the
+    1e-11 bar and give zero blocks a single digit."""
+    lad = W.ladder(4, 13, seed=6, tile_lo=3, tile_hi=6, ec=ec, build_v=True)
+    a, b, c, d, i, j = lad.labels
+    vh = lad.v.read().copy()
+    ov, ot, orr = (O.BlockTensor([s.tile_sizes for s in x.spaces], [s.tile_spins for s in x.spaces], [0, 0, 1, 1])
+                   for x in (lad.v, lad.t2, lad.r2))
+    ov.data[:ov.total] = vh
+    ot.data[:ot.total] = lad.t2_host
+    O.mult_bufacc(orr, [1, 2, 5, 6], 1.0, ov, [1, 2, 3, 4], ot, [3, 4, 5, 6])
+    zero_blocks = [bid for bid in ov.blockids() if not np.any(ov.block(bid))]
+    assert zero_blocks  # the spin-flip blocks of a Cholesky-built v
+    ec.set_precision(tb.Precision.INT8, 1e-11)
+    try:
+        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(profile=True)
+        st = lad.sch.op_stats(-1)
+    finally:
+        ec.set_precision(tb.Precision.FP64)
+    assert rel_err(lad.r2.read(), orr.data[:orr.total]) <= INT8_TOL
+    assert st["slices_min"] == 1 and st["slices_max"] == 7
+
+
 def test_int8_slice_count_controls_error(ec):
     lad, want = _ladder_case(ec, seed=4)
     a, b, c, d, i, j = lad.labels
