@@ -96,63 +96,83 @@ __device__ __forceinline__ int32_t koff(const SplitBlock& b, int32_t k) {
   return b.kcontig ? k : decomp(k, b.nk, b.kdim, b.kstr);
 }
 
-// One warp per (block, row): row max -> exponent e, then the S base-256 digit
-// slices of X = trunc(x * 2^(8S-1-e)) for 16 consecutive k per thread, stored as one
-// 16-byte vector per slice (the k-run of one row inside one 16-byte core-matrix
-// row).  Padding rows / columns get zero digits.  chunk table: (block, first row)
-// per 8 rows.  blockmax[b] collects the largest row exponent of each block (rows
-// that are entirely zero do not count).
+// trunc(x * 2^sh) as a two's-complement integer, |result| < 2^63, from the IEEE-754
+// fields (x = m * 2^(E-52) with the 53-bit integer m): a shift of m, no FP64 pipe.
+__device__ __forceinline__ long long scaled_trunc(double x, int sh) {
+  const long long bits = __double_as_longlong(x);
+  const int       E    = (int) ((bits >> 52) & 0x7FF);
+  const long long frac = bits & 0xFFFFFFFFFFFFFll;
+  const long long m    = E ? (frac | (1ll << 52)) : frac; // subnormals: no hidden bit
+  const int       s    = (E ? E : 1) - 1075 + sh;         // x * 2^sh = m * 2^s
+  long long       v;
+  if(s >= 0) v = m << s;
+  else v = (s > -64) ? (m >> (-s)) : 0;
+  return bits < 0 ? -v : v;
+}
+
+// One CTA per 8-row group of one block (the rows of one core-matrix row group):
+// warp w finds the max |x| of row w (exponent e_w), then the CTA emits the S
+// base-256 digits of X = trunc(x * 2^(8S-1-e)) one 8-row x 16-k core matrix per warp
+// and step: thread (row r, quad q) converts k = 4q..4q+3 of its row and writes 4
+// bytes per digit slice, so each warp store is one contiguous 128-byte core matrix.
+// Padding rows / columns get zero digits.  blockmax[b] collects the largest row
+// exponent of each block (rows that are entirely zero do not count).
 template<int S>
 __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ blocks,
                                                const int2* __restrict__ chunks, int nchunks,
                                                const double* __restrict__ src, uint8_t* __restrict__ dst,
                                                int32_t* __restrict__ exps, int32_t* __restrict__ blockmax) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ int     s_sh[8];
+  __shared__ int32_t s_off[8];
+  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
-    const int2       ch  = chunks[c];
-    const SplitBlock b   = blocks[ch.x];
-    const int        row = ch.y + warp;
-    if(row >= b.rows_pad) continue;
-    const bool    live   = row < b.rows;
-    const int32_t rowoff = live ? decomp(row, b.nr, b.rdim, b.rstr) : 0;
-    const double* s      = src + b.src_off + rowoff;
-    double        mx     = 0.0;
-    if(live)
-      for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + koff(b, k))));
+    const int2       ch = chunks[c];
+    const SplitBlock b  = blocks[ch.x];
+    {
+      const int     row    = ch.y + warp;
+      const bool    live   = row < b.rows;
+      const int32_t rowoff = live ? decomp(row, b.nr, b.rdim, b.rstr) : 0;
+      const double* s      = src + b.src_off + rowoff;
+      double        mx     = 0.0;
+      if(live)
+        for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + koff(b, k))));
 #pragma unroll
-    for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    int e = 0;
-    if(mx > 0.0) frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1): |x| < 2^e
-    const int sh   = 8 * S - 1 - e;
-    const int tile = row / b.tile_rows, r = row - tile * b.tile_rows;
-    const int nkc  = b.K_pad / KC;
-    uint8_t*  out  = dst + b.dst_off + (int64_t) tile * nkc * S * b.tile_rows * KC;
-    for(int g = lane; g < b.K_pad / 16; g += 32) {
-      const int k0 = g * 16;
-      long long X[16];
-#pragma unroll
-      for(int x = 0; x < 16; x++) {
-        const int k = k0 + x;
-        X[x]        = (live && k < b.K) ? __double2ll_rz(ldexp(__ldg(s + koff(b, k)), sh)) : 0ll;
+      for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      int e = 0;
+      if(mx > 0.0) frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1): |x| < 2^e
+      if(lane == 0) {
+        s_sh[warp]  = live ? 8 * S - 1 - e : -1; // -1: padding row
+        s_off[warp] = rowoff;
+        exps[b.exp_off + row] = e;
+        if(mx > 0.0) atomicMax(blockmax + b.id, e);
       }
-      const int kc = k0 / KC;
-      uint8_t*  o  = out + (int64_t) kc * S * b.tile_rows * KC + canon_off(r, k0 - kc * KC, b.tile_rows);
+    }
+    __syncthreads();
+    const int r = lane >> 2, q = lane & 3; // row within the 8-row group, k quad
+    const int sh = s_sh[r];
+    const double* s   = src + b.src_off + s_off[r];
+    const int     g8  = (ch.y % b.tile_rows) >> 3;
+    const int     nkc = b.K_pad / KC;
+    uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
+                   q * 4;
+    for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) { // one core matrix per warp and step
+      const int k0 = k16 * 16 + q * 4;
+      long long X[4];
+#pragma unroll
+      for(int x = 0; x < 4; x++) {
+        const int k = k0 + x;
+        X[x]        = (sh >= 0 && k < b.K) ? scaled_trunc(__ldg(s + koff(b, k)), sh) : 0ll;
+      }
+      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * b.tile_rows * 16;
 #pragma unroll
       for(int i = 0; i < S; i++) {
         const int ds = 8 * (S - 1 - i); // digit i; d_0 keeps the sign bits
-        uint32_t  w[4];
-#pragma unroll
-        for(int q = 0; q < 4; q++)
-          w[q] = (uint32_t) ((X[4 * q] >> ds) & 0xFF) | ((uint32_t) ((X[4 * q + 1] >> ds) & 0xFF) << 8) |
-                 ((uint32_t) ((X[4 * q + 2] >> ds) & 0xFF) << 16) |
-                 ((uint32_t) ((X[4 * q + 3] >> ds) & 0xFF) << 24);
-        *reinterpret_cast<uint4*>(o + (int64_t) i * b.tile_rows * KC) = make_uint4(w[0], w[1], w[2], w[3]);
+        const uint32_t w = (uint32_t) ((X[0] >> ds) & 0xFF) | ((uint32_t) ((X[1] >> ds) & 0xFF) << 8) |
+                           ((uint32_t) ((X[2] >> ds) & 0xFF) << 16) | ((uint32_t) ((X[3] >> ds) & 0xFF) << 24);
+        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w;
       }
     }
-    if(lane == 0) {
-      exps[b.exp_off + row] = e;
-      if(mx > 0.0) atomicMax(blockmax + b.id, e);
-    }
+    __syncthreads();
   }
 }
 
@@ -200,7 +220,7 @@ constexpr uint32_t stage_bytes() {
 
 template<int S, int NT>
 constexpr size_t smem_bytes() {
-  return (size_t) STAGES * stage_bytes<S, NT>() + 1024;
+  return (size_t) STAGES * stage_bytes<S, NT>() + 2048;
 }
 
 template<int S, int NT>
@@ -211,8 +231,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   uint64_t*          full   = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE);
   uint64_t*          empty  = full + STAGES;
   uint64_t*          tfull  = empty + STAGES;
-  uint64_t*          tempty = tfull + 1;
-  uint32_t*          tslot  = reinterpret_cast<uint32_t*>(tempty + 1);
+  uint64_t*          tempty = tfull + 1;                                    // one per diagonal
+  double*            sc     = reinterpret_cast<double*>(tempty + 8);         // column scales
+  uint32_t*          tslot  = reinterpret_cast<uint32_t*>(sc + NT);
   const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if(threadIdx.x == 0) {
@@ -221,7 +242,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    mbar_init(tempty, 128);
+    for(int d = 0; d < S; d++) mbar_init(&tempty[d], 128);
     fence_mbarrier_init();
   }
   if(warp == 1) tmem_alloc(tslot, 512);
@@ -270,8 +291,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         for(int t = g.task_begin; t < g.task_end; t++) {
           const int nkc = p.tasks[t].nkc;
           const int st  = p.tslices[t];
-          if(!mbar_wait(tempty, tphase ^ 1, p.err, 2)) goto done_mma;
-          tc_fence_after();
           for(int kc = 0; kc < nkc; kc++) {
             if(!mbar_wait(&full[stage], phase, p.err, 3)) goto done_mma;
             tc_fence_after();
@@ -279,6 +298,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 #pragma unroll
             for(int d = 0; d < S; d++) {
               if(d >= st) break;
+              if(kc == 0) { // diagonal d of the previous task must have been read out
+                if(!mbar_wait(&tempty[d], tphase ^ 1, p.err, 2)) goto done_mma;
+                tc_fence_after();
+              }
 #pragma unroll
               for(int i = 0; i <= d; i++) {
                 const int      j  = d - i;
@@ -287,6 +310,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                 mma_i8(tmem + d * NT, ad, bd, idesc_i8(MT, NT, i == 0, j == 0), kc > 0 || i > 0);
               }
             }
+            if(kc == 0) // keep the unused diagonals' barriers in phase
+              for(int d = st; d < S; d++)
+                if(!mbar_wait(&tempty[d], tphase ^ 1, p.err, 2)) goto done_mma;
             umma_commit(&empty[stage]); // stage free once these MMAs have read it
             if(++stage == STAGES) {
               stage = 0;
@@ -312,7 +338,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       for(int x = 0; x < NT; x++) racc[x] = 0.0;
       bool ok = true;
       for(int t = g.task_begin; t < g.task_end; t++) {
-        if(!mbar_wait(tfull, tphase, p.err, 4)) {
+        // the 128 epilogue threads agree on a timeout, so none is left in a barrier
+        const bool     waited = mbar_wait(tfull, tphase, p.err, 4);
+        uint32_t       anyfail;
+        asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
+                     "bar.red.or.pred q, 1, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                     : "=r"(anyfail)
+                     : "r"((uint32_t) waited)
+                     : "memory");
+        if(anyfail) {
           ok = false;
           break;
         }
@@ -322,27 +356,40 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         const int    st = p.tslices[t];
         const int    er = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
         const double sr = ldexp(1.0, er - 7);
+        // per-column scales 2^(e_col - 7) of this task, shared by the 128 rows (the
+        // barrier above also ends every thread's use of the previous task's scales)
+        const int et = threadIdx.x - 64;
+        if(et < NT) sc[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - 7);
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        // drain diagonal by diagonal; each diagonal's TMEM is released as soon as it
+        // has been read, so the next task's MMAs into it can start
+        constexpr int CW = NT <= 64 ? NT : 48; // columns in flight per wait
 #pragma unroll
-        for(int c0 = 0; c0 < NT; c0 += 16) {
-          double tacc[16];
+        for(int d = 0; d < S; d++) {
+          if(d < st) {
+            const double w = pow2i(-8 * d) * sr;
 #pragma unroll
-          for(int x = 0; x < 16; x++) tacc[x] = 0.0;
+            for(int c0 = 0; c0 < NT; c0 += CW) {
+              constexpr int NL = CW / 16;
+              uint32_t      v[CW];
 #pragma unroll
-          for(int d = 0; d < S; d++) {
-            if(d >= st) break;
-            uint32_t v[16];
-            tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + d * NT + c0, v);
-            tmem_wait_ld();
-            const double w = pow2i(-8 * d);
+              for(int l = 0; l < NL; l++)
+                if(c0 + 16 * l < NT)
+                  tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + d * NT + c0 + 16 * l,
+                            *reinterpret_cast<uint32_t(*)[16]>(v + 16 * l));
+              tmem_wait_ld();
+              if(c0 + CW >= NT) {
+                tc_fence_before();
+                mbar_arrive(&tempty[d]);
+              }
 #pragma unroll
-            for(int x = 0; x < 16; x++) tacc[x] += (double) (int32_t) v[x] * w;
+              for(int x = 0; x < CW; x++)
+                if(c0 + x < NT) racc[c0 + x] = fma((double) (int32_t) v[x], w * sc[c0 + x], racc[c0 + x]);
+            }
           }
-          const int32_t* ec = p.exps + tk.b_exp + item.nt * NT + c0;
-#pragma unroll
-          for(int x = 0; x < 16; x++) racc[c0 + x] += tacc[x] * sr * ldexp(1.0, __ldg(ec + x) - 7);
+          else
+            mbar_arrive(&tempty[d]);
         }
-        tc_fence_before();
-        mbar_arrive(tempty);
       }
       if(!ok) break;
       // C (+)= alpha * result, in C's own layout (transpose_output fused here)
