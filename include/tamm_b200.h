@@ -90,6 +90,30 @@ int tb_fill(double* x, int64_t n, double value, int is_assign, void* stream);
  * and the flat AddOp plan, addop.hpp:426-454). */
 int tb_axpby(double alpha, const double* x, double beta, double* y, int64_t n, void* stream);
 
+/* Split-INT8 C += alpha * A * B for ONE block triple without allocating anything.
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory — applications whose device memory is already owned by other
+ * allocators (TAMM's RMM pool takes 80% of the free memory at start-up, a caching
+ * allocator the rest), or code that must not trigger the device-wide
+ * synchronisation cudaMalloc / cudaFree can cause.  It makes no cudaMalloc,
+ * cudaMallocAsync, cudaFree or host-heap call: its scratch (digit slices,
+ * exponents, the one-task work list) is a file-scope device array of 64 MiB that
+ * every GPU loading the library holds until exit.  A triple needing more scratch
+ * (about 7 * K * (M + N) bytes at the default 7 digits) is rejected with
+ * TB_ERR_INVALID and a message giving the size.  Labels as in tb_block_multiply
+ * (plain contractions only: no Hadamard or one-sided reduction labels); nslices 0
+ * picks the digit count for a 1e-11 target, 3..8 forces it.  The first call on a
+ * device looks up the array's device address once for that device (make it before
+ * any stream capture).  Every call reuses the same array and leaves its contents
+ * behind; each call resets what it needs to start from a known value, and calls
+ * that overlap on the GPU (other streams, other threads) race on the array.  The
+ * call returns after the stream has drained. */
+int tb_block_multiply_int8_noalloc(double alpha, const double* a, const int64_t* adims,
+                                   const int* alabels, int na, const double* b,
+                                   const int64_t* bdims, const int* blabels, int nb, double* c,
+                                   const int64_t* cdims, const int* clabels, int nc, int nslices,
+                                   void* stream);
+
 /* sqrt(sum x^2) over x[0:n], written to *host_out after the stream drains
  * (tamm::norm, src/tamm/tamm_utils.hpp:1180-1200).  Deterministic two-pass reduction. */
 int tb_norm2(const double* x, int64_t n, double* host_out, void* stream);

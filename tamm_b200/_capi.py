@@ -49,6 +49,8 @@ PROTOS = {
     "tb_block_multiply": [C.c_double, vp, i64p, ip, C.c_int, vp, i64p, ip, C.c_int, C.c_double, vp,
                           i64p, ip, C.c_int, C.c_int, C.c_int, vp],
     "tb_block_assign": [vp, i64p, ip, C.c_int, C.c_double, vp, i64p, ip, C.c_int, C.c_int, vp],
+    "tb_block_multiply_int8_noalloc": [C.c_double, vp, i64p, ip, C.c_int, vp, i64p, ip, C.c_int, vp, i64p, ip,
+                                       C.c_int, C.c_int, vp],
     "tb_fill": [vp, C.c_int64, C.c_double, C.c_int, vp],
     "tb_axpby": [C.c_double, vp, C.c_double, vp, C.c_int64, vp],
     "tb_norm2": [vp, C.c_int64, dp, vp],

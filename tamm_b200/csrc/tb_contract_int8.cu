@@ -809,4 +809,252 @@ void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double*
   fail(TB_ERR_NOT_IMPLEMENTED, "BF16x3 contraction is not built yet");
 }
 
+// ------------------------------------------------------------------------------
+// Split-INT8 block multiply that allocates nothing (tb_block_multiply_int8_noalloc).
+//
+// Some callers cannot allocate device memory: an application whose device memory
+// is already owned by other allocators (TAMM's RMM pool reserves 80% of the free
+// memory at start-up and a framework's caching allocator keeps the rest, so a
+// cudaMalloc here fails or fragments), or code that must not trigger the
+// device-wide synchronisation that cudaMalloc / cudaFree can cause.  For them this
+// entry point keeps all of its scratch (digit slices, exponents and the one-task
+// work list) in one file-scope device array of fixed size, reserved when the
+// library's device code is loaded and held by every GPU that loads it until exit.
+
+namespace {
+
+constexpr int64_t kNoAllocBytes = int64_t(64) << 20; // 64 MiB of scratch per GPU
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocDevices = 64;
+void*         g_noalloc_base[kNoAllocDevices] = {nullptr}; // device address, per device
+
+// Control words and descriptors at fixed offsets of the scratch.
+constexpr int64_t kCtlErr = 0, kCtlBlockMax = 8, kCtlSlices = 16, kCtlDesc = 256, kCtlItems = 1280;
+
+struct NoAllocDesc {
+  SplitBlock a, b;
+  DevGroup   g;
+  I8Task     task;
+  I8TaskMeta meta;
+  int32_t    mtiles, ntiles, nchunk_a, nchunk_b;
+  int64_t    chunks_off;
+};
+static_assert(kCtlDesc + 2 * sizeof(SplitBlock) + sizeof(DevGroup) + sizeof(I8Task) + sizeof(I8TaskMeta) <=
+                kCtlItems,
+              "descriptor area overflows into the item list");
+
+// Writes the work list and chunk tables of one block triple into the scratch and
+// resets what must start from a known value (error word, block max exponents).
+__global__ void k_noalloc_setup(NoAllocDesc d, unsigned char* base) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  if(tid == 0) {
+    *reinterpret_cast<int*>(base + kCtlErr)              = 0;
+    reinterpret_cast<int32_t*>(base + kCtlBlockMax)[0]   = (int32_t) 0x80808080;
+    reinterpret_cast<int32_t*>(base + kCtlBlockMax)[1]   = (int32_t) 0x80808080;
+    SplitBlock* sb                                       = reinterpret_cast<SplitBlock*>(base + kCtlDesc);
+    sb[0]                                                = d.a;
+    sb[1]                                                = d.b;
+    *reinterpret_cast<DevGroup*>(sb + 2)                 = d.g;
+    *reinterpret_cast<I8Task*>(reinterpret_cast<DevGroup*>(sb + 2) + 1) = d.task;
+    *reinterpret_cast<I8TaskMeta*>(reinterpret_cast<I8Task*>(reinterpret_cast<DevGroup*>(sb + 2) + 1) + 1) =
+      d.meta;
+  }
+  I8Item* items = reinterpret_cast<I8Item*>(base + kCtlItems);
+  for(int i = tid; i < d.mtiles * d.ntiles; i += nth) items[i] = I8Item{0, i / d.ntiles, i % d.ntiles, 0};
+  int2* chunks = reinterpret_cast<int2*>(base + d.chunks_off);
+  for(int i = tid; i < d.nchunk_a + d.nchunk_b; i += nth)
+    chunks[i] = i < d.nchunk_a ? make_int2(0, 8 * i) : make_int2(1, 8 * (i - d.nchunk_a));
+}
+
+template<int S>
+void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off, int64_t slices_off,
+                    const LabelClasses& lc, double alpha, const double* A, const double* B, double* C,
+                    cudaStream_t st) {
+  constexpr int NT   = S <= 6 ? 80 : 64;
+  SplitBlock*   sb   = reinterpret_cast<SplitBlock*>(base + kCtlDesc);
+  DevGroup*     grp  = reinterpret_cast<DevGroup*>(sb + 2);
+  I8Task*       tsk  = reinterpret_cast<I8Task*>(grp + 1);
+  I8TaskMeta*   meta = reinterpret_cast<I8TaskMeta*>(tsk + 1);
+  int2*         ch   = reinterpret_cast<int2*>(base + d.chunks_off);
+  int32_t*      bmax = reinterpret_cast<int32_t*>(base + kCtlBlockMax);
+  uint8_t*      tsl  = base + kCtlSlices;
+  int32_t*      exps = reinterpret_cast<int32_t*>(base + exps_off);
+  uint8_t*      sl   = base + slices_off;
+  k_noalloc_setup<<<8, 256, 0, st>>>(d, base);
+  const int cap = sm_count() * 8;
+  k_split<S><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
+  k_split<S><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
+  k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
+  I8Params p;
+  p.slices  = sl;
+  p.exps    = exps;
+  p.tasks   = tsk;
+  p.groups  = grp;
+  p.items   = reinterpret_cast<const I8Item*>(base + kCtlItems);
+  p.nitems  = d.mtiles * d.ntiles;
+  p.C       = C;
+  p.alpha   = alpha;
+  p.lc      = lc;
+  p.err     = reinterpret_cast<int*>(base + kCtlErr);
+  p.tslices = tsl;
+  const size_t smem = smem_bytes<S, NT>();
+  TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+  k_contract_i8<S, NT><<<std::min(p.nitems, sm_count()), NTHREADS, smem, st>>>(p);
+  TB_CUDA(cudaGetLastError());
+}
+
+} // namespace
+
 } // namespace tb
+
+extern "C" int tb_block_multiply_int8_noalloc(double alpha, const double* a, const int64_t* adims,
+                                              const int* alabels, int na, const double* b,
+                                              const int64_t* bdims, const int* blabels, int nb,
+                                              double* c, const int64_t* cdims, const int* clabels,
+                                              int nc, int nslices, void* stream) {
+  using namespace tb;
+  try {
+    TB_EXPECTS(a != nullptr && b != nullptr && c != nullptr, "a, b and c must be non-null");
+    TB_EXPECTS((na == 0 || (adims && alabels)) && (nb == 0 || (bdims && blabels)) && (nc == 0 || (cdims && clabels)),
+               "dims/labels arrays must be given for every non-scalar operand");
+    TB_EXPECTS(nslices == 0 || (nslices >= 3 && nslices <= 8), "nslices must be 0 (target 1e-11) or 3..8");
+    const LabelClasses lc = classify(clabels, nc, alabels, na, blabels, nb);
+    if(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0)
+      fail(TB_ERR_NOT_IMPLEMENTED, "the allocation-free split-INT8 entry point takes plain contractions only "
+                                   "(no Hadamard, one-sided reduction or outer-product labels)");
+    for(int i = 0; i < na; i++) TB_EXPECTS(adims[i] > 0 && adims[i] < (1 << 30), "block extent out of range");
+    for(int i = 0; i < nb; i++) TB_EXPECTS(bdims[i] > 0 && bdims[i] < (1 << 30), "block extent out of range");
+    for(int i = 0; i < nc; i++) TB_EXPECTS(cdims[i] > 0 && cdims[i] < (1 << 30), "block extent out of range");
+    const int S  = nslices > 0 ? nslices : slices_for(1e-11);
+    const int NT = S <= 6 ? 80 : 64;
+
+    // block geometry, the same views the allocating path builds (build_layout)
+    int64_t astr[kMaxModes], bstr[kMaxModes];
+    {
+      int64_t s = 1;
+      for(int i = na - 1; i >= 0; i--) {
+        astr[i] = s;
+        s *= adims[i];
+      }
+      s = 1;
+      for(int i = nb - 1; i >= 0; i--) {
+        bstr[i] = s;
+        s *= bdims[i];
+      }
+    }
+    NoAllocDesc d{};
+    int64_t     M = 1, N = 1, K = 1;
+    for(int j = 0; j < lc.nm; j++) {
+      TB_EXPECTS(cdims[lc.m_c[j]] == adims[lc.m_a[j]], "A-outer label extents differ (C vs A)");
+      d.a.rdim[j] = (int32_t) adims[lc.m_a[j]];
+      d.a.rstr[j] = (int32_t) astr[lc.m_a[j]];
+      M *= adims[lc.m_a[j]];
+    }
+    for(int j = 0; j < lc.nn; j++) {
+      TB_EXPECTS(cdims[lc.n_c[j]] == bdims[lc.n_b[j]], "B-outer label extents differ (C vs B)");
+      d.b.rdim[j] = (int32_t) bdims[lc.n_b[j]];
+      d.b.rstr[j] = (int32_t) bstr[lc.n_b[j]];
+      N *= bdims[lc.n_b[j]];
+    }
+    for(int j = 0; j < lc.nk; j++) {
+      TB_EXPECTS(adims[lc.k_a[j]] == bdims[lc.k_b[j]], "inner label extents differ (A vs B)");
+      d.a.kdim[j] = d.b.kdim[j] = (int32_t) adims[lc.k_a[j]];
+      d.a.kstr[j] = (int32_t) astr[lc.k_a[j]];
+      d.b.kstr[j] = (int32_t) bstr[lc.k_b[j]];
+      K *= adims[lc.k_a[j]];
+    }
+    TB_EXPECTS(M * K < (1ll << 31) && N * K < (1ll << 31) && M * N < (1ll << 31),
+               "a single block must hold fewer than 2^31 elements");
+    const int64_t Mp = rup(M, MT), Np = rup(N, NT), Kp = rup(K, KC);
+    const int64_t abytes = S * Mp * Kp, bbytes = S * Np * Kp;
+    const int64_t mtiles = Mp / MT, ntiles = Np / NT;
+    const int64_t chunks_off = rup(kCtlItems + 16 * mtiles * ntiles, 256);
+    const int64_t exps_off   = rup(chunks_off + 8 * (Mp / 8 + Np / 8), 256);
+    const int64_t sl_off     = rup(exps_off + 4 * (Mp + Np), 256);
+    const int64_t need       = sl_off + abytes + bbytes;
+    if(need > kNoAllocBytes)
+      fail(TB_ERR_INVALID, "tb_block_multiply_int8_noalloc: this block triple needs " + std::to_string(need) +
+                             " bytes of scratch; the static scratch holds " + std::to_string(kNoAllocBytes) +
+                             " bytes (64 MiB)");
+
+    d.a.src_off = 0;
+    d.a.dst_off = 0;
+    d.a.exp_off = 0;
+    d.a.id      = 0;
+    d.a.rows    = (int32_t) M;
+    d.a.K       = (int32_t) K;
+    d.a.rows_pad  = (int32_t) Mp;
+    d.a.K_pad     = (int32_t) Kp;
+    d.a.tile_rows = MT;
+    d.a.nr        = lc.nm;
+    d.a.nk        = lc.nk;
+    d.a.kcontig   = 1;
+    for(int j = 0; j < lc.nk; j++) d.a.kcontig &= (lc.k_a[j] == na - lc.nk + j) ? 1 : 0;
+    d.b.src_off   = 0;
+    d.b.dst_off   = abytes;
+    d.b.exp_off   = (int32_t) Mp;
+    d.b.id        = 1;
+    d.b.rows      = (int32_t) N;
+    d.b.K         = (int32_t) K;
+    d.b.rows_pad  = (int32_t) Np;
+    d.b.K_pad     = (int32_t) Kp;
+    d.b.tile_rows = NT;
+    d.b.nr        = lc.nn;
+    d.b.nk        = lc.nk;
+    d.b.kcontig   = 1;
+    for(int j = 0; j < lc.nk; j++) d.b.kcontig &= (lc.k_b[j] == nb - lc.nk + j) ? 1 : 0;
+    d.g.c_off      = 0;
+    d.g.task_begin = 0;
+    d.g.task_end   = 1;
+    for(int i = 0; i < nc; i++) d.g.cdims[i] = (int32_t) cdims[i];
+    d.task.a_off = 0;
+    d.task.b_off = abytes;
+    d.task.a_exp = 0;
+    d.task.b_exp = (int32_t) Mp;
+    d.task.nkc   = (int32_t) (Kp / KC);
+    d.meta.a_block = 0;
+    d.meta.b_block = 1;
+    int lk = 0;
+    while((1ll << lk) < K) lk++;
+    d.meta.log2k  = lk;
+    d.mtiles      = (int32_t) mtiles;
+    d.ntiles      = (int32_t) ntiles;
+    d.nchunk_a    = (int32_t) (Mp / 8);
+    d.nchunk_b    = (int32_t) (Np / 8);
+    d.chunks_off  = chunks_off;
+
+    // set-up once per device, with that device current: the device address of the
+    // static scratch (its host-side name is only a stand-in, not a device address)
+    int dev = 0;
+    TB_CUDA(cudaGetDevice(&dev));
+    TB_EXPECTS(dev >= 0 && dev < kNoAllocDevices, "device index out of range");
+    if(g_noalloc_base[dev] == nullptr) {
+      void* ptr = nullptr;
+      TB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+      g_noalloc_base[dev] = ptr;
+    }
+    auto*      base = static_cast<unsigned char*>(g_noalloc_base[dev]);
+    const auto st   = static_cast<cudaStream_t>(stream);
+    switch(S) {
+      case 3: noalloc_launch<3>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+      case 4: noalloc_launch<4>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+      case 5: noalloc_launch<5>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+      case 6: noalloc_launch<6>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+      case 7: noalloc_launch<7>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+      default: noalloc_launch<8>(d, base, exps_off, sl_off, lc, alpha, a, b, c, st); break;
+    }
+    int h = 0;
+    TB_CUDA(cudaMemcpyAsync(&h, base + kCtlErr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TB_CUDA(cudaStreamSynchronize(st));
+    if(h != 0) fail(TB_ERR_TIMEOUT, "split-INT8 contraction: a device-side wait gave up (code " + std::to_string(h) + ")");
+  } catch(const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch(const std::exception& e) {
+    set_last_error(e.what());
+    return TB_ERR_INVALID;
+  }
+  return TB_OK;
+}

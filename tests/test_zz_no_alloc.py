@@ -1,0 +1,95 @@
+"""GPU test of tb_block_multiply_int8_noalloc, the split-INT8 block multiply for callers
+that cannot allocate device memory (their memory already belongs to other allocators,
+or they must avoid the synchronisation a cudaMalloc / cudaFree can cause): it keeps its
+scratch in a fixed 64 MiB device array instead of allocating.
+
+Two calls in a row, on different block shapes, must each match the allocating
+tb_block_multiply in TB_MODE_INT8 within the split-INT8 tolerance of the other tests
+(max |diff| <= 1e-11 * max |product|), so nothing the first call leaves in the shared
+array leaks into the second.  Kept in its own file that pytest collects last."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tamm_b200 import _capi as A
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+INT8_TOL = 1e-11
+
+
+def _i64(v):
+    return np.asarray(list(v) or [0], dtype=np.int64)
+
+
+def _i32(v):
+    return np.asarray(list(v) or [0], dtype=np.int32)
+
+
+def _case(shape, labels, seed):
+    cl, al, bl = labels
+    lab = {c: -ord(c) for c in "abcdijk"}
+    a = np.zeros([shape[c] for c in al])
+    b = np.zeros([shape[c] for c in bl])
+    c0 = np.zeros([shape[c] for c in cl])
+    O.fill_uniform(a.reshape(-1), seed)
+    O.fill_normal(b.reshape(-1), seed + 1, 0, 0.0, 1e-2)
+    O.fill_uniform(c0.reshape(-1), seed + 2)
+    return a, b, c0, [lab[x] for x in al], [lab[x] for x in bl], [lab[x] for x in cl]
+
+
+def _args(a, al, b, bl, c0, cl):
+    da = torch.from_numpy(a.reshape(-1).copy()).cuda()
+    db = torch.from_numpy(b.reshape(-1).copy()).cuda()
+    dc = torch.from_numpy(c0.reshape(-1).copy()).cuda()
+    keep = [_i64(a.shape), _i32(al), _i64(b.shape), _i32(bl), _i64(c0.shape), _i32(cl)]
+    return (da, db, dc), keep
+
+
+def _allocating(alpha, a, al, b, bl, c0, cl):
+    (da, db, dc), k = _args(a, al, b, bl, c0, cl)
+    A.call("tb_block_multiply", alpha, da.data_ptr(), k[0].ctypes.data_as(A.i64p), k[1].ctypes.data_as(A.ip),
+           a.ndim, db.data_ptr(), k[2].ctypes.data_as(A.i64p), k[3].ctypes.data_as(A.ip), b.ndim, 1.0,
+           dc.data_ptr(), k[4].ctypes.data_as(A.i64p), k[5].ctypes.data_as(A.ip), c0.ndim, 0, A.TB_MODE_INT8,
+           C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return dc.cpu().numpy().reshape(c0.shape)
+
+
+def _no_alloc(alpha, a, al, b, bl, c0, cl):
+    (da, db, dc), k = _args(a, al, b, bl, c0, cl)
+    A.call("tb_block_multiply_int8_noalloc", alpha, da.data_ptr(), k[0].ctypes.data_as(A.i64p),
+           k[1].ctypes.data_as(A.ip), a.ndim, db.data_ptr(), k[2].ctypes.data_as(A.i64p),
+           k[3].ctypes.data_as(A.ip), b.ndim, dc.data_ptr(), k[4].ctypes.data_as(A.i64p),
+           k[5].ctypes.data_as(A.ip), c0.ndim, 0, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return dc.cpu().numpy().reshape(c0.shape)
+
+
+def test_no_alloc_matches_allocating_entry_point_two_calls():
+    cases = [
+        (dict(a=24, b=31, c=29, d=37, i=20, j=20), ("abij", "abcd", "cdij"), 41),  # ladder-shaped tile pair
+        (dict(a=13, b=9, c=7, d=5, i=3, j=11), ("ijab", "cadb", "jdci"), 42),      # permuted labels
+    ]
+    for shape, labels, seed in cases:  # two calls in a row on the shared scratch
+        a, b, c0, al, bl, cl = _case(shape, labels, seed)
+        want = _allocating(0.75, a, al, b, bl, c0, cl)
+        got = _no_alloc(0.75, a, al, b, bl, c0, cl)
+        prod = want - c0
+        assert np.max(np.abs(got - want)) <= INT8_TOL * np.max(np.abs(prod))
+
+
+def test_no_alloc_rejects_triples_beyond_the_static_scratch():
+    L = A.lib()
+    dims = _i64([4096, 4096])
+    lab_a, lab_b, lab_c = _i32([-1, -3]), _i32([-3, -2]), _i32([-1, -2])
+    x = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rc = L.tb_block_multiply_int8_noalloc(1.0, x.data_ptr(), dims.ctypes.data_as(A.i64p), lab_a.ctypes.data_as(A.ip),
+                                          2, x.data_ptr(), dims.ctypes.data_as(A.i64p), lab_b.ctypes.data_as(A.ip), 2,
+                                          x.data_ptr(), dims.ctypes.data_as(A.i64p), lab_c.ctypes.data_as(A.ip), 2, 0,
+                                          None)
+    assert rc == A.TB_ERR_INVALID
+    assert "64 MiB" in A.last_error()
