@@ -5,9 +5,11 @@
 // labels in A's order — the Ainter / Binter views of kernels::block_multiply,
 // multiply.hpp:304-330, without materialising them in FP64).  Each row is scaled by
 // a power of two 2^-e (e = exponent of the row's max |x|, per block) and cut into S
-// base-256 digits of the two's-complement integer X = trunc(x * 2^(8S-1-e)):
-//     X = d_0 * 256^(S-1) + d_1 * 256^(S-2) + ... + d_(S-1),
-// d_0 signed (s8), d_1.. unsigned (u8).  A * B is then the sum over digit pairs of
+// balanced base-256 digits of the integer X = round(x * 2^(8S-1-e)), |X| <= 127 * 256^(S-1)
+// (e is raised by one for the rare rows whose max lies within 1/128 below 2^e):
+//     X = d_0 * 256^(S-1) + d_1 * 256^(S-2) + ... + d_(S-1),   every d_i in [-128, 127]
+// (s8; zero-mean digits keep the dropped low-order products unbiased, so their error
+// grows like sqrt(K) instead of K).  A * B is then the sum over digit pairs of
 // exact INT8 x INT8 -> INT32 tensor-core products; pairs (i, j) with equal i + j share
 // one power of two, so the S(S+1)/2 products with i + j <= S - 1 accumulate into S
 // INT32 TMEM accumulators ("diagonals").  After each (A block, B block) task the
@@ -18,7 +20,7 @@
 // Truncation: each operand is exact to 2^-(8S-1) of its row maximum and the dropped
 // pairs (i + j >= S) weigh at most ~S * 2^(2-8S) of row-max x col-max x K.  The slice
 // count is chosen per task: the largest task of an output block gets the S the error
-// target needs (S = 7, 28 INT8 products, for 1e-11), tasks 2^(8m) smaller get S - m,
+// target needs (S = 6, 21 INT8 products, for 1e-11), tasks 2^(8m) smaller get S - m,
 // numerically zero blocks one digit.  This is the error-free splitting of Ozaki,
 // Ogita, Oishi and Rump with the INT8 tensor-core digit layout of Ozaki / Uchino /
 // Imamura's DGEMM emulation.
@@ -96,9 +98,10 @@ __device__ __forceinline__ int32_t koff(const SplitBlock& b, int32_t k) {
   return b.kcontig ? k : decomp(k, b.nk, b.kdim, b.kstr);
 }
 
-// trunc(x * 2^sh) as a two's-complement integer, |result| < 2^63, from the IEEE-754
-// fields (x = m * 2^(E-52) with the 53-bit integer m): a shift of m, no FP64 pipe.
-__device__ __forceinline__ long long scaled_trunc(double x, int sh) {
+// round(x * 2^sh) (half away from zero) as a two's-complement integer, |result| <
+// 2^63, from the IEEE-754 fields (x = m * 2^(E-52) with the 53-bit integer m): a
+// shift of m, no FP64 pipe.
+__device__ __forceinline__ long long scaled_round(double x, int sh) {
   const long long bits = __double_as_longlong(x);
   const int       E    = (int) ((bits >> 52) & 0x7FF);
   const long long frac = bits & 0xFFFFFFFFFFFFFll;
@@ -106,8 +109,35 @@ __device__ __forceinline__ long long scaled_trunc(double x, int sh) {
   const int       s    = (E ? E : 1) - 1075 + sh;         // x * 2^sh = m * 2^s
   long long       v;
   if(s >= 0) v = m << s;
-  else v = (s > -64) ? (m >> (-s)) : 0;
+  else if(s > -63) v = (m + (1ll << (-s - 1))) >> (-s);
+  else v = 0;
   return bits < 0 ? -v : v;
+}
+
+// Balanced base-256 digits of X (|X| <= 127 * 256^(S-1)): d[S-1] .. d[1] are the signed
+// low bytes of the running quotient, d[0] the rest, |d[0]| <= 127.
+template<int S>
+__device__ __forceinline__ void balanced_digits(long long X, int8_t (&d)[S]) {
+#pragma unroll
+  for(int i = S - 1; i > 0; i--) {
+    const int8_t lo = (int8_t) (X & 0xFF);
+    d[i]            = lo;
+    X               = (X - lo) >> 8;
+  }
+  d[0] = (int8_t) X;
+}
+
+constexpr int kPadRow = -0x7fffffff; // shift marker of a padding row (no digits)
+
+// Row exponent e with |x| * 2^-e <= 127/128 for every x of the row, so that
+// round(x * 2^(8S-1-e)) has a leading balanced digit within [-127, 127].
+__device__ __forceinline__ int row_exponent(double mx) {
+  int e = 0;
+  if(mx > 0.0) {
+    const double f = frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1)
+    if(f > 127.0 / 128.0) e += 1;
+  }
+  return e;
 }
 
 // One CTA per 8-row group of one block (the rows of one core-matrix row group):
@@ -138,10 +168,9 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
         for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + koff(b, k))));
 #pragma unroll
       for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      int e = 0;
-      if(mx > 0.0) frexp(mx, &e); // mx = f * 2^e, f in [0.5, 1): |x| < 2^e
+      const int e = row_exponent(mx);
       if(lane == 0) {
-        s_sh[warp]  = live ? 8 * S - 1 - e : -1; // -1: padding row
+        s_sh[warp]  = live ? 8 * S - 1 - e : kPadRow;
         s_off[warp] = rowoff;
         exps[b.exp_off + row] = e;
         if(mx > 0.0) atomicMax(blockmax + b.id, e);
@@ -150,25 +179,24 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
     __syncthreads();
     const int r = lane >> 2, q = lane & 3; // row within the 8-row group, k quad
     const int sh = s_sh[r];
-    const double* s   = src + b.src_off + s_off[r];
+    const double* s   = src + b.src_off + s_off[r];  // digits of X = round(x * 2^sh)
     const int     g8  = (ch.y % b.tile_rows) >> 3;
     const int     nkc = b.K_pad / KC;
     uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
                    q * 4;
     for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) { // one core matrix per warp and step
       const int k0 = k16 * 16 + q * 4;
-      long long X[4];
+      int8_t dg[4][S];
 #pragma unroll
       for(int x = 0; x < 4; x++) {
         const int k = k0 + x;
-        X[x]        = (sh >= 0 && k < b.K) ? scaled_trunc(__ldg(s + koff(b, k)), sh) : 0ll;
+        balanced_digits<S>((sh != kPadRow && k < b.K) ? scaled_round(__ldg(s + koff(b, k)), sh) : 0ll, dg[x]);
       }
       uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * b.tile_rows * 16;
 #pragma unroll
       for(int i = 0; i < S; i++) {
-        const int ds = 8 * (S - 1 - i); // digit i; d_0 keeps the sign bits
-        const uint32_t w = (uint32_t) ((X[0] >> ds) & 0xFF) | ((uint32_t) ((X[1] >> ds) & 0xFF) << 8) |
-                           ((uint32_t) ((X[2] >> ds) & 0xFF) << 16) | ((uint32_t) ((X[3] >> ds) & 0xFF) << 24);
+        const uint32_t w = (uint32_t) (uint8_t) dg[0][i] | ((uint32_t) (uint8_t) dg[1][i] << 8) |
+                           ((uint32_t) (uint8_t) dg[2][i] << 16) | ((uint32_t) (uint8_t) dg[3][i] << 24);
         *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w;
       }
     }
@@ -176,21 +204,120 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
   }
 }
 
+// Same digits as k_split, with the operand read from HBM once: each half of an
+// 8-row chunk (4 rows) is staged in shared memory with coalesced loads while the row
+// maxima are formed, then converted from shared memory (one 16-k group of the 4 rows
+// per warp and step: 2 bytes per thread and slice, 64 contiguous bytes per warp).
+// Shared memory: 4 * K_pad doubles (K_pad <= kStagedMaxK).
+constexpr int kStagedMaxK = 3072;
+
+template<int S>
+__global__ void __launch_bounds__(256) k_split_staged(const SplitBlock* __restrict__ blocks,
+                                                      const int2* __restrict__ chunks, int nchunks,
+                                                      const double* __restrict__ src,
+                                                      uint8_t* __restrict__ dst, int32_t* __restrict__ exps,
+                                                      int32_t* __restrict__ blockmax) {
+  extern __shared__ double srow[]; // [4][K_pad]
+  __shared__ double        s_red[8][4];
+  __shared__ int           s_sh[4];
+  const int                tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int2       ch = chunks[c];
+    const SplitBlock b  = blocks[ch.x];
+    const int        Kp = b.K_pad;
+    for(int half = 0; half < 2; half++) {
+      const int row0 = ch.y + 4 * half;
+#pragma unroll
+      for(int r = 0; r < 4; r++) {
+        const bool    live   = row0 + r < b.rows;
+        const int32_t rowoff = live ? decomp(row0 + r, b.nr, b.rdim, b.rstr) : 0;
+        const double* s      = src + b.src_off + rowoff;
+        double        mx     = 0.0;
+        for(int k = tid; k < Kp; k += 256) {
+          const double v = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
+          srow[r * Kp + k] = v;
+          mx               = fmax(mx, fabs(v));
+        }
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if(lane == 0) s_red[warp][r] = mx;
+      }
+      __syncthreads();
+      if(tid < 4) {
+        double mx = 0.0;
+        for(int w = 0; w < 8; w++) mx = fmax(mx, s_red[w][tid]);
+        const int e   = row_exponent(mx);
+        const int row = row0 + tid;
+        s_sh[tid]     = row < b.rows ? 8 * S - 1 - e : kPadRow;
+        exps[b.exp_off + row] = e;
+        if(mx > 0.0) atomicMax(blockmax + b.id, e);
+      }
+      __syncthreads();
+      // One 32-byte K chunk of the 4 rows per warp and step: thread (row r, quad q)
+      // converts k = 4q..4q+3 and writes 4 bytes per slice.  Y = round(x * 2^sh) +
+      // 0x80..80 has plain base-256 bytes u_i, and the balanced digits are u_i - 128,
+      // i.e. the bytes of Y with the top bit flipped: gathered 4 at a time by PRMT.
+      const int r = lane >> 3, q = lane & 7;
+      const int sh  = s_sh[r];
+      const int rin = row0 % b.tile_rows + r; // row within the tile
+      // 2^sh as two factors, so that no factor overflows for extreme row exponents
+      const double   f1   = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
+      const uint64_t bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
+      uint8_t* out = dst + b.dst_off + (int64_t) (row0 / b.tile_rows) * (Kp / KC) * S * b.tile_rows * KC +
+                     ((4 * q) >> 4) * b.tile_rows * 16 + (rin >> 3) * 128 + (rin & 7) * 16 + ((4 * q) & 15);
+      for(int kc = warp; kc < Kp / KC; kc += 8) {
+        const double2 v01 = *reinterpret_cast<const double2*>(srow + r * Kp + kc * KC + 4 * q);
+        const double2 v23 = *reinterpret_cast<const double2*>(srow + r * Kp + kc * KC + 4 * q + 2);
+        const double  v[4] = {v01.x, v01.y, v23.x, v23.y};
+        uint32_t      lo[4], hi[4];
+#pragma unroll
+        for(int x = 0; x < 4; x++) {
+          const uint64_t Y = (uint64_t) (sh != kPadRow ? __double2ll_rn(v[x] * f1 * f2) : 0ll) + bias;
+          lo[x]            = (uint32_t) Y;
+          hi[x]            = (uint32_t) (Y >> 32);
+        }
+        uint8_t* o = out + (int64_t) kc * S * b.tile_rows * KC;
+#pragma unroll
+        for(int i = 0; i < S; i++) {
+          const int p = S - 1 - i; // byte of Y holding digit i
+          uint32_t  w;
+          if(p < 4) {
+            const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
+            const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          else {
+            const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
+            const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w ^ 0x80808080u;
+        }
+      }
+      __syncthreads(); // srow is refilled by the next half / chunk
+    }
+  }
+}
+
 // Slice count per task: a task whose largest possible product (2^(maxexp A + maxexp
 // B) * K) is 2^(8m) below the largest of its output group needs m fewer digits for
 // the same absolute truncation error; numerically zero blocks keep one digit.
+// One warp per output group, lanes over its tasks.
 __global__ void k_task_slices(const I8TaskMeta* __restrict__ meta, const DevGroup* __restrict__ groups,
                               int ngroups, const int32_t* __restrict__ blockmax, int smax,
                               uint8_t* __restrict__ tslices) {
-  for(int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ngroups; gi += gridDim.x * blockDim.x) {
-    constexpr int  kNone = -1000000; // blockmax slots start at 0x80808080 (no nonzero row)
-    const DevGroup g     = groups[gi];
-    int            eg    = kNone;
-    for(int t = g.task_begin; t < g.task_end; t++) {
+  constexpr int kNone = -1000000; // blockmax slots start at 0x80808080 (no nonzero row)
+  const int     lane  = threadIdx.x & 31;
+  for(int gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < ngroups; gi += (gridDim.x * blockDim.x) >> 5) {
+    const DevGroup g  = groups[gi];
+    int            eg = kNone;
+    for(int t = g.task_begin + lane; t < g.task_end; t += 32) {
       const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
       if(ea > kNone && eb > kNone) eg = max(eg, ea + eb + meta[t].log2k);
     }
-    for(int t = g.task_begin; t < g.task_end; t++) {
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) eg = max(eg, __shfl_xor_sync(0xffffffffu, eg, o));
+    for(int t = g.task_begin + lane; t < g.task_end; t += 32) {
       const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
       int       s  = 1;
       if(ea > kNone && eb > kNone) s = max(1, smax - (eg - (ea + eb + meta[t].log2k)) / 8);
@@ -307,7 +434,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                 const int      j  = d - i;
                 const uint64_t ad = umma_desc_kmajor(a0 + i * MT * KC, MT * 16, 128);
                 const uint64_t bd = umma_desc_kmajor(b0 + j * NT * KC, NT * 16, 128);
-                mma_i8(tmem + d * NT, ad, bd, idesc_i8(MT, NT, i == 0, j == 0), kc > 0 || i > 0);
+                mma_i8(tmem + d * NT, ad, bd, idesc_i8(MT, NT, true, true), kc > 0 || i > 0);
               }
             }
             if(kc == 0) // keep the unused diagonals' barriers in phase
@@ -445,6 +572,7 @@ struct I8Layout {
   std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
   int64_t                 slice_bytes = 0, a_bytes = 0;
+  int32_t                 a_maxkp = 0, b_maxkp = 0; // largest K_pad of the A / B blocks
   int64_t                 nexp = 0, a_nexp = 0;
   double                  int8_ops = 0;
   SplitBlock*             d_ablocks = nullptr;
@@ -601,6 +729,8 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   chunks(L->a_blocks, L->a_chunks);
   chunks(L->b_blocks, L->b_chunks);
+  for(const auto& b: L->a_blocks) L->a_maxkp = std::max(L->a_maxkp, b.K_pad);
+  for(const auto& b: L->b_blocks) L->b_maxkp = std::max(L->b_maxkp, b.K_pad);
   // output tiles, longest first
   std::vector<std::pair<int64_t, I8Item>> v;
   for(size_t gi = 0; gi < wl.groups.size(); gi++) {
@@ -653,15 +783,23 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
   const int grid_cap = sm_count() * 8;
   // 0x80808080: below every exponent sum, marks blocks without a nonzero row
   TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
-  if(!L.a_chunks.empty())
-    k_split<S><<<std::min<int64_t>((int64_t) L.a_chunks.size(), grid_cap), 256, 0, st>>>(
-      L.d_ablocks, L.d_achunks, (int) L.a_chunks.size(), A, slices, exps, L.d_blockmax);
-  if(!L.b_chunks.empty())
-    k_split<S><<<std::min<int64_t>((int64_t) L.b_chunks.size(), grid_cap), 256, 0, st>>>(
-      L.d_bblocks, L.d_bchunks, (int) L.b_chunks.size(), B, slices, exps, L.d_blockmax);
+  auto one = [&](const SplitBlock* blocks, const int2* chunks, size_t nchunks, int32_t maxkp, const double* src) {
+    if(nchunks == 0) return;
+    if(maxkp <= kStagedMaxK) { // operand read once, staged through shared memory
+      const size_t smem = sizeof(double) * 4 * (size_t) maxkp;
+      TB_CUDA(cudaFuncSetAttribute(k_split_staged<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+      k_split_staged<S><<<std::min<int64_t>((int64_t) nchunks, grid_cap), 256, smem, st>>>(
+        blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
+    }
+    else
+      k_split<S><<<std::min<int64_t>((int64_t) nchunks, grid_cap), 256, 0, st>>>(blocks, chunks, (int) nchunks,
+                                                                                 src, slices, exps, L.d_blockmax);
+  };
+  one(L.d_ablocks, L.d_achunks, L.a_chunks.size(), L.a_maxkp, A);
+  one(L.d_bblocks, L.d_bchunks, L.b_chunks.size(), L.b_maxkp, B);
   const int ng = (int) wl.groups.size();
   if(ng > 0)
-    k_task_slices<<<(ng + 255) / 256, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
+    k_task_slices<<<(ng + 7) / 8, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -706,12 +844,13 @@ void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double
 }
 
 // Largest slice count for an error target: the truncation bound S * 2^(2 - 8S) of
-// row-max x col-max x K, times 2^10 for the cancellation between that scale and the
-// largest |C| seen on coupled-cluster data (O=40/V=360 ladder: S = 6 -> 1.1e-10,
-// S = 7 -> 4e-13 measured); smallest S meeting the target.
+// row-max x col-max x K, times 2^6 for the cancellation between that scale and the
+// largest |C| seen on coupled-cluster data (O=40/V=360 ladder, balanced digits:
+// S = 5 -> 6.3e-10, S = 6 -> 2.9e-12, S = 7 -> 1.4e-14 measured); smallest S meeting
+// the target.
 int slices_for(double err_target) {
   for(int S = 3; S <= 8; S++)
-    if(S * std::ldexp(1.0, 2 - 8 * S) * 1024.0 <= err_target) return S;
+    if(S * std::ldexp(1.0, 2 - 8 * S) * 64.0 <= err_target) return S;
   return 8;
 }
 
