@@ -100,7 +100,7 @@ def test_int8_cholesky_ladder_with_zero_spin_blocks(ec):
     finally:
         ec.set_precision(tb.Precision.FP64)
     assert rel_err(lad.r2.read(), orr.data[:orr.total]) <= INT8_TOL
-    assert st["slices_min"] == 1 and st["slices_max"] == 7
+    assert st["slices_min"] == 1 and st["slices_max"] == 6  # 1e-11 needs 6 digits
 
 
 def test_int8_slice_count_controls_error(ec):
