@@ -204,98 +204,128 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
   }
 }
 
-// Same digits as k_split, with the operand read from HBM once: each half of an
-// 8-row chunk (4 rows) is staged in shared memory with coalesced loads while the row
-// maxima are formed, then converted from shared memory (one 16-k group of the 4 rows
-// per warp and step: 2 bytes per thread and slice, 64 contiguous bytes per warp).
-// Shared memory: 4 * K_pad doubles (K_pad <= kStagedMaxK).
-constexpr int kStagedMaxK = 3072;
-
+// Split in one pass over HBM: one CTA per 8-row group.  Phase 1, warp w streams row w
+// (16-byte loads from the row's first 16-byte boundary, four in flight per lane) for
+// its max |x| and row exponent; phase 2 re-reads the 8 rows, now resident in L2, one
+// 8-row x 16-k core matrix per warp and step: thread (row r, quad q) turns k =
+// 4q..4q+3 into Y = round(x * 2^(8S-1-e)) + 0x80..80, whose plain base-256 bytes are
+// the balanced digits + 128.  The bytes of 4 values are gathered per slice with PRMT,
+// flipped back with one XOR and stored as one 4-byte word, so every warp store is a
+// contiguous 128-byte core matrix.  Residency (four CTAs per SM at 60 registers)
+// bounds the rows held in L2 between the phases to 4 x 148 x 8 rows (87 MB at K =
+// 2304, within the 126 MB L2).
 template<int S>
-__global__ void __launch_bounds__(256) k_split_staged(const SplitBlock* __restrict__ blocks,
-                                                      const int2* __restrict__ chunks, int nchunks,
-                                                      const double* __restrict__ src,
-                                                      uint8_t* __restrict__ dst, int32_t* __restrict__ exps,
-                                                      int32_t* __restrict__ blockmax) {
-  extern __shared__ double srow[]; // [4][K_pad]
-  __shared__ double        s_red[8][4];
-  __shared__ int           s_sh[4];
-  const int                tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+__global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restrict__ blocks,
+                                                     const int2* __restrict__ chunks, int nchunks,
+                                                     const double* __restrict__ src, uint8_t* __restrict__ dst,
+                                                     int32_t* __restrict__ exps, int32_t* __restrict__ blockmax) {
+  __shared__ int     s_sh[8];
+  __shared__ int32_t s_off[8];
+  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t     bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
   for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const int2       ch = chunks[c];
     const SplitBlock b  = blocks[ch.x];
-    const int        Kp = b.K_pad;
-    for(int half = 0; half < 2; half++) {
-      const int row0 = ch.y + 4 * half;
+    {
+      const int     row    = ch.y + warp;
+      const bool    live   = row < b.rows;
+      const int32_t rowoff = live ? decomp(row, b.nr, b.rdim, b.rstr) : 0;
+      double        mx     = 0.0;
+      if(live) {
+        const double* s = src + b.src_off + rowoff;
+        double        m[8];
 #pragma unroll
-      for(int r = 0; r < 4; r++) {
-        const bool    live   = row0 + r < b.rows;
-        const int32_t rowoff = live ? decomp(row0 + r, b.nr, b.rdim, b.rstr) : 0;
-        const double* s      = src + b.src_off + rowoff;
-        double        mx     = 0.0;
-        for(int k = tid; k < Kp; k += 256) {
-          const double v = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
-          srow[r * Kp + k] = v;
-          mx               = fmax(mx, fabs(v));
+        for(int x = 0; x < 8; x++) m[x] = 0.0;
+        if(b.kcontig) {
+          // 16-byte loads from the first 16-byte boundary of the row on
+          const int      p0 = (reinterpret_cast<uintptr_t>(s) & 15) ? 1 : 0;
+          const int      np = (b.K - p0) >> 1;
+          const double2* s2 = reinterpret_cast<const double2*>(s + p0);
+          int            k  = lane;
+          for(; k + 96 < np; k += 128) {
+            double2 t[4];
+#pragma unroll
+            for(int x = 0; x < 4; x++) t[x] = __ldg(s2 + k + 32 * x);
+#pragma unroll
+            for(int x = 0; x < 4; x++) {
+              m[2 * x]     = fmax(m[2 * x], fabs(t[x].x));
+              m[2 * x + 1] = fmax(m[2 * x + 1], fabs(t[x].y));
+            }
+          }
+          for(; k < np; k += 32) {
+            const double2 t = __ldg(s2 + k);
+            m[0]            = fmax(m[0], fmax(fabs(t.x), fabs(t.y)));
+          }
+          if(lane == 0 && p0) m[1] = fmax(m[1], fabs(__ldg(s)));
+          if(lane == 1 && p0 + 2 * np < b.K) m[1] = fmax(m[1], fabs(__ldg(s + b.K - 1)));
         }
+        else
+          for(int k = lane; k < b.K; k += 32) m[0] = fmax(m[0], fabs(__ldg(s + koff(b, k))));
 #pragma unroll
-        for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if(lane == 0) s_red[warp][r] = mx;
+        for(int x = 0; x < 8; x++) mx = fmax(mx, m[x]);
       }
-      __syncthreads();
-      if(tid < 4) {
-        double mx = 0.0;
-        for(int w = 0; w < 8; w++) mx = fmax(mx, s_red[w][tid]);
-        const int e   = row_exponent(mx);
-        const int row = row0 + tid;
-        s_sh[tid]     = row < b.rows ? 8 * S - 1 - e : kPadRow;
+#pragma unroll
+      for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if(lane == 0) {
+        const int e = row_exponent(mx);
+        s_sh[warp]  = live ? 8 * S - 1 - e : kPadRow;
+        s_off[warp] = rowoff;
         exps[b.exp_off + row] = e;
         if(mx > 0.0) atomicMax(blockmax + b.id, e);
       }
-      __syncthreads();
-      // One 32-byte K chunk of the 4 rows per warp and step: thread (row r, quad q)
-      // converts k = 4q..4q+3 and writes 4 bytes per slice.  Y = round(x * 2^sh) +
-      // 0x80..80 has plain base-256 bytes u_i, and the balanced digits are u_i - 128,
-      // i.e. the bytes of Y with the top bit flipped: gathered 4 at a time by PRMT.
-      const int r = lane >> 3, q = lane & 7;
-      const int sh  = s_sh[r];
-      const int rin = row0 % b.tile_rows + r; // row within the tile
-      // 2^sh as two factors, so that no factor overflows for extreme row exponents
-      const double   f1   = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
-      const uint64_t bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
-      uint8_t* out = dst + b.dst_off + (int64_t) (row0 / b.tile_rows) * (Kp / KC) * S * b.tile_rows * KC +
-                     ((4 * q) >> 4) * b.tile_rows * 16 + (rin >> 3) * 128 + (rin & 7) * 16 + ((4 * q) & 15);
-      for(int kc = warp; kc < Kp / KC; kc += 8) {
-        const double2 v01 = *reinterpret_cast<const double2*>(srow + r * Kp + kc * KC + 4 * q);
-        const double2 v23 = *reinterpret_cast<const double2*>(srow + r * Kp + kc * KC + 4 * q + 2);
-        const double  v[4] = {v01.x, v01.y, v23.x, v23.y};
-        uint32_t      lo[4], hi[4];
+    }
+    __syncthreads();
+    const int     r = lane >> 2, q = lane & 3; // row within the 8-row group, k quad
+    const int     sh   = s_sh[r];
+    const bool    live = sh != kPadRow;
+    const double* s    = src + b.src_off + s_off[r];
+    // 2^sh as two factors, so that no factor overflows for extreme row exponents
+    const double f1  = ldexp(1.0, live ? sh / 2 : 0), f2 = ldexp(1.0, live ? sh - sh / 2 : 0);
+    const int    g8  = (ch.y % b.tile_rows) >> 3;
+    const int    nkc = b.K_pad / KC;
+    uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
+                   q * 4;
+    const bool vec = live && b.kcontig && !(reinterpret_cast<uintptr_t>(s) & 15);
+    for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) {
+      const int k0 = k16 * 16 + q * 4;
+      double    v[4];
+      if(vec && k0 + 3 < b.K) {
+        const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
+        const double2 v23 = __ldg(reinterpret_cast<const double2*>(s + k0 + 2));
+        v[0] = v01.x, v[1] = v01.y, v[2] = v23.x, v[3] = v23.y;
+      }
+      else
 #pragma unroll
         for(int x = 0; x < 4; x++) {
-          const uint64_t Y = (uint64_t) (sh != kPadRow ? __double2ll_rn(v[x] * f1 * f2) : 0ll) + bias;
-          lo[x]            = (uint32_t) Y;
-          hi[x]            = (uint32_t) (Y >> 32);
+          const int k = k0 + x;
+          v[x]        = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
         }
-        uint8_t* o = out + (int64_t) kc * S * b.tile_rows * KC;
+      uint32_t lo[4], hi[4];
 #pragma unroll
-        for(int i = 0; i < S; i++) {
-          const int p = S - 1 - i; // byte of Y holding digit i
-          uint32_t  w;
-          if(p < 4) {
-            const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
-            const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
-            w                 = __byte_perm(t0, t1, 0x5410);
-          }
-          else {
-            const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
-            const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
-            w                 = __byte_perm(t0, t1, 0x5410);
-          }
-          *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w ^ 0x80808080u;
-        }
+      for(int x = 0; x < 4; x++) {
+        const uint64_t Y = (uint64_t) __double2ll_rn(v[x] * f1 * f2) + bias;
+        lo[x]            = (uint32_t) Y;
+        hi[x]            = (uint32_t) (Y >> 32);
       }
-      __syncthreads(); // srow is refilled by the next half / chunk
+      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * b.tile_rows * 16;
+#pragma unroll
+      for(int i = 0; i < S; i++) {
+        const int p = S - 1 - i; // byte of Y holding digit i
+        uint32_t  w;
+        if(p < 4) {
+          const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
+          const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
+          w                 = __byte_perm(t0, t1, 0x5410);
+        }
+        else {
+          const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
+          const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
+          w                 = __byte_perm(t0, t1, 0x5410);
+        }
+        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w ^ 0x80808080u;
+      }
     }
+    __syncthreads(); // s_sh / s_off are rewritten for the next chunk
   }
 }
 
@@ -572,7 +602,6 @@ struct I8Layout {
   std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
   int64_t                 slice_bytes = 0, a_bytes = 0;
-  int32_t                 a_maxkp = 0, b_maxkp = 0; // largest K_pad of the A / B blocks
   int64_t                 nexp = 0, a_nexp = 0;
   double                  int8_ops = 0;
   SplitBlock*             d_ablocks = nullptr;
@@ -729,8 +758,6 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   chunks(L->a_blocks, L->a_chunks);
   chunks(L->b_blocks, L->b_chunks);
-  for(const auto& b: L->a_blocks) L->a_maxkp = std::max(L->a_maxkp, b.K_pad);
-  for(const auto& b: L->b_blocks) L->b_maxkp = std::max(L->b_maxkp, b.K_pad);
   // output tiles, longest first
   std::vector<std::pair<int64_t, I8Item>> v;
   for(size_t gi = 0; gi < wl.groups.size(); gi++) {
@@ -783,20 +810,13 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
   const int grid_cap = sm_count() * 8;
   // 0x80808080: below every exponent sum, marks blocks without a nonzero row
   TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
-  auto one = [&](const SplitBlock* blocks, const int2* chunks, size_t nchunks, int32_t maxkp, const double* src) {
+  auto one = [&](const SplitBlock* blocks, const int2* chunks, size_t nchunks, const double* src) {
     if(nchunks == 0) return;
-    if(maxkp <= kStagedMaxK) { // operand read once, staged through shared memory
-      const size_t smem = sizeof(double) * 4 * (size_t) maxkp;
-      TB_CUDA(cudaFuncSetAttribute(k_split_staged<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-      k_split_staged<S><<<std::min<int64_t>((int64_t) nchunks, grid_cap), 256, smem, st>>>(
-        blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
-    }
-    else
-      k_split<S><<<std::min<int64_t>((int64_t) nchunks, grid_cap), 256, 0, st>>>(blocks, chunks, (int) nchunks,
-                                                                                 src, slices, exps, L.d_blockmax);
+    const int grid = (int) std::min<int64_t>((int64_t) nchunks, grid_cap);
+    k_split_fused<S><<<grid, 256, 0, st>>>(blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
   };
-  one(L.d_ablocks, L.d_achunks, L.a_chunks.size(), L.a_maxkp, A);
-  one(L.d_bblocks, L.d_bchunks, L.b_chunks.size(), L.b_maxkp, B);
+  one(L.d_ablocks, L.d_achunks, L.a_chunks.size(), A);
+  one(L.d_bblocks, L.d_bchunks, L.b_chunks.size(), B);
   const int ng = (int) wl.groups.size();
   if(ng > 0)
     k_task_slices<<<(ng + 7) / 8, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
