@@ -98,35 +98,6 @@ __device__ __forceinline__ int32_t koff(const SplitBlock& b, int32_t k) {
   return b.kcontig ? k : decomp(k, b.nk, b.kdim, b.kstr);
 }
 
-// round(x * 2^sh) (half away from zero) as a two's-complement integer, |result| <
-// 2^63, from the IEEE-754 fields (x = m * 2^(E-52) with the 53-bit integer m): a
-// shift of m, no FP64 pipe.
-__device__ __forceinline__ long long scaled_round(double x, int sh) {
-  const long long bits = __double_as_longlong(x);
-  const int       E    = (int) ((bits >> 52) & 0x7FF);
-  const long long frac = bits & 0xFFFFFFFFFFFFFll;
-  const long long m    = E ? (frac | (1ll << 52)) : frac; // subnormals: no hidden bit
-  const int       s    = (E ? E : 1) - 1075 + sh;         // x * 2^sh = m * 2^s
-  long long       v;
-  if(s >= 0) v = m << s;
-  else if(s > -63) v = (m + (1ll << (-s - 1))) >> (-s);
-  else v = 0;
-  return bits < 0 ? -v : v;
-}
-
-// Balanced base-256 digits of X (|X| <= 127 * 256^(S-1)): d[S-1] .. d[1] are the signed
-// low bytes of the running quotient, d[0] the rest, |d[0]| <= 127.
-template<int S>
-__device__ __forceinline__ void balanced_digits(long long X, int8_t (&d)[S]) {
-#pragma unroll
-  for(int i = S - 1; i > 0; i--) {
-    const int8_t lo = (int8_t) (X & 0xFF);
-    d[i]            = lo;
-    X               = (X - lo) >> 8;
-  }
-  d[0] = (int8_t) X;
-}
-
 constexpr int kPadRow = -0x7fffffff; // shift marker of a padding row (no digits)
 
 // Row exponent e with |x| * 2^-e <= 127/128 for every x of the row, so that
@@ -140,70 +111,6 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return e;
 }
 
-// One CTA per 8-row group of one block (the rows of one core-matrix row group):
-// warp w finds the max |x| of row w (exponent e_w), then the CTA emits the S
-// base-256 digits of X = trunc(x * 2^(8S-1-e)) one 8-row x 16-k core matrix per warp
-// and step: thread (row r, quad q) converts k = 4q..4q+3 of its row and writes 4
-// bytes per digit slice, so each warp store is one contiguous 128-byte core matrix.
-// Padding rows / columns get zero digits.  blockmax[b] collects the largest row
-// exponent of each block (rows that are entirely zero do not count).
-template<int S>
-__global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ blocks,
-                                               const int2* __restrict__ chunks, int nchunks,
-                                               const double* __restrict__ src, uint8_t* __restrict__ dst,
-                                               int32_t* __restrict__ exps, int32_t* __restrict__ blockmax) {
-  __shared__ int     s_sh[8];
-  __shared__ int32_t s_off[8];
-  const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
-    const int2       ch = chunks[c];
-    const SplitBlock b  = blocks[ch.x];
-    {
-      const int     row    = ch.y + warp;
-      const bool    live   = row < b.rows;
-      const int32_t rowoff = live ? decomp(row, b.nr, b.rdim, b.rstr) : 0;
-      const double* s      = src + b.src_off + rowoff;
-      double        mx     = 0.0;
-      if(live)
-        for(int k = lane; k < b.K; k += 32) mx = fmax(mx, fabs(__ldg(s + koff(b, k))));
-#pragma unroll
-      for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      const int e = row_exponent(mx);
-      if(lane == 0) {
-        s_sh[warp]  = live ? 8 * S - 1 - e : kPadRow;
-        s_off[warp] = rowoff;
-        exps[b.exp_off + row] = e;
-        if(mx > 0.0) atomicMax(blockmax + b.id, e);
-      }
-    }
-    __syncthreads();
-    const int r = lane >> 2, q = lane & 3; // row within the 8-row group, k quad
-    const int sh = s_sh[r];
-    const double* s   = src + b.src_off + s_off[r];  // digits of X = round(x * 2^sh)
-    const int     g8  = (ch.y % b.tile_rows) >> 3;
-    const int     nkc = b.K_pad / KC;
-    uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
-                   q * 4;
-    for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) { // one core matrix per warp and step
-      const int k0 = k16 * 16 + q * 4;
-      int8_t dg[4][S];
-#pragma unroll
-      for(int x = 0; x < 4; x++) {
-        const int k = k0 + x;
-        balanced_digits<S>((sh != kPadRow && k < b.K) ? scaled_round(__ldg(s + koff(b, k)), sh) : 0ll, dg[x]);
-      }
-      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * b.tile_rows * 16;
-#pragma unroll
-      for(int i = 0; i < S; i++) {
-        const uint32_t w = (uint32_t) (uint8_t) dg[0][i] | ((uint32_t) (uint8_t) dg[1][i] << 8) |
-                           ((uint32_t) (uint8_t) dg[2][i] << 16) | ((uint32_t) (uint8_t) dg[3][i] << 24);
-        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w;
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // Split in one pass over HBM: one CTA per 8-row group.  Phase 1, warp w streams row w
 // (16-byte loads from the row's first 16-byte boundary, four in flight per lane) for
 // its max |x| and row exponent; phase 2 re-reads the 8 rows, now resident in L2, one
@@ -211,7 +118,10 @@ __global__ void __launch_bounds__(256) k_split(const SplitBlock* __restrict__ bl
 // 4q..4q+3 into Y = round(x * 2^(8S-1-e)) + 0x80..80, whose plain base-256 bytes are
 // the balanced digits + 128.  The bytes of 4 values are gathered per slice with PRMT,
 // flipped back with one XOR and stored as one 4-byte word, so every warp store is a
-// contiguous 128-byte core matrix.  Residency (four CTAs per SM at 60 registers)
+// contiguous 128-byte core matrix.
+// Slice layout per 32-byte K chunk of a tile: [K half (16 bytes)][digit][row][16 bytes],
+// i.e. the S digits' core matrices of one K half follow each other, so that the digits
+// j0..j1 of a B tile form one UMMA operand of (j1 - j0 + 1) x NT rows.  Residency (four CTAs per SM at 60 registers)
 // bounds the rows held in L2 between the phases to 4 x 148 x 8 rows (87 MB at K =
 // 2304, within the 126 MB L2).
 template<int S>
@@ -307,7 +217,7 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
         lo[x]            = (uint32_t) Y;
         hi[x]            = (uint32_t) (Y >> 32);
       }
-      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * b.tile_rows * 16;
+      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
 #pragma unroll
       for(int i = 0; i < S; i++) {
         const int p = S - 1 - i; // byte of Y holding digit i
@@ -322,7 +232,7 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
           const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
           w                 = __byte_perm(t0, t1, 0x5410);
         }
-        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * KC) = w ^ 0x80808080u;
+        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * 16) = w ^ 0x80808080u;
       }
     }
     __syncthreads(); // s_sh / s_off are rewritten for the next chunk
@@ -385,6 +295,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   static_assert(S * NT <= 512, "TMEM holds 512 columns");
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr uint32_t A_BYTES = S * MT * KC, B_BYTES = S * NT * KC, STAGE = A_BYTES + B_BYTES;
+  constexpr int      kStack  = 256 / NT; // B digits per MMA (UMMA N <= 256)
   uint64_t*          full   = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE);
   uint64_t*          empty  = full + STAGES;
   uint64_t*          tfull  = empty + STAGES;
@@ -421,12 +332,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           const uint8_t* ga = p.slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
           const uint8_t* gb = p.slices + tk.b_off + (int64_t) item.nt * tk.nkc * B_BYTES;
           const uint32_t st = p.tslices[t]; // only the task's leading digits travel
-          const uint32_t ab = st * MT * KC, bb = st * NT * KC;
+          const uint32_t ab = st * MT * 16, bb = st * NT * 16; // per K half
           for(int kc = 0; kc < tk.nkc; kc++) {
             if(!mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) goto done_producer;
-            mbar_arrive_expect_tx(&full[stage], ab + bb);
-            bulk_g2s(smem + stage * STAGE, ga + (int64_t) kc * A_BYTES, ab, &full[stage]);
-            bulk_g2s(smem + stage * STAGE + A_BYTES, gb + (int64_t) kc * B_BYTES, bb, &full[stage]);
+            mbar_arrive_expect_tx(&full[stage], 2 * (ab + bb));
+            uint8_t*       sa = smem + stage * STAGE;
+            const uint8_t* ka = ga + (int64_t) kc * A_BYTES;
+            const uint8_t* kb = gb + (int64_t) kc * B_BYTES;
+            if(st == S) { // both K halves in one copy per operand
+              bulk_g2s(sa, ka, A_BYTES, &full[stage]);
+              bulk_g2s(sa + A_BYTES, kb, B_BYTES, &full[stage]);
+            }
+            else
+              for(int h = 0; h < 2; h++) {
+                bulk_g2s(sa + h * (A_BYTES / 2), ka + h * (A_BYTES / 2), ab, &full[stage]);
+                bulk_g2s(sa + A_BYTES + h * (B_BYTES / 2), kb + h * (B_BYTES / 2), bb, &full[stage]);
+              }
             if(++stage == STAGES) {
               stage = 0;
               phase ^= 1;
@@ -438,7 +359,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
     }
   }
   else if(warp == 1) {
-    // ---------------- MMA issuer: S(S+1)/2 digit products per K step --------------
+    // ------- MMA issuer: S(S+1)/2 digit products per K step in stacked-B MMAs --------
     if(elect_one()) {
       int      stage = 0;
       uint32_t phase = 0, tphase = 0;
@@ -452,24 +373,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
             if(!mbar_wait(&full[stage], phase, p.err, 3)) goto done_mma;
             tc_fence_after();
             const uint32_t a0 = smem_u32(smem + stage * STAGE), b0 = a0 + A_BYTES;
+            // A digit i times the stacked B digits j0 .. j0 + nd - 1 in one MMA of N =
+            // nd * NT: it adds into the adjacent diagonals i + j0 .. i + j0 + nd - 1
+            int waited = 0; // diagonals taken back from the epilogue (first K step)
 #pragma unroll
-            for(int d = 0; d < S; d++) {
-              if(d >= st) break;
-              if(kc == 0) { // diagonal d of the previous task must have been read out
-                if(!mbar_wait(&tempty[d], tphase ^ 1, p.err, 2)) goto done_mma;
-                tc_fence_after();
-              }
+            for(int i = 0; i < S; i++) {
+              if(i >= st) break;
+              const uint64_t ad = umma_desc_kmajor(a0 + i * MT * 16, S * MT * 16, 128);
 #pragma unroll
-              for(int i = 0; i <= d; i++) {
-                const int      j  = d - i;
-                const uint64_t ad = umma_desc_kmajor(a0 + i * MT * KC, MT * 16, 128);
-                const uint64_t bd = umma_desc_kmajor(b0 + j * NT * KC, NT * 16, 128);
-                mma_i8(tmem + d * NT, ad, bd, idesc_i8(MT, NT, true, true), kc > 0 || i > 0);
+              for(int j0 = 0; j0 < S; j0 += kStack) {
+                if(j0 >= st - i) break;
+                const int nd = min(kStack, st - i - j0);
+                if(kc == 0) // the previous task's diagonals must have been read out
+                  for(; waited <= i + j0 + nd - 1; waited++) {
+                    if(!mbar_wait(&tempty[waited], tphase ^ 1, p.err, 2)) goto done_mma;
+                    tc_fence_after();
+                  }
+                const uint64_t bd = umma_desc_kmajor(b0 + j0 * NT * 16, S * NT * 16, 128);
+                mma_i8(tmem + (i + j0) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), kc > 0 || i > 0);
               }
             }
             if(kc == 0) // keep the unused diagonals' barriers in phase
-              for(int d = st; d < S; d++)
-                if(!mbar_wait(&tempty[d], tphase ^ 1, p.err, 2)) goto done_mma;
+              for(; waited < S; waited++)
+                if(!mbar_wait(&tempty[waited], tphase ^ 1, p.err, 2)) goto done_mma;
             umma_commit(&empty[stage]); // stage free once these MMAs have read it
             if(++stage == STAGES) {
               stage = 0;
@@ -1043,8 +969,8 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   uint8_t*      sl   = base + slices_off;
   k_noalloc_setup<<<8, 256, 0, st>>>(d, base);
   const int cap = sm_count() * 8;
-  k_split<S><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
-  k_split<S><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
+  k_split_fused<S><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
+  k_split_fused<S><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
   k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
   I8Params p;
   p.slices  = sl;
