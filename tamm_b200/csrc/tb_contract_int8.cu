@@ -43,8 +43,9 @@ using namespace sm100;
 
 constexpr int MT = 128; // UMMA M: output rows of a tile
 constexpr int KC = 32;  // bytes of K per pipeline stage (one INT8 MMA k-step)
-constexpr int STAGES = 4;
-constexpr int NTHREADS = 192; // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
+constexpr int kMaxSmem = 227 * 1024; // dynamic shared memory per CTA on sm_100
+constexpr int NEPI     = 256;           // epilogue threads (warps 2-9)
+constexpr int NTHREADS = 64 + NEPI;     // warp 0 producer, warp 1 MMA issuer, warps 2-9 epilogue
 
 // One operand block to split into digit slices.
 struct SplitBlock {
@@ -82,14 +83,6 @@ __device__ __forceinline__ int32_t decomp(int32_t x, int n, const int32_t* dims,
     x = q;
   }
   return off;
-}
-
-// Byte position of (row r, k) inside one K chunk of one digit slice of a row tile of
-// `tile_rows` rows: UMMA canonical K-major layout without swizzle (8 x 16-byte core
-// matrices; the two 16-byte K halves tile_rows * 16 bytes apart; 8-row groups 128
-// bytes apart).
-__device__ __forceinline__ int32_t canon_off(int r, int kk, int tile_rows) {
-  return (kk >> 4) * (tile_rows * 16) + (r >> 3) * 128 + (r & 7) * 16 + (kk & 15);
 }
 
 // Offset of the k-th K element of a row: contiguous K (the inner labels are the
@@ -278,16 +271,26 @@ struct I8Params {
   LabelClasses    lc;
   int*            err;
   const uint8_t*  tslices; // digit count of each task (1..S)
+  int*            ctr;     // next output tile to hand out (zero at launch)
 };
 
 template<int S, int NT>
-constexpr uint32_t stage_bytes() {
+__host__ __device__ constexpr uint32_t stage_bytes() {
   return (uint32_t) S * (MT + NT) * KC;
+}
+
+constexpr int kTail  = 3072; // barriers, column scales and C offsets behind the stages
+constexpr int kQueue = 4;    // output tiles in flight between producer, MMA issuer and epilogue
+
+// Pipeline depth: as many stages as fit beside the tail, at most 6.
+template<int S, int NT>
+__host__ __device__ constexpr int stages() {
+  return (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) < 6 ? (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) : 6;
 }
 
 template<int S, int NT>
 constexpr size_t smem_bytes() {
-  return (size_t) STAGES * stage_bytes<S, NT>() + 2048;
+  return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail;
 }
 
 template<int S, int NT>
@@ -296,12 +299,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr uint32_t A_BYTES = S * MT * KC, B_BYTES = S * NT * KC, STAGE = A_BYTES + B_BYTES;
   constexpr int      kStack  = 256 / NT; // B digits per MMA (UMMA N <= 256)
+  constexpr int      STAGES  = stages<S, NT>();
+  static_assert(STAGES >= 2, "two pipeline stages at least");
   uint64_t*          full   = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE);
   uint64_t*          empty  = full + STAGES;
   uint64_t*          tfull  = empty + STAGES;
   uint64_t*          tempty = tfull + 1;                                    // one per diagonal
-  double*            sc     = reinterpret_cast<double*>(tempty + 8);         // column scales
-  uint32_t*          tslot  = reinterpret_cast<uint32_t*>(sc + NT);
+  uint64_t*          qfull  = tempty + 8;                                    // tile queue
+  uint64_t*          qempty = qfull + kQueue;
+  double*            sc     = reinterpret_cast<double*>(qempty + kQueue);    // column scales, 2 x NT
+  int32_t*           noff   = reinterpret_cast<int32_t*>(sc + 2 * NT);       // C column offsets, 2 x NT
+  int32_t*           qitem  = noff + 2 * NT;
+  uint32_t*          tslot  = reinterpret_cast<uint32_t*>(qitem + kQueue);
+  static_assert(sizeof(uint64_t) * (2 * 6 + 1 + 8 + 2 * kQueue) + (sizeof(double) + sizeof(int32_t)) * 2 * NT +
+                    4 * kQueue + 4 <=
+                  kTail,
+                "shared-memory tail");
   const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if(threadIdx.x == 0) {
@@ -310,7 +323,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    for(int d = 0; d < S; d++) mbar_init(&tempty[d], 128);
+    for(int d = 0; d < S; d++) mbar_init(&tempty[d], NEPI);
+    for(int i = 0; i < kQueue; i++) {
+      mbar_init(&qfull[i], 1);
+      mbar_init(&qempty[i], 1 + NEPI); // the MMA issuer and every epilogue thread
+    }
     fence_mbarrier_init();
   }
   if(warp == 1) tmem_alloc(tslot, 512);
@@ -324,7 +341,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
     if(elect_one()) {
       int      stage = 0;
       uint32_t phase = 0;
-      for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+      int       qslot = 0;
+      uint32_t  qph   = 0;
+      while(true) { // tiles are handed out longest first, to whichever CTA is free
+        if(!mbar_wait(&qempty[qslot], qph ^ 1, p.err, 5)) goto done_producer;
+        const int it = atomicAdd(p.ctr, 1);
+        qitem[qslot] = it < p.nitems ? it : -1;
+        mbar_arrive(&qfull[qslot]);
+        if(++qslot == kQueue) {
+          qslot = 0;
+          qph ^= 1;
+        }
+        if(it >= p.nitems) break;
         const I8Item   item = p.items[it];
         const DevGroup g    = p.groups[item.group];
         for(int t = g.task_begin; t < g.task_end; t++) {
@@ -363,7 +391,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
     if(elect_one()) {
       int      stage = 0;
       uint32_t phase = 0, tphase = 0;
-      for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+      int       qslot = 0;
+      uint32_t  qph   = 0;
+      while(true) {
+        if(!mbar_wait(&qfull[qslot], qph, p.err, 6)) goto done_mma;
+        const int it = qitem[qslot];
+        mbar_arrive(&qempty[qslot]);
+        if(++qslot == kQueue) {
+          qslot = 0;
+          qph ^= 1;
+        }
+        if(it < 0) break;
         const I8Item   item = p.items[it];
         const DevGroup g    = p.groups[item.group];
         for(int t = g.task_begin; t < g.task_end; t++) {
@@ -411,23 +449,90 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   }
   else {
     // ---------------- epilogue: FP64 recombination of the diagonals ----------------
-    const int q = warp & 3, row = q * 32 + lane;
-    uint32_t  tphase = 0;
-    double    racc[NT];
-    for(int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+    // Eight warps: warp w reads TMEM lanes 32 * (w % 4) (its rows) and one half of the
+    // tile's columns, so two warps share every lane quarter.
+    constexpr int NH = NT / 2;
+    const int     q = warp & 3, row = q * 32 + lane, col0 = ((warp - 2) >> 2) * NH;
+    const int     et = threadIdx.x - 64; // column whose scale this thread loads
+    uint32_t      tphase = 0, tcount = 0, icount = 0;
+    double        racc[NH];
+    int           qslot = 0;
+    uint32_t      qph   = 0;
+    for(;; icount++) {
+      int it;
+      {
+        // the epilogue threads agree on a timeout, so none is left in a barrier
+        const bool got = mbar_wait(&qfull[qslot], qph, p.err, 7);
+        uint32_t   anyfail;
+        asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
+                     "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                     : "=r"(anyfail)
+                     : "r"((uint32_t) got), "n"(NEPI)
+                     : "memory");
+        if(anyfail) break;
+        it = qitem[qslot];
+        mbar_arrive(&qempty[qslot]);
+        if(++qslot == kQueue) {
+          qslot = 0;
+          qph ^= 1;
+        }
+      }
+      if(it < 0) break;
       const I8Item   item = p.items[it];
       const DevGroup g    = p.groups[item.group];
 #pragma unroll
-      for(int x = 0; x < NT; x++) racc[x] = 0.0;
+      for(int x = 0; x < NH; x++) racc[x] = 0.0;
       bool ok = true;
-      for(int t = g.task_begin; t < g.task_end; t++) {
-        // the 128 epilogue threads agree on a timeout, so none is left in a barrier
+      // C addressing of the tile (transpose_output fused: C's own label order),
+      // computed while the tile's first task runs: the thread's row offset, and the
+      // tile's column offsets in shared memory (alternating buffers by tile; the first
+      // task's barrier below publishes them, the readers two tiles back are done)
+      int64_t  rowoff = -1;
+      int32_t* nof    = noff + (icount & 1) * NT;
+      {
+        int64_t cstr[kMaxModes];
+        int64_t s = 1;
+        for(int i = p.lc.nc - 1; i >= 0; i--) {
+          cstr[i] = s;
+          s *= g.cdims[i];
+        }
+        int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
+        int32_t M = 1, N = 1;
+        for(int j = 0; j < p.lc.nm; j++) {
+          mdim[j] = g.cdims[p.lc.m_c[j]];
+          mstr[j] = (int32_t) cstr[p.lc.m_c[j]];
+          M *= mdim[j];
+        }
+        for(int j = 0; j < p.lc.nn; j++) {
+          ndim[j] = g.cdims[p.lc.n_c[j]];
+          nstr[j] = (int32_t) cstr[p.lc.n_c[j]];
+          N *= ndim[j];
+        }
+        const int m = item.mt * MT + row;
+        if(m < M) rowoff = g.c_off + decomp(m, p.lc.nm, mdim, mstr);
+        if(et < NT) {
+          const int n = item.nt * NT + et;
+          nof[et]     = n < N ? decomp(n, p.lc.nn, ndim, nstr) : -1;
+        }
+      }
+      for(int t = g.task_begin; t < g.task_end; t++, tcount++) {
+        // The task's metadata and column scales 2^(e_col - 7) are fetched before its
+        // accumulators are complete, so their latency overlaps the task's MMAs.  The
+        // scales alternate between two buffers: the readers of this buffer (two tasks
+        // back) all passed the previous task's barrier below.
+        const I8Task tk  = p.tasks[t];
+        const int    st  = p.tslices[t];
+        const int    er  = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
+        double*      scb = sc + (tcount & 1) * NT;
+        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - 7);
+        // the epilogue threads agree on a timeout, so none is left in a barrier; the
+        // barrier also publishes the scales
         const bool     waited = mbar_wait(tfull, tphase, p.err, 4);
         uint32_t       anyfail;
         asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
-                     "bar.red.or.pred q, 1, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                     "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
                      : "=r"(anyfail)
-                     : "r"((uint32_t) waited)
+                     : "r"((uint32_t) waited), "n"(NEPI)
                      : "memory");
         if(anyfail) {
           ok = false;
@@ -435,39 +540,37 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
         tphase ^= 1;
         tc_fence_after();
-        const I8Task tk = p.tasks[t];
-        const int    st = p.tslices[t];
-        const int    er = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
-        const double sr = ldexp(1.0, er - 7);
-        // per-column scales 2^(e_col - 7) of this task, shared by the 128 rows (the
-        // barrier above also ends every thread's use of the previous task's scales)
-        const int et = threadIdx.x - 64;
-        if(et < NT) sc[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - 7);
-        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        // Diagonal d carries the row factor 2^k, k = e_row - 7 - 8d.  For k well inside
+        // the normal range it is applied inside the int32 -> double conversion:
+        // v * 2^k = (2^52 + 2^31 + v) * 2^k - (2^52 + 2^31) * 2^k, whose first term is
+        // assembled from its bits (high word: exponent 1075 + k, low word: v + 2^31) —
+        // exact, with no conversion instruction and no multiply.
+        const bool   fast = er - 7 - 8 * (S - 1) >= -1000 && er - 7 <= 900;
+        const double sr   = ldexp(1.0, er - 7);
         // drain diagonal by diagonal; each diagonal's TMEM is released as soon as it
         // has been read, so the next task's MMAs into it can start
-        constexpr int CW = NT <= 64 ? NT : 48; // columns in flight per wait
 #pragma unroll
         for(int d = 0; d < S; d++) {
           if(d < st) {
-            const double w = pow2i(-8 * d) * sr;
+            uint32_t       v[NH];
+            const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + d * NT + col0;
 #pragma unroll
-            for(int c0 = 0; c0 < NT; c0 += CW) {
-              constexpr int NL = CW / 16;
-              uint32_t      v[CW];
+            for(int l = 0; l + 16 <= NH; l += 16) tmem_ld16(ta + l, *reinterpret_cast<uint32_t(*)[16]>(v + l));
+            if(NH % 16) tmem_ld8(ta + NH - 8, *reinterpret_cast<uint32_t(*)[8]>(v + NH - 8));
+            tmem_wait_ld();
+            tc_fence_before();
+            mbar_arrive(&tempty[d]);
+            if(fast) {
+              const int    hi   = 0x43300000 + (er - 7 - 8 * d) * (1 << 20);
+              const double bias = __hiloint2double(hi, (int) 0x80000000u);
 #pragma unroll
-              for(int l = 0; l < NL; l++)
-                if(c0 + 16 * l < NT)
-                  tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + d * NT + c0 + 16 * l,
-                            *reinterpret_cast<uint32_t(*)[16]>(v + 16 * l));
-              tmem_wait_ld();
-              if(c0 + CW >= NT) {
-                tc_fence_before();
-                mbar_arrive(&tempty[d]);
-              }
+              for(int x = 0; x < NH; x++)
+                racc[x] = fma(__hiloint2double(hi, (int) (v[x] ^ 0x80000000u)) - bias, scb[col0 + x], racc[x]);
+            }
+            else {
+              const double w = pow2i(-8 * d) * sr;
 #pragma unroll
-              for(int x = 0; x < CW; x++)
-                if(c0 + x < NT) racc[c0 + x] = fma((double) (int32_t) v[x], w * sc[c0 + x], racc[c0 + x]);
+              for(int x = 0; x < NH; x++) racc[x] = fma((double) (int32_t) v[x], w * scb[col0 + x], racc[x]);
             }
           }
           else
@@ -475,37 +578,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
       }
       if(!ok) break;
-      // C (+)= alpha * result, in C's own layout (transpose_output fused here)
-      int64_t cstr[kMaxModes];
-      {
-        int64_t s = 1;
-        for(int i = p.lc.nc - 1; i >= 0; i--) {
-          cstr[i] = s;
-          s *= g.cdims[i];
-        }
-      }
-      int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
-      int32_t M = 1, N = 1;
-      for(int j = 0; j < p.lc.nm; j++) {
-        mdim[j] = g.cdims[p.lc.m_c[j]];
-        mstr[j] = (int32_t) cstr[p.lc.m_c[j]];
-        M *= mdim[j];
-      }
-      for(int j = 0; j < p.lc.nn; j++) {
-        ndim[j] = g.cdims[p.lc.n_c[j]];
-        nstr[j] = (int32_t) cstr[p.lc.n_c[j]];
-        N *= ndim[j];
-      }
-      const int m = item.mt * MT + row;
-      if(m < M) {
-        double* crow = p.C + g.c_off + decomp(m, p.lc.nm, mdim, mstr);
+      // C (+)= alpha * result: one reduction per element (c + alpha * r, rounded once,
+      // as a load-add-store would be; every element of C belongs to exactly one output
+      // tile), performed at L2, so the epilogue does not wait for C's memory
+      if(rowoff >= 0) {
+        double* crow = p.C + rowoff;
 #pragma unroll
-        for(int x = 0; x < NT; x++) {
-          const int n = item.nt * NT + x;
-          if(n < N) {
-            double* cp = crow + decomp(n, p.lc.nn, ndim, nstr);
-            *cp += p.alpha * racc[x];
-          }
+        for(int x = 0; x < NH; x++) {
+          const int o = nof[col0 + x];
+          if(o >= 0) atomicAdd(crow + o, p.alpha * racc[x]);
         }
       }
     }
@@ -540,6 +621,7 @@ struct I8Layout {
   int32_t*                d_blockmax = nullptr;
   uint8_t*                d_tslices  = nullptr;
   int*                    d_err     = nullptr;
+  int*                    d_ctr     = nullptr; // tile counter of the GEMM's dynamic schedule
   int                     device    = -1;
   ~I8Layout() {
     if(device >= 0) {
@@ -554,6 +636,7 @@ struct I8Layout {
       cudaFree(d_blockmax);
       cudaFree(d_tslices);
       cudaFree(d_err);
+      cudaFree(d_ctr);
     }
   }
 };
@@ -720,6 +803,7 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_tslices), std::max<size_t>(1, L->tasks.size())));
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_err), sizeof(int)));
   TB_CUDA(cudaMemset(L->d_err, 0, sizeof(int)));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&L->d_ctr), sizeof(int)));
   return L;
 }
 
@@ -765,6 +849,8 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   p.lc     = lc;
   p.err     = L.d_err;
   p.tslices = L.d_tslices;
+  p.ctr     = L.d_ctr;
+  TB_CUDA(cudaMemsetAsync(L.d_ctr, 0, sizeof(int), st));
   const size_t smem = smem_bytes<S, NT>();
   static bool  configured[64] = {false};
   int          dev            = 0;
@@ -916,7 +1002,7 @@ constexpr int kNoAllocDevices = 64;
 void*         g_noalloc_base[kNoAllocDevices] = {nullptr}; // device address, per device
 
 // Control words and descriptors at fixed offsets of the scratch.
-constexpr int64_t kCtlErr = 0, kCtlBlockMax = 8, kCtlSlices = 16, kCtlDesc = 256, kCtlItems = 1280;
+constexpr int64_t kCtlErr = 0, kCtlCtr = 4, kCtlBlockMax = 8, kCtlSlices = 16, kCtlDesc = 256, kCtlItems = 1280;
 
 struct NoAllocDesc {
   SplitBlock a, b;
@@ -936,6 +1022,7 @@ __global__ void k_noalloc_setup(NoAllocDesc d, unsigned char* base) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   if(tid == 0) {
     *reinterpret_cast<int*>(base + kCtlErr)              = 0;
+    *reinterpret_cast<int*>(base + kCtlCtr)              = 0;
     reinterpret_cast<int32_t*>(base + kCtlBlockMax)[0]   = (int32_t) 0x80808080;
     reinterpret_cast<int32_t*>(base + kCtlBlockMax)[1]   = (int32_t) 0x80808080;
     SplitBlock* sb                                       = reinterpret_cast<SplitBlock*>(base + kCtlDesc);
@@ -972,7 +1059,7 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   k_split_fused<S><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
   k_split_fused<S><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
   k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
-  I8Params p;
+  I8Params p{};
   p.slices  = sl;
   p.exps    = exps;
   p.tasks   = tsk;
@@ -984,6 +1071,7 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   p.lc      = lc;
   p.err     = reinterpret_cast<int*>(base + kCtlErr);
   p.tslices = tsl;
+  p.ctr     = reinterpret_cast<int*>(base + kCtlCtr);
   const size_t smem = smem_bytes<S, NT>();
   TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
   k_contract_i8<S, NT><<<std::min(p.nitems, sm_count()), NTHREADS, smem, st>>>(p);
