@@ -351,7 +351,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"fp64": "f64", "int8": "s8/u8 digits, s32 accumulate, f64 recombination",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "int8": "s8 balanced digits, s32 accumulate, f64 recombination",
                                            "bf16x3": "bf16x3"}[headline],
             "data": "synthetic (seeded; no dataset)",
             "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}", "mode": headline,
