@@ -275,6 +275,44 @@ int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out);
 /* Drops queued ops without running them. */
 int tb_sched_clear(tb_sched s);
 
+/* ========================================================== DIFFERENTIATION === */
+
+/* No counterpart in TAMM (it has no automatic differentiation).  A tape records
+ * Functions that run eagerly on its own Scheduler, in the context's precision mode:
+ *   Contract  y(Ly) = alpha * a(La) * b(Lb)
+ *             backward: da(La) += alpha * dy(Ly) * b(Lb),  db(Lb) += alpha * a(La) * dy(Ly)
+ *             (the dy-weighted contractions over the labels free in the other operand:
+ *             TAMM's MultOp with swapped operands, multop.hpp:576-893);
+ *   Dot       s = alpha * sum p(Lp) * q(Lq)  (same label set, any order)
+ *             backward: dp += alpha * q,  dq += alpha * p  (AddOp, addop.hpp:242-271).
+ * The objective is the sum of the Dot values.  tb_tape_backward accumulates its
+ * gradient into the gradient tensors given for the leaves (zero them first; reset
+ * the tape before recording the next evaluation).  Tensors that are neither leaves
+ * nor Contract outputs are constants.  At the start of the backward sweep, Contract
+ * outputs are kept in recording order while their total size fits budget_bytes;
+ * the rest are freed and recomputed from their producer when the sweep needs their
+ * values.  The tape holds plain references: destroy it before its tensors. */
+typedef struct tb_tape_s* tb_tape;
+int tb_tape_create(tb_ctx ctx, int64_t budget_bytes, tb_tape* out);
+int tb_tape_destroy(tb_tape t);
+/* Declares x a leaf whose gradient accumulates into grad (same spaces and spin mask;
+ * NULL: x is a constant). */
+int tb_tape_leaf(tb_tape t, tb_tensor x, tb_tensor grad);
+/* Contract Function; y is an allocated tensor written once on this tape, labelled
+ * over its full spaces.  An operand label summed inside that operand alone (whose
+ * gradient would need a broadcast output) is TB_ERR_NOT_IMPLEMENTED. */
+int tb_tape_contract(tb_tape t, tb_labeled y, double alpha, tb_labeled a, tb_labeled b);
+/* Dot Function; *value (may be NULL) receives alpha * sum p * q. */
+int tb_tape_dot(tb_tape t, double alpha, tb_labeled p, tb_labeled q, double* value);
+int tb_tape_backward(tb_tape t);
+/* Recorded Functions, objective (sum of the Dot values), bytes of Contract outputs
+ * kept by the last backward sweep, and how many outputs it recomputed. */
+int tb_tape_info(tb_tape t, int64_t* nnodes, double* objective, int64_t* kept_bytes,
+                 int64_t* recomputed);
+/* Forgets the recorded Functions and intermediate gradients (leaves stay declared);
+ * outputs freed by the budget get their storage back. */
+int tb_tape_reset(tb_tape t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,8 +5,8 @@ in include/tamm_b200.h); this package is a thin Python front-end over it.
 """
 from ._capi import TambError, lib, last_error  # noqa: F401
 from .tamm import (ExecutionContext, ExecutionHW, IndexSpace, LabeledTensor, Precision,  # noqa: F401
-                   Scheduler, Tensor, TiledIndexLabel, TiledIndexSpace)
+                   Scheduler, Tape, Tensor, TiledIndexLabel, TiledIndexSpace)
 
 __all__ = ["ExecutionContext", "ExecutionHW", "IndexSpace", "LabeledTensor", "Precision",
-           "Scheduler", "Tensor", "TiledIndexLabel", "TiledIndexSpace", "TambError", "lib",
+           "Scheduler", "Tape", "Tensor", "TiledIndexLabel", "TiledIndexSpace", "TambError", "lib",
            "last_error"]

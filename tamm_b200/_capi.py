@@ -107,6 +107,14 @@ PROTOS = {
     "tb_sched_profile": [h, i64p, dp, dp, C.c_int64],
     "tb_sched_clear": [h],
     "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
+    "tb_tape_create": [h, C.c_int64, C.POINTER(h)],
+    "tb_tape_destroy": [h],
+    "tb_tape_leaf": [h, h, h],
+    "tb_tape_contract": [h, tb_labeled, C.c_double, tb_labeled, tb_labeled],
+    "tb_tape_dot": [h, C.c_double, tb_labeled, tb_labeled, dp],
+    "tb_tape_backward": [h],
+    "tb_tape_info": [h, i64p, dp, i64p, i64p],
+    "tb_tape_reset": [h],
 }
 
 _lib = None

@@ -48,22 +48,22 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
 
 using namespace tb;
 
-#define TB_API_BEGIN try {
-#define TB_API_END                                                                      \
-  }                                                                                     \
-  catch(const tb::Error& e) {                                                           \
-    tb::set_last_error(e.what());                                                       \
-    return e.code;                                                                      \
-  }                                                                                     \
-  catch(const std::bad_alloc&) {                                                        \
-    tb::set_last_error("host allocation failed");                                       \
-    return TB_ERR_NO_MEMORY;                                                            \
-  }                                                                                     \
-  catch(const std::exception& e) {                                                      \
-    tb::set_last_error(e.what());                                                       \
-    return TB_ERR_INVALID;                                                              \
-  }                                                                                     \
-  return TB_OK;
+#include "tb_api.hpp"
+
+namespace tb {
+Labeled labeled_from_c(const tb_labeled& x) {
+  TB_EXPECTS(x.tensor != nullptr, "labelled operand without a tensor");
+  Labeled l;
+  l.t = x.tensor->p.get();
+  for(int i = 0; i < l.t->nmodes; i++) {
+    TB_EXPECTS(x.labels != nullptr, "labelled operand without labels");
+    l.labels.push_back(x.labels[i]);
+    l.ltis.push_back((x.label_tis && x.label_tis[i]) ? x.label_tis[i]->p : l.t->tis[i]);
+  }
+  return l;
+}
+
+} // namespace tb
 
 #define REQUIRE_ARG(x) TB_EXPECTS((x), #x " must be non-null / valid")
 
@@ -627,17 +627,7 @@ int tb_tensor_norm(tb_tensor t, double* out) {
   TB_API_END
 }
 
-static Labeled to_labeled(const tb_labeled& x) {
-  REQUIRE_ARG(x.tensor != nullptr);
-  Labeled l;
-  l.t = x.tensor->p.get();
-  for(int i = 0; i < l.t->nmodes; i++) {
-    REQUIRE_ARG(x.labels != nullptr);
-    l.labels.push_back(x.labels[i]);
-    l.ltis.push_back((x.label_tis && x.label_tis[i]) ? x.label_tis[i]->p : l.t->tis[i]);
-  }
-  return l;
-}
+static Labeled to_labeled(const tb_labeled& x) { return tb::labeled_from_c(x); }
 
 int tb_sched_create(tb_ctx ctx, tb_sched* out) {
   TB_API_BEGIN

@@ -107,6 +107,9 @@ struct Labeled {
   std::vector<std::shared_ptr<TIS>> ltis; // label space per mode
 };
 
+// tb_labeled (C ABI) -> Labeled; NULL label spaces mean the tensor's own.
+Labeled labeled_from_c(const tb_labeled& x);
+
 struct Op {
   enum Kind { Set, Add, Mult } kind;
   Labeled lhs, a, b;

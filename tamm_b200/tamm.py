@@ -470,3 +470,66 @@ class Scheduler:
             A.lib().tb_sched_destroy(self.h)
         except Exception:
             pass
+
+
+class Tape:
+    """Differentiation of a contraction sequence (no counterpart in TAMM): a tape of
+    Functions run eagerly on their own Scheduler, in the context's precision mode.
+
+        tape = Tape(ec, budget_bytes)
+        tape.leaf(t2, g)                                  # g accumulates dE/dt2
+        tape.contract(X(a, b, i, j), v(a, b, c, d) * t2(c, d, i, j))
+        e1 = tape.dot(w(i, j, a, b), t2(a, b, i, j))
+        e2 = tape.dot(t2(a, b, i, j), X(a, b, i, j), 0.25)
+        tape.backward()                                   # g += dE/dt2, E = e1 + e2
+
+    Contract's backward is the pair of swapped-operand contractions dA += alpha *
+    dC * B, dB += alpha * A * dC; Dot's is a pair of permuted adds.  Contract outputs
+    beyond `budget_bytes` (in recording order) are freed at the start of the backward
+    sweep and recomputed when needed.  Call reset() before the next evaluation."""
+
+    def __init__(self, ec: ExecutionContext, budget_bytes: int = 1 << 62):
+        self.ec = ec
+        self.h = A.h()
+        call("tb_tape_create", ec.h, int(budget_bytes), C.byref(self.h))
+        self._keep = []
+
+    def leaf(self, x: Tensor, grad: Tensor | None = None):
+        call("tb_tape_leaf", self.h, x.h, grad.h if grad is not None else None)
+        return self
+
+    def contract(self, y: LabeledTensor, product):
+        if isinstance(product, LabeledTensor) or not isinstance(product, _Product) or len(product.factors) != 2:
+            raise ValueError("contract takes y(labels) and a product of two labelled tensors")
+        ids: dict = {}
+        l, a, b = (_to_c_labeled(t, ids, self._keep) for t in (y, product.factors[0], product.factors[1]))
+        call("tb_tape_contract", self.h, l, float(product.alpha), a, b)
+        return self
+
+    def dot(self, p: LabeledTensor, q: LabeledTensor, alpha: float = 1.0) -> float:
+        ids: dict = {}
+        x, y = (_to_c_labeled(t, ids, self._keep) for t in (p, q))
+        v = C.c_double()
+        call("tb_tape_dot", self.h, float(alpha), x, y, C.byref(v))
+        return v.value
+
+    def backward(self):
+        call("tb_tape_backward", self.h)
+        return self
+
+    def info(self):
+        n, kept, rec = C.c_int64(), C.c_int64(), C.c_int64()
+        obj = C.c_double()
+        call("tb_tape_info", self.h, C.byref(n), C.byref(obj), C.byref(kept), C.byref(rec))
+        return {"nodes": n.value, "objective": obj.value, "kept_bytes": kept.value, "recomputed": rec.value}
+
+    def reset(self):
+        call("tb_tape_reset", self.h)
+        self._keep = []
+        return self
+
+    def __del__(self):
+        try:
+            A.lib().tb_tape_destroy(self.h)
+        except Exception:
+            pass

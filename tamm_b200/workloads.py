@@ -13,7 +13,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .tamm import ExecutionContext, IndexSpace, Scheduler, Tensor, TiledIndexSpace, mult_info
+from .tamm import ExecutionContext, IndexSpace, Scheduler, Tape, Tensor, TiledIndexSpace, mult_info
 
 
 def mo_index_space(oa: int, va: int) -> IndexSpace:
@@ -158,3 +158,89 @@ def ladder(oa: int, va: int, seed: int = 1, tile_lo: int = 24, tile_hi: int = 48
 def mult_flops(lhs, a, b):
     """Admitted FP64 FLOPs of lhs += a * b (no GPU needed)."""
     return mult_info(lhs, a, b)[2]
+
+
+@dataclass
+class EnergyProblem:
+    """E(t2) = sum w(i,j,a,b) t2(a,b,i,j) + 1/4 sum t2(a,b,i,j) X(a,b,i,j),
+    X(a,b,i,j) = v(a,b,c,d) t2(c,d,i,j), on the ladder's spin-blocked spaces, with its
+    gradient dE/dt2 = w(i,j,a,b) + 1/4 X + 1/4 sum_ab v(a,b,c,d) t2(a,b,i,j)."""
+    lad: Ladder
+    w: Tensor
+    X: Tensor
+    g: Tensor
+    tape: Tape
+    w_host: np.ndarray
+
+
+def energy_problem(oa: int, va: int, seed: int = 3, tile_lo: int = 24, tile_hi: int = 48,
+                   ec: ExecutionContext | None = None, build_v: bool = True,
+                   budget_bytes: int = 1 << 62) -> EnergyProblem:
+    """Config of the adjoint check: ladder inputs (v from Cholesky vectors, t2 from
+    the orbital-energy denominators) and w ~ N(0, 1) / sqrt(O * V)."""
+    lad = ladder(oa, va, seed=seed, tile_lo=tile_lo, tile_hi=tile_hi, ec=ec, build_v=build_v)
+    O, V = lad.O, lad.V
+    w = Tensor([O, O, V, V], spin=(2, 2)).allocate(lad.ec)
+    rng = np.random.default_rng(seed + 29)
+    w_host = rng.normal(0.0, 1.0, size=w.nelems) / math.sqrt((2 * oa) * (2 * va))
+    w.write(w_host)
+    X = Tensor([V, V, O, O], spin=(2, 2)).allocate(lad.ec)
+    g = Tensor([V, V, O, O], spin=(2, 2)).allocate(lad.ec)
+    return EnergyProblem(lad, w, X, g, Tape(lad.ec, budget_bytes), w_host)
+
+
+def energy(P: EnergyProblem, gradient: bool = False) -> float:
+    """E(t2) through the tape; with gradient=True, P.g = dE/dt2 afterwards."""
+    a, b, c, d, i, j = P.lad.labels
+    t2, v = P.lad.t2, P.lad.v
+    tape = P.tape.reset()
+    if gradient:
+        P.lad.sch(P.g().assign(0.0)).execute()
+        tape.leaf(t2, P.g)
+    tape.contract(P.X(a, b, i, j), v(a, b, c, d) * t2(c, d, i, j))
+    e = tape.dot(P.w(i, j, a, b), t2(a, b, i, j))
+    e += tape.dot(t2(a, b, i, j), P.X(a, b, i, j), 0.25)
+    if gradient:
+        tape.backward()
+    return e
+
+
+def fd_amplitudes(t: Tensor, count: int, seed: int):
+    """`count` distinct stored amplitudes of t, chosen at random: (block id, element
+    index within the block, packed offset)."""
+    rng = np.random.default_rng(seed)
+    keys, offs = t.block_table()
+    nts = [s.num_tiles for s in t.spaces]
+    out, seen = [], set()
+    while len(out) < count:
+        bi = int(rng.integers(len(keys)))
+        key, bid = int(keys[bi]), []
+        for n in reversed(nts):
+            bid.append(key % n)
+            key //= n
+        bid = bid[::-1]
+        size = int(np.prod(t.block_dims(bid)))
+        e = int(rng.integers(size))
+        if (bi, e) in seen:
+            continue
+        seen.add((bi, e))
+        out.append((bid, e, int(offs[bi]) + e))
+    return out
+
+
+def finite_difference(P: EnergyProblem, amps, h: float = 1e-5):
+    """Central differences (E(t2 + h e_k) - E(t2 - h e_k)) / 2h at the given amplitudes."""
+    t2 = P.lad.t2
+    out = []
+    for bid, e, _ in amps:
+        blk = t2.get(bid)
+        x0 = float(blk.reshape(-1)[e])
+        vals = []
+        for s in (+1.0, -1.0):
+            b2 = blk.copy().reshape(-1)
+            b2[e] = x0 + s * h
+            t2.put(bid, b2)
+            vals.append(energy(P))
+        t2.put(bid, blk)
+        out.append((vals[0] - vals[1]) / (2.0 * h))
+    return np.array(out)
