@@ -477,6 +477,7 @@ public:
   ExecutionContext& ec() { return ec_; }
 
 private:
+  friend class Tape;
   struct Lowered {
     std::shared_ptr<std::vector<int>>    labels;
     std::shared_ptr<std::vector<tb_tis>> spaces;
@@ -498,6 +499,66 @@ private:
   }
   ExecutionContext            ec_;
   std::shared_ptr<tb_sched_s> h_;
+};
+
+// Forward/backward Functions on a Scheduler (no counterpart in TAMM; tb_tape_* in
+// tamm_b200.h).  Contract's backward is the pair of swapped-operand contractions
+// dA += alpha * dC * B, dB += alpha * A * dC; Dot's a pair of permuted adds; the
+// objective is the sum of the Dot values.  Contract outputs beyond the memory budget
+// are freed at the start of backward() and recomputed when needed.
+//
+//   Tape tape{ec};
+//   tape.leaf(t2, g);                                       // g += dE/dt2
+//   tape.contract(X(a, b, i, j), v(a, b, c, d) * t2(c, d, i, j));
+//   double E = tape.dot(w(i, j, a, b), t2(a, b, i, j)) + tape.dot(t2(a, b, i, j), X(a, b, i, j), 0.25);
+//   tape.backward();
+class Tape {
+public:
+  explicit Tape(const ExecutionContext& ec, int64_t budget_bytes = INT64_MAX): ec_(ec) {
+    tb_tape t = nullptr;
+    check(tb_tape_create(ec.handle(), budget_bytes, &t));
+    h_ = std::shared_ptr<tb_tape_s>(t, [](tb_tape x) { tb_tape_destroy(x); });
+  }
+
+  template<typename T>
+  Tape& leaf(const Tensor<T>& x, const Tensor<T>& grad) {
+    check(tb_tape_leaf(h_.get(), x.handle(), grad.handle()));
+    return *this;
+  }
+
+  template<typename T>
+  Tape& contract(const LabeledTensor<T>& y, const Product& p) {
+    if(p.factors.size() != 2) throw Error(TB_ERR_INVALID, "contract takes a product of two labelled tensors");
+    std::map<std::string, int>    ids;
+    std::vector<Scheduler::Lowered> keep;
+    tb_labeled                    ly = Scheduler::lower(y, ids, keep);
+    tb_labeled                    la = Scheduler::lower(p.factors[0], ids, keep);
+    tb_labeled                    lb = Scheduler::lower(p.factors[1], ids, keep);
+    check(tb_tape_contract(h_.get(), ly, p.alpha, la, lb));
+    return *this;
+  }
+
+  double dot(const LabeledTensorBase& p, const LabeledTensorBase& q, double alpha = 1.0) {
+    std::map<std::string, int>    ids;
+    std::vector<Scheduler::Lowered> keep;
+    tb_labeled                    lp = Scheduler::lower(p, ids, keep);
+    tb_labeled                    lq = Scheduler::lower(q, ids, keep);
+    double                        v  = 0.0;
+    check(tb_tape_dot(h_.get(), alpha, lp, lq, &v));
+    return v;
+  }
+
+  void backward() { check(tb_tape_backward(h_.get())); }
+  void reset() { check(tb_tape_reset(h_.get())); }
+  int64_t recomputed() const {
+    int64_t r = 0;
+    check(tb_tape_info(h_.get(), nullptr, nullptr, nullptr, &r));
+    return r;
+  }
+
+private:
+  ExecutionContext           ec_;
+  std::shared_ptr<tb_tape_s> h_;
 };
 
 } // namespace tamm

@@ -150,6 +150,69 @@ static int test_random_contraction(ExecutionContext& ec, Precision p, double tol
   return 0;
 }
 
+// Dense host copy of a 2-mode tensor (no spin) through block get().
+static std::vector<double> dense2(const Tensor<double>& T, const TiledIndexSpace& s0, const TiledIndexSpace& s1) {
+  std::vector<int64_t> z0 = s0.tile_sizes(), z1 = s1.tile_sizes();
+  int64_t              n0 = 0, n1 = 0;
+  for(auto x: z0) n0 += x;
+  for(auto x: z1) n1 += x;
+  std::vector<double> out(n0 * n1);
+  int64_t             o0 = 0;
+  for(int64_t t0 = 0; t0 < (int64_t) z0.size(); o0 += z0[t0++]) {
+    int64_t o1 = 0;
+    for(int64_t t1 = 0; t1 < (int64_t) z1.size(); o1 += z1[t1++]) {
+      auto    blk = T.get({t0, t1});
+      int64_t q   = 0;
+      for(int64_t x0 = 0; x0 < z0[t0]; x0++)
+        for(int64_t x1 = 0; x1 < z1[t1]; x1++) out[(o0 + x0) * n1 + o1 + x1] = blk[q++];
+    }
+  }
+  return out;
+}
+
+// Tape: E(t) = sum w(i,a) t(a,i) + 1/2 sum t(a,i) X(a,i), X = M(a,b) t(b,i);
+// dE/dt(a,i) = w(i,a) + 1/2 X(a,i) + 1/2 sum_b M(b,a) t(b,i), against host loops,
+// with the intermediate kept and with it recomputed (zero budget).
+static int test_tape_gradient(ExecutionContext& ec, int64_t budget) {
+  TiledIndexSpace Vt{IndexSpace{range(12)}, 5}, Ot{IndexSpace{range(6)}, 4};
+  auto [a, b] = Vt.labels<2>("all");
+  auto [i]    = Ot.labels<1>("all");
+  Tensor<double> M{Vt, Vt}, t{Vt, Ot}, w{Ot, Vt}, X{Vt, Ot}, g{Vt, Ot};
+  Scheduler      sch{ec};
+  sch.allocate(M, t, w, X, g);
+  std::mt19937_64                        gen(3);
+  std::uniform_real_distribution<double> U(-1, 1);
+  for(auto* T: {&M, &t, &w}) {
+    std::vector<double> v(T->size());
+    for(auto& x: v) x = U(gen);
+    T->write(v);
+  }
+  sch(g() = 0.0).execute();
+  Tape tape{ec, budget};
+  tape.leaf(t, g);
+  tape.contract(X(a, i), M(a, b) * t(b, i));
+  const double E = tape.dot(w(i, a), t(a, i)) + tape.dot(t(a, i), X(a, i), 0.5);
+  tape.backward();
+  REQUIRE(tape.recomputed() == (budget == 0 ? 1 : 0));
+  auto dm = dense2(M, Vt, Vt), dt = dense2(t, Vt, Ot), dw = dense2(w, Ot, Vt), dg = dense2(g, Vt, Ot);
+  double e = 0, maxerr = 0, maxg = 0;
+  for(int ia = 0; ia < 12; ia++)
+    for(int ii = 0; ii < 6; ii++) {
+      double x = 0, y = 0;
+      for(int ib = 0; ib < 12; ib++) {
+        x += dm[ia * 12 + ib] * dt[ib * 6 + ii];
+        y += dm[ib * 12 + ia] * dt[ib * 6 + ii];
+      }
+      e += dw[ii * 12 + ia] * dt[ia * 6 + ii] + 0.5 * dt[ia * 6 + ii] * x;
+      const double want = dw[ii * 12 + ia] + 0.5 * x + 0.5 * y;
+      maxerr            = std::fmax(maxerr, std::fabs(want - dg[ia * 6 + ii]));
+      maxg              = std::fmax(maxg, std::fabs(want));
+    }
+  REQUIRE(std::fabs(E - e) <= 1e-12 * std::fabs(e));
+  REQUIRE(maxerr <= 1e-12 * maxg);
+  return 0;
+}
+
 int main() {
   ExecutionContext ec{0, int64_t(2) << 30};
   int              rc = 0;
@@ -158,6 +221,8 @@ int main() {
   rc |= test_3d_4d_mult_ops(ec);
   rc |= test_random_contraction(ec, Precision::FP64, 1e-12);
   rc |= test_random_contraction(ec, Precision::INT8, 1e-11);
+  rc |= test_tape_gradient(ec, INT64_MAX);
+  rc |= test_tape_gradient(ec, 0);
   if(rc == 0) std::printf("ALL PASSED\n");
   return rc;
 }
