@@ -99,7 +99,7 @@ int tb_axpby(double alpha, const double* x, double beta, double* y, int64_t n, v
  * cudaMallocAsync, cudaFree or host-heap call: its scratch (digit slices,
  * exponents, the one-task work list) is a file-scope device array of 64 MiB that
  * every GPU loading the library holds until exit.  A triple needing more scratch
- * (about 7 * K * (M + N) bytes at the default 7 digits) is rejected with
+ * (about 6 * K * (M + N) bytes at the default 6 digits) is rejected with
  * TB_ERR_INVALID and a message giving the size.  Labels as in tb_block_multiply
  * (plain contractions only: no Hadamard or one-sided reduction labels); nslices 0
  * picks the digit count for a 1e-11 target, 3..8 forces it.  The first call on a
@@ -159,6 +159,8 @@ typedef struct tb_stats {
   int64_t scratch_bytes;  /* scratch used by the split operands */
   double split_ms;        /* device time of the operand splitting (profiled runs) */
   double gemm_ms;         /* device time of the tensor-core contraction kernel (profiled runs) */
+  int    mode;            /* kernel that ran: TB_MODE_FP64 or TB_MODE_INT8 (autotuner's choice) */
+  int    tile_n;          /* split-INT8 output tile width (0: the default for the slice count) */
 } tb_stats;
 
 /* C += alpha * sum over tasks of A * B, all groups, one stream-ordered pass.
@@ -227,6 +229,11 @@ int tb_tensor_block_size(tb_tensor t, const int64_t* blockid, int64_t* out);
 int tb_tensor_block_dims(tb_tensor t, const int64_t* blockid, int64_t* dims);
 /* Element offset of a stored block, -1 if the block is not admitted. */
 int tb_tensor_locate(tb_tensor t, const int64_t* blockid, int64_t* offset);
+/* Gives an unallocated tensor caller-owned device storage of >= 8 * nelems bytes,
+ * 16-byte aligned (no counterpart in TAMM): several tensors used one after another
+ * in stream order can share one buffer, e.g. the batches of an integral tensor
+ * built on demand.  tb_tensor_deallocate detaches it without freeing. */
+int tb_tensor_attach(tb_tensor t, tb_ctx ctx, void* device_ptr, int64_t bytes);
 /* Tensor::get / put / add of one block with a HOST buffer of n >= block size
  * (tensor_impl.hpp:321-455; get of a non-admitted block returns zeros). */
 int tb_tensor_get(tb_tensor t, const int64_t* blockid, double* host, int64_t n);
@@ -274,6 +281,41 @@ int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64
 int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out);
 /* Drops queued ops without running them. */
 int tb_sched_clear(tb_sched s);
+
+/* Scalar results kept on the device, in 64 slots per Scheduler (read with
+ * tb_sched_scalars after execute or a graph launch): slot = alpha * sum a * b over
+ * the stored elements (a and b with the same labels and block layout), or
+ * slot = alpha * sqrt(sum a * a) (tamm::norm, tamm_utils.hpp:1180-1200). */
+int tb_sched_dot(tb_sched s, int slot, double alpha, tb_labeled a, tb_labeled b);
+int tb_sched_norm(tb_sched s, int slot, double alpha, tb_labeled a);
+int tb_sched_scalars(tb_sched s, double* host, int n);
+/* Orbital-energy denominator update of CC amplitudes (TAMM's jacobi_cc via
+ * apply_ewise, tamm_utils.hpp:866-936): t += alpha * r / D element by element, with
+ * D = sum over modes of signs[m] * eps[orbital index of mode m] (eps over the root
+ * index space shared by t's modes, neps entries; r with t's labels and layout). */
+int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const double* eps, int64_t neps,
+                   const double* signs);
+/* Autotuner (no counterpart in TAMM): with enable != 0, the first execution of each
+ * contraction under a split-INT8 request times the candidate kernels (FP64; split-
+ * INT8 with output tiles 80 / 64 / 48 wide where the slice count allows) on a saved
+ * copy of the output and keeps the fastest for that contraction and request. */
+int tb_sched_autotune(tb_sched s, int enable);
+/* The choice for op `index` of the last execute (ncand = 0: not tuned) and the
+ * timed candidates (up to cap). */
+int tb_sched_tune_info(tb_sched s, int64_t index, int* mode, int* tile_n, int* ncand, int* cand_modes,
+                       int* cand_tiles, double* cand_ms, int cap);
+
+/* CUDA graph of the queued ops (no counterpart in TAMM): runs them once eagerly
+ * (building plans, work lists and autotuner choices), then captures the same ops on
+ * the context's stream.  tb_graph_launch enqueues one replay; tb_graph_sync waits
+ * for it and checks the device error words of its split-INT8 contractions.  The
+ * tensors the ops use must stay allocated while the graph exists; the graph keeps
+ * the scratch its capture used. */
+typedef struct tb_graph_s* tb_graph;
+int tb_sched_graph_create(tb_sched s, tb_graph* out);
+int tb_graph_launch(tb_graph g);
+int tb_graph_sync(tb_graph g);
+int tb_graph_destroy(tb_graph g);
 
 /* ========================================================== DIFFERENTIATION === */
 

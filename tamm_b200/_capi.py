@@ -35,7 +35,7 @@ h = C.c_void_p  # opaque handles
 class tb_stats(C.Structure):
     _fields_ = [("flops", C.c_double), ("int8_ops", C.c_double), ("slices_min", C.c_int),
                 ("slices_max", C.c_int), ("scratch_bytes", C.c_int64), ("split_ms", C.c_double),
-                ("gemm_ms", C.c_double)]
+                ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int)]
 
 
 class tb_labeled(C.Structure):
@@ -107,6 +107,17 @@ PROTOS = {
     "tb_sched_profile": [h, i64p, dp, dp, C.c_int64],
     "tb_sched_clear": [h],
     "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
+    "tb_tensor_attach": [h, h, vp, C.c_int64],
+    "tb_sched_dot": [h, C.c_int, C.c_double, tb_labeled, tb_labeled],
+    "tb_sched_norm": [h, C.c_int, C.c_double, tb_labeled],
+    "tb_sched_scalars": [h, dp, C.c_int],
+    "tb_sched_denom": [h, tb_labeled, C.c_double, tb_labeled, dp, C.c_int64, dp],
+    "tb_sched_autotune": [h, C.c_int],
+    "tb_sched_tune_info": [h, C.c_int64, ip, ip, ip, ip, ip, dp, C.c_int],
+    "tb_sched_graph_create": [h, C.POINTER(h)],
+    "tb_graph_launch": [h],
+    "tb_graph_sync": [h],
+    "tb_graph_destroy": [h],
     "tb_tape_create": [h, C.c_int64, C.POINTER(h)],
     "tb_tape_destroy": [h],
     "tb_tape_leaf": [h, h, h],

@@ -157,7 +157,8 @@ __global__ void __launch_bounds__(kThreads) k_dot_partial(const double* __restri
   }
 }
 
-__global__ void k_dot_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+__global__ void k_dot_final(const double* __restrict__ part, int np, double* __restrict__ out, double scale = 1.0,
+                            int root = 0) {
   __shared__ double ws[32];
   double            s = 0.0;
   for(int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
@@ -168,7 +169,29 @@ __global__ void k_dot_final(const double* __restrict__ part, int np, double* __r
   if(threadIdx.x == 0) {
     double t = 0.0;
     for(int w = 0; w < (int) (blockDim.x / 32); w++) t += ws[w];
-    *out = t;
+    *out = scale * (root ? sqrt(t) : t);
+  }
+}
+
+// t += scale * r / D over the admitted blocks of t (r has t's layout), with
+// D = sum over modes of sign_m * eps[first_m + index_m]: the orbital-energy
+// denominator of a CC amplitude update (D = e_a + e_b - e_i - e_j for t2(a,b,i,j)).
+// One CTA per block, threads over its elements.
+__global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, const double* __restrict__ r,
+                                                    double scale, const DenomBlock* __restrict__ blocks,
+                                                    int nmodes, const double* __restrict__ eps, DenomSigns sg) {
+  const DenomBlock b = blocks[blockIdx.x];
+  int64_t          n = 1;
+  for(int m = 0; m < nmodes; m++) n *= b.dims[m];
+  for(int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+    int64_t x = e;
+    double  d = 0.0;
+    for(int m = nmodes - 1; m >= 0; m--) {
+      const int64_t q = x / b.dims[m];
+      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
+      x = q;
+    }
+    t[b.off + e] += scale * r[b.off + e] / d;
   }
 }
 
@@ -330,6 +353,24 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
   TB_CUDA(cudaFreeAsync(part, stream));
   TB_CUDA(cudaStreamSynchronize(stream));
   return h;
+}
+
+void launch_dot_to(const double* x, const double* y, int64_t n, double scale, int root, double* out, double* part,
+                   cudaStream_t stream) {
+  if(n <= 0) {
+    TB_CUDA(cudaMemsetAsync(out, 0, sizeof(double), stream));
+    return;
+  }
+  k_dot_partial<<<kRedBlocks, kThreads, 0, stream>>>(x, y, n, part);
+  k_dot_final<<<1, 1024, 0, stream>>>(part, kRedBlocks, out, scale, root);
+  TB_CUDA(cudaGetLastError());
+}
+
+void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
+                  const double* eps, DenomSigns signs, cudaStream_t stream) {
+  if(nblocks <= 0) return;
+  k_denom<<<nblocks, kThreads, 0, stream>>>(t, r, scale, blocks, nmodes, eps, signs);
+  TB_CUDA(cudaGetLastError());
 }
 
 void launch_fill_random(double* x, int64_t n, uint64_t seed, uint64_t first, int dist, double p0,

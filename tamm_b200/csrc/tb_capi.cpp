@@ -17,8 +17,10 @@ std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bo
 // Mode dispatch of one grouped contraction.
 void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
                   double* C, cudaStream_t stream, Arena* arena) {
-  plan.last       = tb_stats{};
-  plan.last.flops = wl.flops;
+  plan.last          = tb_stats{};
+  plan.last.flops    = wl.flops;
+  plan.last.mode     = plan.mode;
+  plan.last.tile_n   = plan.tile_n;
   plan.arena      = arena;
   if(wl.tasks.empty()) return;
   switch(plan.mode) {
@@ -476,11 +478,24 @@ int tb_tensor_allocate(tb_tensor t, tb_ctx ctx) {
   TB_API_END
 }
 
+int tb_tensor_attach(tb_tensor t, tb_ctx ctx, void* device_ptr, int64_t bytes) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && ctx != nullptr && device_ptr != nullptr);
+  if(t->p->data != nullptr) fail(TB_ERR_STATE, "tensor already allocated");
+  TB_EXPECTS(bytes >= (int64_t) sizeof(double) * t->p->nelems, "attached storage smaller than the tensor");
+  TB_EXPECTS((reinterpret_cast<uintptr_t>(device_ptr) & 15) == 0, "attached storage must be 16-byte aligned");
+  t->p->data = static_cast<double*>(device_ptr);
+  t->p->owns = false;
+  t->p->ctx  = ctx->p;
+  TB_API_END
+}
+
 int tb_tensor_deallocate(tb_tensor t) {
   TB_API_BEGIN
   REQUIRE_ARG(t != nullptr);
-  if(t->p->data && t->p->ctx) t->p->ctx->arena->deallocate(t->p->data);
+  if(t->p->data && t->p->ctx && t->p->owns) t->p->ctx->arena->deallocate(t->p->data);
   t->p->data = nullptr;
+  t->p->owns = true;
   t->p->ctx.reset();
   TB_API_END
 }
@@ -739,6 +754,160 @@ int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out) {
              "op index out of range (profile the execute first)");
   *out = s->p->prof_stats[index];
   TB_API_END
+}
+
+int tb_sched_dot(tb_sched s, int slot, double alpha, tb_labeled a, tb_labeled b) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  Op op;
+  op.kind  = Op::Dot;
+  op.a     = to_labeled(a);
+  op.b     = to_labeled(b);
+  op.alpha = alpha;
+  op.slot  = slot;
+  TB_EXPECTS(slot >= 0 && slot < Sched::kSlots, "scalar slot out of range (0..63)");
+  TB_EXPECTS(op.a.labels == op.b.labels && op.a.t->keys == op.b.t->keys && op.a.t->offsets == op.b.t->offsets &&
+               op.a.t->nmodes == op.b.t->nmodes,
+             "dot operands need the same labels in the same order over the same block layout");
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
+int tb_sched_norm(tb_sched s, int slot, double alpha, tb_labeled a) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  Op op;
+  op.kind  = Op::Dot;
+  op.a     = to_labeled(a);
+  op.b     = op.a;
+  op.alpha = alpha;
+  op.slot  = slot;
+  op.root  = 1;
+  TB_EXPECTS(slot >= 0 && slot < Sched::kSlots, "scalar slot out of range (0..63)");
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
+int tb_sched_scalars(tb_sched s, double* host, int n) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && host != nullptr);
+  TB_EXPECTS(n >= 0 && n <= Sched::kSlots, "at most 64 scalar slots");
+  TB_CUDA(cudaSetDevice(s->p->ctx->device));
+  TB_CUDA(cudaMemcpyAsync(host, s->p->scalars(), sizeof(double) * n, cudaMemcpyDeviceToHost, s->p->ctx->stream));
+  TB_CUDA(cudaStreamSynchronize(s->p->ctx->stream));
+  TB_API_END
+}
+
+int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const double* eps, int64_t neps,
+                   const double* signs) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && eps != nullptr && signs != nullptr && neps >= 0);
+  Op op;
+  op.kind  = Op::Denom;
+  op.lhs   = to_labeled(t);
+  op.a     = to_labeled(r);
+  op.alpha = alpha;
+  const Tensor& T = *op.lhs.t;
+  TB_EXPECTS(op.lhs.labels == op.a.labels && T.keys == op.a.t->keys && T.offsets == op.a.t->offsets,
+             "denominator update: r needs t's labels and block layout");
+  for(int m = 1; m < T.nmodes; m++)
+    TB_EXPECTS(T.tis[m]->root->is == T.tis[0]->root->is, "denominator update: all modes over one root index space");
+  auto d = std::make_shared<DenomSpec>();
+  d->eps.assign(eps, eps + neps);
+  for(int m = 0; m < T.nmodes; m++) d->signs[m] = signs[m];
+  op.denom = d;
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
+int tb_sched_autotune(tb_sched s, int enable) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  s->p->autotune = enable != 0;
+  TB_API_END
+}
+
+int tb_sched_tune_info(tb_sched s, int64_t index, int* mode, int* tile_n, int* ncand, int* cand_modes,
+                       int* cand_tiles, double* cand_ms, int cap) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  const int64_t n0 = (int64_t) s->p->last_first;
+  TB_EXPECTS(index >= 0 && n0 + index < (int64_t) s->p->start, "op index out of range (execute first)");
+  const Op& op = s->p->ops[n0 + index];
+  auto      it = s->p->tune_cache.find(op.tune_key);
+  if(op.tune_key.empty() || it == s->p->tune_cache.end()) {
+    if(ncand) *ncand = 0;
+    return TB_OK;
+  }
+  const TuneChoice& c = it->second;
+  if(mode) *mode = c.mode;
+  if(tile_n) *tile_n = c.tile_n;
+  if(ncand) *ncand = (int) c.ms.size();
+  for(int i = 0; i < (int) c.ms.size() && i < cap; i++) {
+    if(cand_modes) cand_modes[i] = c.modes[i];
+    if(cand_tiles) cand_tiles[i] = c.tiles[i];
+    if(cand_ms) cand_ms[i] = c.ms[i];
+  }
+  TB_API_END
+}
+
+int tb_sched_graph_create(tb_sched s, tb_graph* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && out != nullptr);
+  Sched&       S     = *s->p;
+  const size_t first = S.start;
+  TB_EXPECTS(first < S.ops.size(), "no queued ops to capture");
+  S.execute(false); // warm-up: plans, work lists, split layouts, autotuner choices
+  TB_CUDA(cudaStreamSynchronize(S.ctx->stream));
+  auto g = std::make_unique<Graph>();
+  g->ctx        = S.ctx;
+  g->pool.arena = S.ctx->arena.get();
+  S.pinned      = &g->pool;
+  cudaStream_t st = S.ctx->stream;
+  TB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+  try {
+    for(size_t i = first; i < S.ops.size(); i++) S.run(S.ops[i]);
+  } catch(...) {
+    cudaGraph_t dead = nullptr;
+    cudaStreamEndCapture(st, &dead);
+    if(dead) cudaGraphDestroy(dead);
+    S.pinned = nullptr;
+    throw;
+  }
+  S.pinned = nullptr;
+  TB_CUDA(cudaStreamEndCapture(st, &g->graph));
+  TB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  for(size_t i = first; i < S.ops.size(); i++)
+    if(S.ops[i].kind == Op::Mult) {
+      g->int8_lists.push_back(S.ops[i].wl);
+      g->plans.push_back(S.ops[i].plan);
+    }
+  auto* h = new tb_graph_s();
+  h->p    = std::move(g);
+  *out    = h;
+  TB_API_END
+}
+
+int tb_graph_launch(tb_graph g) {
+  TB_API_BEGIN
+  REQUIRE_ARG(g != nullptr);
+  TB_CUDA(cudaSetDevice(g->p->ctx->device));
+  TB_CUDA(cudaGraphLaunch(g->p->exec, g->p->ctx->stream));
+  TB_API_END
+}
+
+int tb_graph_sync(tb_graph g) {
+  TB_API_BEGIN
+  REQUIRE_ARG(g != nullptr);
+  TB_CUDA(cudaSetDevice(g->p->ctx->device));
+  TB_CUDA(cudaStreamSynchronize(g->p->ctx->stream));
+  for(const auto& wl: g->p->int8_lists) check_int8_errors(*wl, g->p->ctx->stream);
+  TB_API_END
+}
+
+int tb_graph_destroy(tb_graph g) {
+  delete g;
+  return TB_OK;
 }
 
 int tb_sched_clear(tb_sched s) {

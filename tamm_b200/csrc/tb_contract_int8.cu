@@ -645,10 +645,10 @@ int nt_for(int S) { return S <= 6 ? 80 : 64; }
 
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S) {
+std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S, int NT) {
   auto L = std::make_shared<I8Layout>();
   L->S   = S;
-  L->NT  = nt_for(S);
+  L->NT  = NT;
   std::map<int64_t, int> amap, bmap;
   int64_t                aexp = 0, bexp = 0, abytes = 0, bbytes = 0;
   auto                   strides = [](const int32_t* dims, int n, int64_t* str) {
@@ -871,7 +871,12 @@ void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double
   if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
   launch_split<S>(L, wl, A, B, slices, exps, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
-  launch_gemm<S, (S <= 6 ? 80 : 64)>(L, wl, lc, alpha, slices, exps, C, st);
+  // output tile width: 80 columns by default for S <= 6 (S x NT <= 512 TMEM columns)
+  if constexpr(S * 80 <= 512) {
+    if(L.NT == 80) launch_gemm<S, 80>(L, wl, lc, alpha, slices, exps, C, st);
+  }
+  if(L.NT == 64) launch_gemm<S, 64>(L, wl, lc, alpha, slices, exps, C, st);
+  if(L.NT == 48) launch_gemm<S, 48>(L, wl, lc, alpha, slices, exps, C, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
 }
 
@@ -899,13 +904,17 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
     return;
   }
   const int S = plan.nslices > 0 ? std::min(std::max(plan.nslices, 3), 8) : slices_for(plan.err_target);
-  auto&     L = g_layouts[&wl];
-  if(!L || L->S != S) L = build_layout(lc, wl, S);
+  const int NT = plan.tile_n > 0 ? plan.tile_n : nt_for(S);
+  TB_EXPECTS((NT == 48 || NT == 64 || NT == 80) && S * NT <= 512,
+             "split-INT8 output tile width must be 48, 64 or 80 with slices x width <= 512");
+  auto& L = g_layouts[&wl];
+  if(!L || L->S != S || L->NT != NT) L = build_layout(lc, wl, S, NT);
   Scratch sc;
   sc.stream = stream;
   sc.arena  = plan.arena;
-  auto* slices = static_cast<uint8_t*>(sc.get(L->slice_bytes));
-  auto* exps   = static_cast<int32_t*>(sc.get(sizeof(int32_t) * std::max<int64_t>(L->nexp, 1)));
+  const int64_t ebytes = sizeof(int32_t) * std::max<int64_t>(L->nexp, 1);
+  auto* slices = static_cast<uint8_t*>(plan.pinned ? plan.pinned->get(L->slice_bytes) : sc.get(L->slice_bytes));
+  auto* exps   = static_cast<int32_t*>(plan.pinned ? plan.pinned->get(ebytes) : sc.get(ebytes));
   cudaEvent_t  evs[3];
   cudaEvent_t* ev = nullptr;
   if(plan.profile) {
@@ -920,8 +929,14 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
     case 7: run_s<7>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
     default: run_s<8>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
   }
-  sc.put(exps);
-  sc.put(slices);
+  if(plan.pinned) {
+    plan.pinned->put(exps);
+    plan.pinned->put(slices);
+  }
+  else {
+    sc.put(exps);
+    sc.put(slices);
+  }
   if(ev) {
     float a = 0, b = 0;
     TB_CUDA(cudaEventSynchronize(evs[2]));
@@ -967,6 +982,20 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
 }
 
 void forget_int8_layout(const WorkList* wl) { g_layouts.erase(wl); }
+
+int int8_slices_for(double err_target) { return slices_for(err_target); }
+
+void check_int8_errors(const WorkList& wl, cudaStream_t stream) {
+  auto it = g_layouts.find(&wl);
+  if(it == g_layouts.end() || !it->second) return;
+  int h = 0;
+  TB_CUDA(cudaMemcpyAsync(&h, it->second->d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  TB_CUDA(cudaStreamSynchronize(stream));
+  if(h != 0) {
+    cudaMemsetAsync(it->second->d_err, 0, sizeof(int), stream);
+    fail(TB_ERR_TIMEOUT, "split-INT8 contraction: a device-side wait gave up (code " + std::to_string(h) + ")");
+  }
+}
 
 void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
                      double* C, cudaStream_t stream) {

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/tamm_b200.h"
@@ -91,6 +92,17 @@ struct WorkList {
 
 class Arena;
 
+// Scratch of a captured CUDA graph: buffers stay allocated for the graph's lifetime;
+// ops of the graph run in stream order, so a buffer returned by one op can serve the
+// next.  The graph holds the largest scratch of one op, not the sum.
+struct CapturePool {
+  Arena*                                    arena = nullptr;
+  std::vector<std::tuple<void*, int64_t, bool>> bufs; // pointer, bytes, in use
+  void*                                     get(int64_t bytes);
+  void                                      put(void* p);
+  void                                      release(); // back to the arena
+};
+
 struct Plan {
   LabelClasses lc;
   int          mode       = TB_MODE_FP64;
@@ -98,11 +110,17 @@ struct Plan {
   int          nslices    = 0;
   tb_stats     last{};
   Arena*       arena        = nullptr; // scratch source (null: cudaMallocAsync)
+  int          tile_n       = 0;       // split-INT8 output tile width (0: default for S)
   bool         check_errors = true;    // read the device error word after a launch
+  // while a CUDA graph is being captured: scratch comes from (and returns to) this
+  // pool, which keeps it allocated for the graph's replays
+  struct CapturePool* pinned = nullptr;
   bool         profile      = false;   // time the phases with CUDA events (synchronises)
 };
 
 void forget_int8_layout(const WorkList* wl);
+// Largest split-INT8 slice count the error target needs (3..8).
+int int8_slices_for(double err_target);
 
 // ---- launchers (device code in *.cu) ----
 void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,
@@ -127,6 +145,25 @@ void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream);
 double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream);
+// *out = scale * x.y (root: scale * sqrt(x.x)), staying on the device; part holds
+// 1024 doubles of scratch.  y == nullptr means x.x.
+void launch_dot_to(const double* x, const double* y, int64_t n, double scale, int root, double* out, double* part,
+                   cudaStream_t stream);
+// One admitted block of a denominator update: packed offset, dims, and the root
+// orbital index of each mode's first element.
+struct DenomBlock {
+  int64_t off;
+  int64_t dims[kMaxModes];
+  int64_t first[kMaxModes];
+};
+struct DenomSigns {
+  double s[kMaxModes];
+};
+void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
+                  const double* eps, DenomSigns signs, cudaStream_t stream);
+// Reads and clears the device error word of the split-INT8 launches of a work list;
+// throws TB_ERR_TIMEOUT if a device-side wait gave up.
+void check_int8_errors(const WorkList& wl, cudaStream_t stream);
 void   launch_fill_random(double* x, int64_t n, uint64_t seed, uint64_t first, int dist, double p0,
                           double p1, cudaStream_t stream);
 

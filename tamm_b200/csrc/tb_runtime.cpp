@@ -86,6 +86,31 @@ void Scratch::put(void* p) {
   else TB_CUDA(cudaFreeAsync(p, stream));
 }
 
+void* CapturePool::get(int64_t bytes) {
+  bytes = std::max<int64_t>(bytes, 1);
+  int best = -1;
+  for(int i = 0; i < (int) bufs.size(); i++)
+    if(!std::get<2>(bufs[i]) && std::get<1>(bufs[i]) >= bytes &&
+       (best < 0 || std::get<1>(bufs[i]) < std::get<1>(bufs[best])))
+      best = i;
+  if(best < 0) {
+    bufs.emplace_back(arena->allocate(bytes), bytes, false);
+    best = (int) bufs.size() - 1;
+  }
+  std::get<2>(bufs[best]) = true;
+  return std::get<0>(bufs[best]);
+}
+
+void CapturePool::put(void* p) {
+  for(auto& b: bufs)
+    if(std::get<0>(b) == p) std::get<2>(b) = false;
+}
+
+void CapturePool::release() {
+  for(auto& b: bufs) arena->deallocate(std::get<0>(b));
+  bufs.clear();
+}
+
 Ctx::~Ctx() {
   if(stream) {
     cudaSetDevice(device);
@@ -506,6 +531,52 @@ void Sched::run(Op& op) {
     }
     return;
   }
+  if(op.kind == Op::Dot) {
+    op.a.t->require_allocated();
+    op.b.t->require_allocated();
+    TB_EXPECTS(op.slot >= 0 && op.slot < kSlots, "scalar slot out of range (0..63)");
+    launch_dot_to(op.a.t->data, op.root ? nullptr : op.b.t->data, op.a.t->nelems, op.alpha, op.root,
+                  scalars() + op.slot, scalars() + kSlots, st);
+    return;
+  }
+  if(op.kind == Op::Denom) {
+    op.lhs.t->require_allocated();
+    op.a.t->require_allocated();
+    DenomSpec& d = *op.denom;
+    if(!d.d_blocks) { // block table of the update: packed offsets, dims, first orbital index
+      const Tensor&           T = *op.lhs.t;
+      std::vector<DenomBlock> blocks;
+      std::vector<int64_t>    id(T.nmodes);
+      for(size_t bi = 0; bi < T.keys.size(); bi++) {
+        int64_t key = T.keys[bi]; // block id in each mode's own tile numbering
+        for(int m = T.nmodes - 1; m >= 0; m--) {
+          const int64_t n = T.tis[m]->ntiles();
+          id[m]           = key % n;
+          key /= n;
+        }
+        DenomBlock b{};
+        b.off = T.offsets[bi];
+        for(int m = 0; m < T.nmodes; m++) {
+          const int64_t r = T.tis[m]->tiles[id[m]]; // root tile
+          b.dims[m]       = T.tis[m]->root->offsets[r + 1] - T.tis[m]->root->offsets[r];
+          b.first[m]      = T.tis[m]->root->offsets[r];
+          TB_EXPECTS(b.first[m] + b.dims[m] <= (int64_t) d.eps.size(), "orbital energies shorter than the index space");
+        }
+        blocks.push_back(b);
+      }
+      d.ctx     = ctx;
+      d.nblocks = (int) blocks.size();
+      TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d.d_eps), sizeof(double) * std::max<size_t>(d.eps.size(), 1)));
+      TB_CUDA(cudaMemcpy(d.d_eps, d.eps.data(), sizeof(double) * d.eps.size(), cudaMemcpyHostToDevice));
+      TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d.d_blocks), sizeof(DenomBlock) * std::max<size_t>(blocks.size(), 1)));
+      if(!blocks.empty())
+        TB_CUDA(cudaMemcpy(d.d_blocks, blocks.data(), sizeof(DenomBlock) * blocks.size(), cudaMemcpyHostToDevice));
+    }
+    DenomSigns sg{};
+    for(int m = 0; m < kMaxModes; m++) sg.s[m] = d.signs[m];
+    launch_denom(op.lhs.t->data, op.a.t->data, op.alpha, d.d_blocks, d.nblocks, op.lhs.t->nmodes, d.d_eps, sg, st);
+    return;
+  }
   // MultOp
   op.lhs.t->require_allocated();
   op.a.t->require_allocated();
@@ -530,15 +601,128 @@ void Sched::run(Op& op) {
   op.plan->mode       = ctx->mode;
   op.plan->err_target = ctx->err_target;
   op.plan->nslices    = ctx->nslices;
-  op.plan->profile    = profiling;
-  op.flops            = op.wl->flops;
+  op.plan->tile_n     = 0;
+  if(autotune && ctx->mode == TB_MODE_INT8 && !pinned) {
+    const std::string key = signature(op) + "|" + std::to_string(ctx->err_target) + "|" + std::to_string(ctx->nslices);
+    auto              it  = tune_cache.find(key);
+    if(it == tune_cache.end()) {
+      tune(op, key);
+      it = tune_cache.find(key);
+    }
+    op.plan->mode   = it->second.mode;
+    op.plan->tile_n = it->second.tile_n;
+    op.tune_key     = key;
+  }
+  else if(autotune && ctx->mode == TB_MODE_INT8) { // capturing: the warm-up run tuned already
+    auto it = tune_cache.find(signature(op) + "|" + std::to_string(ctx->err_target) + "|" +
+                              std::to_string(ctx->nslices));
+    if(it != tune_cache.end()) {
+      op.plan->mode   = it->second.mode;
+      op.plan->tile_n = it->second.tile_n;
+    }
+  }
+  op.plan->profile      = profiling;
+  op.plan->pinned       = pinned;
+  op.plan->check_errors = pinned == nullptr;
+  op.flops              = op.wl->flops;
   run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
                ctx->arena.get());
-  op.plan->profile = false;
+  op.plan->profile      = false;
+  op.plan->pinned       = nullptr;
+  op.plan->check_errors = true;
+}
+
+// Autotuner: each candidate (the FP64 kernel, the split-INT8 kernel at output tile
+// widths 80 / 64 / 48 where the slice count allows) runs once to warm up and once
+// timed with CUDA events, from the same saved copy of C; C is restored and the
+// fastest candidate is kept for this signature and precision request.
+void Sched::tune(Op& op, const std::string& key) {
+  TuneChoice   ch;
+  cudaStream_t st = ctx->stream;
+  const LabelClasses& lc = op.plan->lc;
+  std::vector<std::pair<int, int>> cand{{TB_MODE_FP64, 0}};
+  const bool int8_kernel = !(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0);
+  if(int8_kernel) {
+    const int S = ctx->nslices > 0 ? std::min(std::max(ctx->nslices, 3), 8) : int8_slices_for(ctx->err_target);
+    for(int nt: {80, 64, 48})
+      if(S * nt <= 512) cand.push_back({TB_MODE_INT8, nt});
+  }
+  if(cand.size() == 1) {
+    ch.mode = TB_MODE_INT8; // nothing to choose: the INT8 request runs its FP64 route
+    tune_cache[key] = ch;
+    return;
+  }
+  Tensor&       C     = *op.lhs.t;
+  const int64_t bytes = (int64_t) sizeof(double) * std::max<int64_t>(C.nelems, 1);
+  double*       save  = static_cast<double*>(ctx->arena->allocate(bytes));
+  TB_CUDA(cudaMemcpyAsync(save, C.data, bytes, cudaMemcpyDeviceToDevice, st));
+  cudaEvent_t e0, e1;
+  TB_CUDA(cudaEventCreate(&e0));
+  TB_CUDA(cudaEventCreate(&e1));
+  double best = 1e300;
+  for(const auto& c: cand) {
+    op.plan->mode   = c.first;
+    op.plan->tile_n = c.second;
+    float ms        = 0;
+    for(int rep = 0; rep < 2; rep++) {
+      TB_CUDA(cudaMemcpyAsync(C.data, save, bytes, cudaMemcpyDeviceToDevice, st));
+      TB_CUDA(cudaEventRecord(e0, st));
+      run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, C.data, st, ctx->arena.get());
+      TB_CUDA(cudaEventRecord(e1, st));
+      TB_CUDA(cudaEventSynchronize(e1));
+      TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    }
+    ch.modes.push_back(c.first);
+    ch.tiles.push_back(c.second);
+    ch.ms.push_back(ms);
+    if(ms < best) {
+      best      = ms;
+      ch.mode   = c.first;
+      ch.tile_n = c.second;
+    }
+  }
+  TB_CUDA(cudaMemcpyAsync(C.data, save, bytes, cudaMemcpyDeviceToDevice, st));
+  TB_CUDA(cudaStreamSynchronize(st));
+  ctx->arena->deallocate(save);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tune_cache[key] = ch;
+}
+
+double* Sched::scalars() {
+  if(!d_scalars) {
+    TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_scalars), sizeof(double) * (kSlots + 1024)));
+    TB_CUDA(cudaMemset(d_scalars, 0, sizeof(double) * (kSlots + 1024)));
+  }
+  return d_scalars;
+}
+
+Sched::~Sched() {
+  if(d_scalars) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_scalars);
+  }
+}
+
+DenomSpec::~DenomSpec() {
+  if(ctx) cudaSetDevice(ctx->device);
+  if(d_eps) cudaFree(d_eps);
+  if(d_blocks) cudaFree(d_blocks);
+}
+
+Graph::~Graph() {
+  if(!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if(exec) cudaGraphExecDestroy(exec);
+  if(graph) cudaGraphDestroy(graph);
+  pool.release();
 }
 
 void Sched::execute(bool profile) {
   TB_CUDA(cudaSetDevice(ctx->device));
+  last_first = start;
   prof_ms.clear();
   prof_flops.clear();
   prof_stats.clear();

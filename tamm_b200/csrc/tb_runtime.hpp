@@ -90,6 +90,7 @@ struct Tensor {
   int64_t                           nelems = 0;
   std::shared_ptr<Ctx>              ctx;
   double*                           data   = nullptr;
+  bool                              owns   = true; // false: storage attached by the caller
 
   void    build_table(); // Distribution_NW (distribution.hpp:201-243)
   bool    is_non_zero(const int64_t* blockid) const;
@@ -107,14 +108,21 @@ struct Labeled {
   std::vector<std::shared_ptr<TIS>> ltis; // label space per mode
 };
 
+struct DenomSpec;
+
 // tb_labeled (C ABI) -> Labeled; NULL label spaces mean the tensor's own.
 Labeled labeled_from_c(const tb_labeled& x);
 
 struct Op {
-  enum Kind { Set, Add, Mult } kind;
+  // Dot: scalar slot `slot` = alpha * sum a * b (root: alpha * sqrt(sum a * a)), kept on
+  // the device; Denom: lhs += alpha * a / D with the orbital-energy denominator D.
+  enum Kind { Set, Add, Mult, Dot, Denom } kind;
   Labeled lhs, a, b;
   double  alpha = 1.0, value = 0.0;
   int     is_assign = 0;
+  int     slot = 0, root = 0;
+  std::shared_ptr<DenomSpec> denom;
+  std::string                tune_key; // set when the autotuner chose this op's kernel
   // cached execution state
   std::shared_ptr<Plan>     plan;
   std::shared_ptr<WorkList> wl;
@@ -128,17 +136,57 @@ struct Op {
   double                                 flops = 0;
 };
 
+// Orbital energies over a root index space (device copy) and per-mode signs of a
+// denominator update, with the block table built on first use.
+struct DenomSpec {
+  std::vector<double>     eps;   // host copy, indexed by root orbital index
+  double                  signs[kMaxModes] = {0};
+  double*                 d_eps    = nullptr;
+  DenomBlock*             d_blocks = nullptr;
+  int                     nblocks  = 0;
+  std::shared_ptr<Ctx>    ctx;
+  ~DenomSpec();
+};
+
+// Choice of the autotuner for one contraction signature and precision request.
+struct TuneChoice {
+  int                 mode   = TB_MODE_FP64;
+  int                 tile_n = 0;
+  std::vector<double> ms;     // timed candidates, in candidate order
+  std::vector<int>    modes, tiles;
+};
+
 struct Sched {
   std::shared_ptr<Ctx>                              ctx;
   std::vector<Op>                                   ops;
-  size_t                                            start = 0;
+  size_t                                            start = 0, last_first = 0; // ops[last_first, start): last execute
   std::vector<double>                               prof_ms, prof_flops;
   std::vector<tb_stats>                             prof_stats;
   bool                                              profiling = false;
   std::map<std::string, std::shared_ptr<Plan>>     plan_cache;
   std::map<std::string, std::shared_ptr<WorkList>> wl_cache;
+  static constexpr int                              kSlots = 64;
+  double*                                           d_scalars = nullptr; // kSlots + 1024 partials
+  bool                                              autotune  = false;
+  std::map<std::string, TuneChoice>                 tune_cache;
+  CapturePool*                                      pinned = nullptr; // set while capturing a graph
   void                                              execute(bool profile);
   void                                              run(Op& op);
+  void                                              tune(Op& op, const std::string& key);
+  double*                                           scalars();
+  ~Sched();
+};
+
+// A captured sequence of scheduler ops: replayed with one graph launch.  Holds the
+// scratch the capture used and the work lists whose error words are checked.
+struct Graph {
+  std::shared_ptr<Ctx>                   ctx;
+  cudaGraph_t                            graph = nullptr;
+  cudaGraphExec_t                        exec  = nullptr;
+  CapturePool                            pool;
+  std::vector<std::shared_ptr<WorkList>> int8_lists;
+  std::vector<std::shared_ptr<Plan>>     plans;
+  ~Graph();
 };
 
 // scratch memory source for split operands
@@ -165,6 +213,9 @@ struct tb_tensor_s {
 };
 struct tb_sched_s {
   std::unique_ptr<tb::Sched> p;
+};
+struct tb_graph_s {
+  std::unique_ptr<tb::Graph> p;
 };
 struct tb_plan_s {
   tb::Plan p;

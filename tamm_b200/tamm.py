@@ -238,6 +238,13 @@ class Tensor:
         call("tb_tensor_deallocate", self.h)
         self.ec = None
 
+    def attach(self, ec: ExecutionContext, device_ptr: int, nbytes: int):
+        """Caller-owned device storage (>= 8 * nelems bytes, 16-byte aligned), e.g. one
+        buffer shared by tensors used one after another in stream order."""
+        call("tb_tensor_attach", self.h, ec.h, C.c_void_p(device_ptr), int(nbytes))
+        self.ec = ec
+        return self
+
     def data_ptr(self):
         p = A.vp()
         call("tb_tensor_data", self.h, C.byref(p))
@@ -455,6 +462,57 @@ class Scheduler:
         call("tb_sched_profile", self.h, C.byref(n), ms.ctypes.data_as(A.dp), fl.ctypes.data_as(A.dp), n.value)
         return ms[:n.value], fl[:n.value]
 
+    # --- device scalars, denominator update, autotuner, CUDA graphs ---
+    def dot(self, slot: int, a: LabeledTensor, b: LabeledTensor, alpha: float = 1.0):
+        """Queue scalar slot = alpha * sum a * b (same labels and block layout)."""
+        ids: dict = {}
+        call("tb_sched_dot", self.h, int(slot), float(alpha), self._labeled(a, ids), self._labeled(b, ids))
+        return self
+
+    def norm(self, slot: int, a: LabeledTensor, alpha: float = 1.0):
+        """Queue scalar slot = alpha * sqrt(sum a * a)."""
+        call("tb_sched_norm", self.h, int(slot), float(alpha), self._labeled(a, {}))
+        return self
+
+    def scalars(self, n: int = 64) -> np.ndarray:
+        out = np.zeros(n)
+        call("tb_sched_scalars", self.h, out.ctypes.data_as(A.dp), int(n))
+        return out
+
+    def denom(self, t: LabeledTensor, alpha: float, r: LabeledTensor, eps, signs):
+        """Queue t += alpha * r / D, D = sum_m signs[m] * eps[orbital index of mode m]."""
+        ids: dict = {}
+        e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+        sg = np.ascontiguousarray(np.asarray(list(signs) + [0.0] * (8 - len(signs)), dtype=np.float64))
+        self._keep += [e, sg]
+        call("tb_sched_denom", self.h, self._labeled(t, ids), float(alpha), self._labeled(r, ids),
+             e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
+        return self
+
+    def autotune(self, enable: bool = True):
+        call("tb_sched_autotune", self.h, int(bool(enable)))
+        return self
+
+    def tune_info(self, index: int):
+        """Autotuner choice for op `index` of the last execute: None if not tuned, else
+        dict(mode, tile_n, candidates=[(mode, tile_n, ms), ...])."""
+        mode, tile, nc = C.c_int(), C.c_int(), C.c_int()
+        cm = (C.c_int * 8)()
+        ct = (C.c_int * 8)()
+        ms = (C.c_double * 8)()
+        call("tb_sched_tune_info", self.h, int(index), C.byref(mode), C.byref(tile), C.byref(nc),
+             C.cast(cm, A.ip), C.cast(ct, A.ip), C.cast(ms, A.dp), 8)
+        if nc.value == 0:
+            return None
+        return {"mode": mode.value, "tile_n": tile.value,
+                "candidates": [(cm[i], ct[i], ms[i]) for i in range(min(nc.value, 8))]}
+
+    def graph(self) -> "Graph":
+        """Run the queued ops once, then capture them into a CUDA graph."""
+        g = A.h()
+        call("tb_sched_graph_create", self.h, C.byref(g))
+        return Graph(g, self)
+
     def op_stats(self, index=-1):
         """Kernel statistics (dict) of one op of the last profiled execute."""
         n = C.c_int64()
@@ -468,6 +526,29 @@ class Scheduler:
     def __del__(self):
         try:
             A.lib().tb_sched_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Graph:
+    """A captured sequence of scheduler ops; launch() enqueues one replay on the
+    context's stream, sync() waits and checks the device error words."""
+
+    def __init__(self, handle, sched):
+        self.h = handle
+        self._sched = sched  # keeps the ops' tensors and the scheduler alive
+
+    def launch(self):
+        call("tb_graph_launch", self.h)
+        return self
+
+    def sync(self):
+        call("tb_graph_sync", self.h)
+        return self
+
+    def __del__(self):
+        try:
+            A.lib().tb_graph_destroy(self.h)
         except Exception:
             pass
 
