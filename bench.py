@@ -98,10 +98,11 @@ class ClockSampler:
 
 def measured_peak(torch, kind):
     """Live cuBLAS throughput on this GPU, the denominator for kernels without a
-    driver-measured peak: FP64 DGEMM (torch.matmul float64) or INT8 (torch._int_mm)."""
+    driver-measured peak: FP64 DGEMM (torch.matmul float64), BF16 (torch.matmul bfloat16)
+    or INT8 (torch._int_mm)."""
     n = 8192
-    if kind == "fp64":
-        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    if kind in ("fp64", "bf16"):
+        a = torch.randn(n, n, dtype=torch.float64 if kind == "fp64" else torch.bfloat16, device="cuda")
         f = lambda: torch.matmul(a, a)  # noqa: E731
     else:
         a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
@@ -316,19 +317,27 @@ def main():
     step(profile=True)
     st = lad.sch.op_stats(-1)
     peaks = load_peaks()
-    if headline == "int8":
+    if headline in ("int8", "bf16x3"):
         S = st["slices_max"]
-        peak = measured_peak(torch, "int8")
         achieved = st["int8_ops"] / (st["gemm_ms"] * 1e-3) / 1e12
+        if headline == "int8":
+            peak = measured_peak(torch, "int8")
+            kernel, src = f"k_contract_i8<S={S}> (tcgen05 kind::i8)", (
+                "measured live: cuBLASLt INT8 GEMM (torch._int_mm) 8192^3 on this GPU; "
+                "MEASURED_PEAKS.json has no INT8 figure")
+            ops = "INT8 tensor ops (2 per multiply-add) incl. padding to 128x80x32 tiles"
+        else:
+            peak = peaks.get("bf16_tflops") or measured_peak(torch, "bf16")
+            kernel, src = "k_contract_i8<S=2, bf16> (tcgen05 kind::f16, bf16 A/B, f32 accumulate)", (
+                "MEASURED_PEAKS.json bf16_tflops (measured burst cuBLAS bf16 GEMM)")
+            ops = "BF16 tensor FLOPs (2 per multiply-add, 3 piece products) incl. padding to 128x80x16 tiles"
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "kernel": f"k_contract_i8<S={S}> (tcgen05 kind::i8)",
-                "ops": "INT8 tensor ops (2 per multiply-add) incl. padding to 128x80x32 tiles",
-                "peak_source": "measured live: cuBLASLt INT8 GEMM (torch._int_mm) 8192^3 on this GPU; "
-                               "MEASURED_PEAKS.json has no INT8 figure",
+                "traffic": None, "kernel": kernel, "ops": ops, "peak_source": src,
                 "gemm_ms": st["gemm_ms"], "split_ms": st["split_ms"]}
-        # the split pass is HBM-bound: FP64 read + S digit bytes written per operand element
+        # the split pass is HBM-bound: FP64 read + S digit bytes (bf16 pieces: 2 bytes
+        # each) written per operand element
         nsplit = lad.v.nelems + lad.t2.nelems
-        split_bytes = nsplit * (8 + S) + 0.0
+        split_bytes = nsplit * (8 + S * (2 if headline == "bf16x3" else 1)) + 0.0
         hbm = peaks.get("hbm_gbs")
         roof["split"] = {"bound": "hbm", "achieved": split_bytes / (st["split_ms"] * 1e-3) / 1e9,
                          "peak": hbm, "unit": "GB/s",
@@ -352,7 +361,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"fp64": "f64", "int8": "s8 balanced digits, s32 accumulate, f64 recombination",
-                                           "bf16x3": "bf16x3"}[headline],
+                                           "bf16x3": "bf16 hi+lo pieces, f32 accumulate, f64 recombination"}[headline],
             "data": "synthetic (seeded; no dataset)",
             "config": {"workload": f"ccsd_ladder_O{2*args.oa}_V{2*args.va}", "mode": headline,
                        "contraction": "r2(a,b,i,j) += v(a,b,c,d) * t2(c,d,i,j), spin-blocked, virt tiles U{24..48}",

@@ -28,6 +28,8 @@
 #include "tb_runtime.hpp"
 #include "tb_sm100.cuh"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -117,7 +119,12 @@ __device__ __forceinline__ int row_exponent(double mx) {
 // j0..j1 of a B tile form one UMMA operand of (j1 - j0 + 1) x NT rows.  Residency (four CTAs per SM at 60 registers)
 // bounds the rows held in L2 between the phases to 4 x 148 x 8 rows (87 MB at K =
 // 2304, within the 126 MB L2).
-template<int S>
+//
+// BF (the BF16x3 mode, S = 2): the row is scaled by 2^-e and each value x cut into two
+// bf16 pieces, hi = bf16(x) and lo = bf16(x - hi) (round to nearest), in the same
+// layout with 2-byte elements: a 16-byte core-matrix row holds 8 values, thread
+// (row r, pair q) converts k = 2q, 2q+1 of an 8-value column.
+template<int S, bool BF>
 __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restrict__ blocks,
                                                      const int2* __restrict__ chunks, int nchunks,
                                                      const double* __restrict__ src, uint8_t* __restrict__ dst,
@@ -171,7 +178,7 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
       for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       if(lane == 0) {
         const int e = row_exponent(mx);
-        s_sh[warp]  = live ? 8 * S - 1 - e : kPadRow;
+        s_sh[warp]  = live ? (BF ? -e : 8 * S - 1 - e) : kPadRow;
         s_off[warp] = rowoff;
         exps[b.exp_off + row] = e;
         if(mx > 0.0) atomicMax(blockmax + b.id, e);
@@ -184,48 +191,79 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
     const double* s    = src + b.src_off + s_off[r];
     // 2^sh as two factors, so that no factor overflows for extreme row exponents
     const double f1  = ldexp(1.0, live ? sh / 2 : 0), f2 = ldexp(1.0, live ? sh - sh / 2 : 0);
-    const int    g8  = (ch.y % b.tile_rows) >> 3;
-    const int    nkc = b.K_pad / KC;
-    uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
-                   q * 4;
-    const bool vec = live && b.kcontig && !(reinterpret_cast<uintptr_t>(s) & 15);
-    for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) {
-      const int k0 = k16 * 16 + q * 4;
-      double    v[4];
-      if(vec && k0 + 3 < b.K) {
-        const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
-        const double2 v23 = __ldg(reinterpret_cast<const double2*>(s + k0 + 2));
-        v[0] = v01.x, v[1] = v01.y, v[2] = v23.x, v[3] = v23.y;
-      }
-      else
+    const int g8 = (ch.y % b.tile_rows) >> 3;
+    if constexpr(BF) {
+      const int nkc = b.K_pad * 2 / KC;
+      uint8_t*  out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 +
+                     r * 16 + q * 4;
+      const bool vec = live && b.kcontig && !(reinterpret_cast<uintptr_t>(s) & 15);
+      for(int k8 = warp; k8 < b.K_pad / 8; k8 += 8) {
+        const int k0 = k8 * 8 + q * 2;
+        double    v[2];
+        if(vec && k0 + 1 < b.K) {
+          const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
+          v[0] = v01.x, v[1] = v01.y;
+        }
+        else
 #pragma unroll
+          for(int x = 0; x < 2; x++) v[x] = (live && k0 + x < b.K) ? __ldg(s + koff(b, k0 + x)) : 0.0;
+        uint32_t hi = 0, lo = 0;
+#pragma unroll
+        for(int x = 0; x < 2; x++) {
+          const double         y = v[x] * f1 * f2;
+          const __nv_bfloat16  h = __double2bfloat16(y);
+          const __nv_bfloat16  t = __double2bfloat16(y - (double) __bfloat162float(h));
+          hi |= (uint32_t) __bfloat16_as_ushort(h) << (16 * x);
+          lo |= (uint32_t) __bfloat16_as_ushort(t) << (16 * x);
+        }
+        uint8_t* o = out + (int64_t) (k8 >> 1) * S * b.tile_rows * KC + (k8 & 1) * S * b.tile_rows * 16;
+        *reinterpret_cast<uint32_t*>(o)                      = hi;
+        *reinterpret_cast<uint32_t*>(o + b.tile_rows * 16) = lo;
+      }
+    }
+    else {
+      const int    nkc = b.K_pad / KC;
+      uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
+                     q * 4;
+      const bool vec = live && b.kcontig && !(reinterpret_cast<uintptr_t>(s) & 15);
+      for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) {
+        const int k0 = k16 * 16 + q * 4;
+        double    v[4];
+        if(vec && k0 + 3 < b.K) {
+          const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
+          const double2 v23 = __ldg(reinterpret_cast<const double2*>(s + k0 + 2));
+          v[0] = v01.x, v[1] = v01.y, v[2] = v23.x, v[3] = v23.y;
+        }
+        else
+  #pragma unroll
+          for(int x = 0; x < 4; x++) {
+            const int k = k0 + x;
+            v[x]        = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
+          }
+        uint32_t lo[4], hi[4];
+  #pragma unroll
         for(int x = 0; x < 4; x++) {
-          const int k = k0 + x;
-          v[x]        = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
+          const uint64_t Y = (uint64_t) __double2ll_rn(v[x] * f1 * f2) + bias;
+          lo[x]            = (uint32_t) Y;
+          hi[x]            = (uint32_t) (Y >> 32);
         }
-      uint32_t lo[4], hi[4];
-#pragma unroll
-      for(int x = 0; x < 4; x++) {
-        const uint64_t Y = (uint64_t) __double2ll_rn(v[x] * f1 * f2) + bias;
-        lo[x]            = (uint32_t) Y;
-        hi[x]            = (uint32_t) (Y >> 32);
-      }
-      uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
-#pragma unroll
-      for(int i = 0; i < S; i++) {
-        const int p = S - 1 - i; // byte of Y holding digit i
-        uint32_t  w;
-        if(p < 4) {
-          const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
-          const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
-          w                 = __byte_perm(t0, t1, 0x5410);
+        uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
+  #pragma unroll
+        for(int i = 0; i < S; i++) {
+          const int p = S - 1 - i; // byte of Y holding digit i
+          uint32_t  w;
+          if(p < 4) {
+            const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
+            const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          else {
+            const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
+            const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * 16) = w ^ 0x80808080u;
         }
-        else {
-          const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
-          const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
-          w                 = __byte_perm(t0, t1, 0x5410);
-        }
-        *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * 16) = w ^ 0x80808080u;
       }
     }
     __syncthreads(); // s_sh / s_off are rewritten for the next chunk
@@ -293,7 +331,9 @@ constexpr size_t smem_bytes() {
   return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail;
 }
 
-template<int S, int NT>
+// BF: the BF16x3 mode (S = 2 bf16 pieces, kind::f16 MMAs with FP32 accumulators; both
+// diagonals carry the same power of two, 2^(e_row + e_col)).
+template<int S, int NT, bool BF>
 __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   static_assert(S * NT <= 512, "TMEM holds 512 columns");
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -428,7 +468,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                     tc_fence_after();
                   }
                 const uint64_t bd = umma_desc_kmajor(b0 + j0 * NT * 16, S * NT * 16, 128);
-                mma_i8(tmem + (i + j0) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), kc > 0 || i > 0);
+                if constexpr(BF) mma_f16(tmem + (i + j0) * NT, ad, bd, idesc_bf16(MT, nd * NT), kc > 0 || i > 0);
+                else mma_i8(tmem + (i + j0) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), kc > 0 || i > 0);
               }
             }
             if(kc == 0) // keep the unused diagonals' barriers in phase
@@ -524,7 +565,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         const int    st  = p.tslices[t];
         const int    er  = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
         double*      scb = sc + (tcount & 1) * NT;
-        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - 7);
+        constexpr int off = BF ? 0 : 7; // digit weights: 2^(e - 7 - 8d) (INT8), 2^e (BF16 pieces)
+        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - off);
         // the epilogue threads agree on a timeout, so none is left in a barrier; the
         // barrier also publishes the scales
         const bool     waited = mbar_wait(tfull, tphase, p.err, 4);
@@ -545,8 +587,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         // v * 2^k = (2^52 + 2^31 + v) * 2^k - (2^52 + 2^31) * 2^k, whose first term is
         // assembled from its bits (high word: exponent 1075 + k, low word: v + 2^31) —
         // exact, with no conversion instruction and no multiply.
-        const bool   fast = er - 7 - 8 * (S - 1) >= -1000 && er - 7 <= 900;
-        const double sr   = ldexp(1.0, er - 7);
+        const bool   fast = !BF && er - 7 - 8 * (S - 1) >= -1000 && er - 7 <= 900;
+        const double sr   = ldexp(1.0, er - off);
         // drain diagonal by diagonal; each diagonal's TMEM is released as soon as it
         // has been read, so the next task's MMAs into it can start
 #pragma unroll
@@ -566,6 +608,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 #pragma unroll
               for(int x = 0; x < NH; x++)
                 racc[x] = fma(__hiloint2double(hi, (int) (v[x] ^ 0x80000000u)) - bias, scb[col0 + x], racc[x]);
+            }
+            else if constexpr(BF) { // FP32 accumulators, exact in FP64
+#pragma unroll
+              for(int x = 0; x < NH; x++) racc[x] = fma((double) __uint_as_float(v[x]), sr * scb[col0 + x], racc[x]);
             }
             else {
               const double w = pow2i(-8 * d) * sr;
@@ -602,7 +648,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 // ---------------------------------------------------------------- host side
 
 struct I8Layout {
-  int                     S = 0, NT = 0;
+  int                     S = 0, NT = 0, esize = 1; // digits, output tile width, bytes per digit
   std::vector<SplitBlock> a_blocks, b_blocks;
   std::vector<int2>       a_chunks, b_chunks;
   std::vector<I8Task>     tasks;
@@ -645,10 +691,12 @@ int nt_for(int S) { return S <= 6 ? 80 : 64; }
 
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S, int NT) {
-  auto L = std::make_shared<I8Layout>();
-  L->S   = S;
-  L->NT  = NT;
+std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S, int NT, int esize) {
+  auto L   = std::make_shared<I8Layout>();
+  L->S     = S;
+  L->NT    = NT;
+  L->esize = esize;
+  const int kstep = KC / esize; // K elements per 32-byte MMA step
   std::map<int64_t, int> amap, bmap;
   int64_t                aexp = 0, bexp = 0, abytes = 0, bbytes = 0;
   auto                   strides = [](const int32_t* dims, int n, int64_t* str) {
@@ -690,10 +738,10 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
         b.id        = (int32_t) L->a_blocks.size();
         b.tile_rows = MT;
         b.rows_pad  = (int32_t) rup(b.rows, MT);
-        b.K_pad     = (int32_t) rup(K, KC);
+        b.K_pad     = (int32_t) rup(K, kstep);
         b.dst_off   = abytes;
         b.exp_off   = (int32_t) aexp;
-        abytes += (int64_t) b.rows_pad * b.K_pad * S;
+        abytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
         aexp += b.rows_pad;
         ia = amap.emplace(tk.a_off, (int) L->a_blocks.size()).first;
         L->a_blocks.push_back(b);
@@ -720,10 +768,10 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
         b.id        = (int32_t) L->b_blocks.size(); // rebased after the A blocks below
         b.tile_rows = L->NT;
         b.rows_pad  = (int32_t) rup(b.rows, L->NT);
-        b.K_pad     = (int32_t) rup(K, KC);
+        b.K_pad     = (int32_t) rup(K, kstep);
         b.dst_off   = bbytes;
         b.exp_off   = (int32_t) bexp;
-        bbytes += (int64_t) b.rows_pad * b.K_pad * S;
+        bbytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
         bexp += b.rows_pad;
         ib = bmap.emplace(tk.b_off, (int) L->b_blocks.size()).first;
         L->b_blocks.push_back(b);
@@ -735,7 +783,7 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
       it.b_off     = B.dst_off; // rebased below
       it.a_exp     = A.exp_off;
       it.b_exp     = B.exp_off;
-      it.nkc       = A.K_pad / KC;
+      it.nkc       = A.K_pad / kstep;
       L->tasks[t]  = it;
       I8TaskMeta mt{};
       mt.a_block = A.id;
@@ -779,7 +827,7 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
     for(int64_t mt = 0; mt < (M + MT - 1) / MT; mt++)
       for(int64_t nt = 0; nt < (N + L->NT - 1) / L->NT; nt++) {
         v.push_back({work, I8Item{(int32_t) gi, (int32_t) mt, (int32_t) nt, 0}});
-        L->int8_ops += 2.0 * MT * L->NT * KC * work * (S * (S + 1) / 2);
+        L->int8_ops += 2.0 * MT * L->NT * kstep * work * (S * (S + 1) / 2);
       }
   }
   std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
@@ -814,7 +862,7 @@ int sm_count() {
   return n;
 }
 
-template<int S>
+template<int S, bool BF>
 void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const double* B, uint8_t* slices,
                   int32_t* exps, cudaStream_t st) {
   const int grid_cap = sm_count() * 8;
@@ -823,17 +871,20 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
   auto one = [&](const SplitBlock* blocks, const int2* chunks, size_t nchunks, const double* src) {
     if(nchunks == 0) return;
     const int grid = (int) std::min<int64_t>((int64_t) nchunks, grid_cap);
-    k_split_fused<S><<<grid, 256, 0, st>>>(blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
+    k_split_fused<S, BF><<<grid, 256, 0, st>>>(blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
   };
   one(L.d_ablocks, L.d_achunks, L.a_chunks.size(), A);
   one(L.d_bblocks, L.d_bchunks, L.b_chunks.size(), B);
   const int ng = (int) wl.groups.size();
-  if(ng > 0)
+  if constexpr(BF) { // both bf16 pieces in every task
+    if(!L.tasks.empty()) TB_CUDA(cudaMemsetAsync(L.d_tslices, S, L.tasks.size(), st));
+  }
+  else if(ng > 0)
     k_task_slices<<<(ng + 7) / 8, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
   TB_CUDA(cudaGetLastError());
 }
 
-template<int S, int NT>
+template<int S, int NT, bool BF>
 void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha,
                  const uint8_t* slices, const int32_t* exps, double* C, cudaStream_t st) {
   if(L.items.empty()) return;
@@ -856,27 +907,27 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   int          dev            = 0;
   TB_CUDA(cudaGetDevice(&dev));
   if(dev < 64 && !configured[dev]) {
-    TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     configured[dev] = true;
   }
   const int grid = (int) std::min<int64_t>((int64_t) L.items.size(), sm_count());
-  k_contract_i8<S, NT><<<grid, NTHREADS, smem, st>>>(p);
+  k_contract_i8<S, NT, BF><<<grid, NTHREADS, smem, st>>>(p);
   TB_CUDA(cudaGetLastError());
 }
 
-template<int S>
+template<int S, bool BF = false>
 void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha, const double* A,
            const double* B, double* C, uint8_t* slices, int32_t* exps, cudaStream_t st,
            cudaEvent_t* ev) {
   if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
-  launch_split<S>(L, wl, A, B, slices, exps, st);
+  launch_split<S, BF>(L, wl, A, B, slices, exps, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
   // output tile width: 80 columns by default for S <= 6 (S x NT <= 512 TMEM columns)
   if constexpr(S * 80 <= 512) {
-    if(L.NT == 80) launch_gemm<S, 80>(L, wl, lc, alpha, slices, exps, C, st);
+    if(L.NT == 80) launch_gemm<S, 80, BF>(L, wl, lc, alpha, slices, exps, C, st);
   }
-  if(L.NT == 64) launch_gemm<S, 64>(L, wl, lc, alpha, slices, exps, C, st);
-  if(L.NT == 48) launch_gemm<S, 48>(L, wl, lc, alpha, slices, exps, C, st);
+  if(L.NT == 64) launch_gemm<S, 64, BF>(L, wl, lc, alpha, slices, exps, C, st);
+  if(L.NT == 48) launch_gemm<S, 48, BF>(L, wl, lc, alpha, slices, exps, C, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
 }
 
@@ -895,20 +946,23 @@ std::map<const WorkList*, std::shared_ptr<I8Layout>> g_layouts; // per work list
 
 } // namespace
 
-void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
-                   double* C, cudaStream_t stream) {
+// Split contraction, shared by the split-INT8 mode (bf = false: S balanced INT8 digits)
+// and the BF16x3 mode (bf = true: two bf16 pieces, three products, FP32 accumulators).
+void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B, double* C,
+                    cudaStream_t stream, bool bf) {
   const LabelClasses& lc = plan.lc;
   if(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0) {
     // Hadamard / one-sided reduction labels and outer products run on the FP64 path.
     launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
     return;
   }
-  const int S = plan.nslices > 0 ? std::min(std::max(plan.nslices, 3), 8) : slices_for(plan.err_target);
-  const int NT = plan.tile_n > 0 ? plan.tile_n : nt_for(S);
+  const int S     = bf ? 2 : (plan.nslices > 0 ? std::min(std::max(plan.nslices, 3), 8) : slices_for(plan.err_target));
+  const int NT    = plan.tile_n > 0 ? plan.tile_n : nt_for(S);
+  const int esize = bf ? 2 : 1;
   TB_EXPECTS((NT == 48 || NT == 64 || NT == 80) && S * NT <= 512,
-             "split-INT8 output tile width must be 48, 64 or 80 with slices x width <= 512");
+             "split output tile width must be 48, 64 or 80 with slices x width <= 512");
   auto& L = g_layouts[&wl];
-  if(!L || L->S != S || L->NT != NT) L = build_layout(lc, wl, S, NT);
+  if(!L || L->S != S || L->NT != NT || L->esize != esize) L = build_layout(lc, wl, S, NT, esize);
   Scratch sc;
   sc.stream = stream;
   sc.arena  = plan.arena;
@@ -921,7 +975,8 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
     for(auto& e: evs) TB_CUDA(cudaEventCreate(&e));
     ev = evs;
   }
-  switch(S) {
+  if(bf) run_s<2, true>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev);
+  else switch(S) {
     case 3: run_s<3>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
     case 4: run_s<4>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
     case 5: run_s<5>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
@@ -960,7 +1015,7 @@ void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A
       const DevGroup& g = wl.groups[it.group];
       for(int t = g.task_begin; t < g.task_end; t++) {
         const int st = ts[t];
-        ops += 2.0 * MT * L->NT * KC * L->tasks[t].nkc * (st * (st + 1) / 2);
+        ops += 2.0 * MT * L->NT * (KC / L->esize) * L->tasks[t].nkc * (st * (st + 1) / 2);
         smin = std::min(smin, st);
         smax = std::max(smax, st);
       }
@@ -997,16 +1052,14 @@ void check_int8_errors(const WorkList& wl, cudaStream_t stream) {
   }
 }
 
-void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
-                     double* C, cudaStream_t stream) {
-  (void) plan;
-  (void) wl;
-  (void) alpha;
-  (void) A;
-  (void) B;
-  (void) C;
-  (void) stream;
-  fail(TB_ERR_NOT_IMPLEMENTED, "BF16x3 contraction is not built yet");
+void contract_int8(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B, double* C,
+                   cudaStream_t stream) {
+  contract_split(plan, wl, alpha, A, B, C, stream, false);
+}
+
+void contract_bf16x3(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B, double* C,
+                     cudaStream_t stream) {
+  contract_split(plan, wl, alpha, A, B, C, stream, true);
 }
 
 // ------------------------------------------------------------------------------
@@ -1085,8 +1138,8 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   uint8_t*      sl   = base + slices_off;
   k_noalloc_setup<<<8, 256, 0, st>>>(d, base);
   const int cap = sm_count() * 8;
-  k_split_fused<S><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
-  k_split_fused<S><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
+  k_split_fused<S, false><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
+  k_split_fused<S, false><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
   k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
   I8Params p{};
   p.slices  = sl;
@@ -1102,8 +1155,8 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   p.tslices = tsl;
   p.ctr     = reinterpret_cast<int*>(base + kCtlCtr);
   const size_t smem = smem_bytes<S, NT>();
-  TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-  k_contract_i8<S, NT><<<std::min(p.nitems, sm_count()), NTHREADS, smem, st>>>(p);
+  TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+  k_contract_i8<S, NT, false><<<std::min(p.nitems, sm_count()), NTHREADS, smem, st>>>(p);
   TB_CUDA(cudaGetLastError());
 }
 
