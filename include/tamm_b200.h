@@ -271,6 +271,17 @@ int tb_sched_mult(tb_sched s, tb_labeled lhs, double alpha, tb_labeled a, tb_lab
  * MultOp uses (multop.hpp:645-893).  Needs no GPU and no allocation. */
 int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, int64_t* ntasks,
                  double* flops);
+/* Owner-computes share for one of nranks processes (TAMM's rule, multop.hpp:880-891,
+ * with a FLOP-balanced assignment): Mult ops of this scheduler compute only the
+ * output blocks this rank owns; Set and Add ops still cover the whole local tensor.
+ * Every rank derives the same assignment from the same operands, without exchange;
+ * assembling the result (e.g. an all-reduce of a zero-initialised output) is the
+ * caller's. */
+int tb_sched_set_owner(tb_sched s, int rank, int nranks);
+/* Output blocks of lhs += a * b owned by `rank` of nranks: their number, FP64 FLOPs
+ * and packed offsets in lhs (up to cap).  Host-only, like tb_mult_info. */
+int tb_mult_owned(tb_labeled lhs, tb_labeled a, tb_labeled b, int rank, int nranks, int64_t* ngroups,
+                  double* flops, int64_t* c_offsets, int64_t cap);
 /* Scheduler::execute(ExecutionHW, profile).  hw: 0 DEFAULT, 1 CPU, 2 GPU — every op
  * runs on the GPU (there is no host execution path); profile records per-op device
  * times readable with tb_sched_profile. */

@@ -12,7 +12,8 @@ std::shared_ptr<TIS> make_tis(const std::shared_ptr<IndexSpace>& is, int64_t til
                               const int64_t* tiles, int64_t ntiles);
 std::shared_ptr<TIS> tis_named(const TIS& parent, const std::string& name);
 std::shared_ptr<TIS> tis_subrange(const TIS& parent, int64_t first, int64_t last);
-std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload);
+std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload, int rank = 0,
+                                        int nranks = 1);
 
 // Mode dispatch of one grouped contraction.
 void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
@@ -723,6 +724,33 @@ int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, i
   if(ngroups) *ngroups = (int64_t) wl->groups.size();
   if(ntasks) *ntasks = (int64_t) wl->tasks.size();
   if(flops) *flops = wl->flops;
+  TB_API_END
+}
+
+int tb_sched_set_owner(tb_sched s, int rank, int nranks) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  TB_EXPECTS(nranks >= 1 && rank >= 0 && rank < nranks, "rank must lie in [0, nranks)");
+  s->p->rank   = rank;
+  s->p->nranks = nranks;
+  TB_API_END
+}
+
+int tb_mult_owned(tb_labeled lhs, tb_labeled a, tb_labeled b, int rank, int nranks, int64_t* ngroups,
+                  double* flops, int64_t* c_offsets, int64_t cap) {
+  TB_API_BEGIN
+  TB_EXPECTS(nranks >= 1 && rank >= 0 && rank < nranks, "rank must lie in [0, nranks)");
+  Op op;
+  op.kind = Op::Mult;
+  op.lhs  = to_labeled(lhs);
+  op.a    = to_labeled(a);
+  op.b    = to_labeled(b);
+  auto lc = classify(op.lhs.labels.data(), (int) op.lhs.labels.size(), op.a.labels.data(),
+                     (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
+  auto wl = mult_worklist(op, lc, false, rank, nranks);
+  if(ngroups) *ngroups = (int64_t) wl->groups.size();
+  if(flops) *flops = wl->flops;
+  for(size_t g = 0; c_offsets && g < wl->groups.size() && (int64_t) g < cap; g++) c_offsets[g] = wl->groups[g].c_off;
   TB_API_END
 }
 

@@ -119,6 +119,8 @@ struct Plan {
 };
 
 void forget_int8_layout(const WorkList* wl);
+// FP64 FLOPs of one task of a group (2 * |C block| * K, times the one-sided steps).
+double task_flops(const LabelClasses& lc, const DevGroup& g, const DevTask& t);
 // Largest split-INT8 slice count the error target needs (3..8).
 int int8_slices_for(double err_target);
 

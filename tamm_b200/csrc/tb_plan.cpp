@@ -146,7 +146,7 @@ static void validate_task(const LabelClasses& lc, const DevGroup& g, const DevTa
   TB_EXPECTS(t.a_off >= 0 && t.b_off >= 0, "negative block offset");
 }
 
-static double task_flops(const LabelClasses& lc, const DevGroup& g, const DevTask& t) {
+double task_flops(const LabelClasses& lc, const DevGroup& g, const DevTask& t) {
   double csz = 1, k = 1;
   for(int i = 0; i < lc.nc; i++) csz *= g.cdims[i];
   for(int j = 0; j < lc.nk; j++) k *= t.adims[lc.k_a[j]];

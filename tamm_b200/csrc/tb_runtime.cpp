@@ -354,7 +354,33 @@ std::string signature(const Op& op) {
 
 // MultOp::execute_bufacc enumeration (multop.hpp:576-893): owned admitted output
 // blocks x admitted reduction tiles, as device work-list groups and tasks.
-std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& lc, bool upload) {
+// Owner of each output block for nranks processes: blocks in decreasing FP64 work
+// (ties by position), each to the rank with the least work so far (ties to the lower
+// rank).  Every rank computes the same assignment from the same work list, so no
+// exchange is needed to agree on it (the role of TAMM's owner-computes rule,
+// multop.hpp:880-891, with a FLOP-balanced distribution instead of GA's).
+std::vector<int> group_owners(const LabelClasses& lc, const WorkList& wl, int nranks) {
+  std::vector<double> work(wl.groups.size(), 0.0);
+  for(size_t g = 0; g < wl.groups.size(); g++)
+    for(int t = wl.groups[g].task_begin; t < wl.groups[g].task_end; t++)
+      work[g] += task_flops(lc, wl.groups[g], wl.tasks[t]);
+  std::vector<size_t> order(wl.groups.size());
+  for(size_t g = 0; g < order.size(); g++) order[g] = g;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work[x] > work[y]; });
+  std::vector<double> load(nranks, 0.0);
+  std::vector<int>    owner(wl.groups.size(), 0);
+  for(size_t g: order) {
+    int r = 0;
+    for(int q = 1; q < nranks; q++)
+      if(load[q] < load[r]) r = q;
+    owner[g] = r;
+    load[r] += work[g];
+  }
+  return owner;
+}
+
+std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& lc, bool upload, int rank,
+                                              int nranks) {
   const Labeled &c = op.lhs, &a = op.a, &b = op.b;
   auto cm = tile_maps(c), am = tile_maps(a), bm = tile_maps(b);
   // reduction labels: unique rhs labels (A then B) not in the lhs, sorted (multop.hpp:593-601)
@@ -428,14 +454,27 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
     g.task_end = (int32_t) wl->tasks.size();
     wl->groups.push_back(g);
   } while(!cid.empty() && next_tuple(itval, c_nt));
+  if(nranks > 1) { // keep the output blocks this rank owns
+    const std::vector<int> owner = group_owners(lc, *wl, nranks);
+    auto                   mine  = std::make_shared<WorkList>();
+    for(size_t gi = 0; gi < wl->groups.size(); gi++) {
+      if(owner[gi] != rank) continue;
+      DevGroup g   = wl->groups[gi];
+      g.task_begin = (int32_t) mine->tasks.size();
+      for(int t = wl->groups[gi].task_begin; t < wl->groups[gi].task_end; t++) mine->tasks.push_back(wl->tasks[t]);
+      g.task_end = (int32_t) mine->tasks.size();
+      mine->groups.push_back(g);
+    }
+    wl = mine;
+  }
   finalize_worklist(lc, *wl, upload);
   return wl;
 }
 
 } // namespace
 
-std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload) {
-  return build_mult_worklist(op, lc, upload);
+std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload, int rank, int nranks) {
+  return build_mult_worklist(op, lc, upload, rank, nranks);
 }
 
 void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
@@ -582,7 +621,7 @@ void Sched::run(Op& op) {
   op.a.t->require_allocated();
   op.b.t->require_allocated();
   if(!op.wl) {
-    const std::string sig = signature(op);
+    const std::string sig = signature(op) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks);
     auto              pit = plan_cache.find(sig);
     if(pit == plan_cache.end()) {
       auto plan        = std::make_shared<Plan>();
@@ -592,7 +631,7 @@ void Sched::run(Op& op) {
       plan->err_target = ctx->err_target;
       plan->nslices    = ctx->nslices;
       plan_cache[sig]  = plan;
-      wl_cache[sig]    = build_mult_worklist(op, plan->lc, true);
+      wl_cache[sig]    = build_mult_worklist(op, plan->lc, true, rank, nranks);
       pit              = plan_cache.find(sig);
     }
     op.plan = pit->second;

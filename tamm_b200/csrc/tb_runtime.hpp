@@ -168,6 +168,7 @@ struct Sched {
   static constexpr int                              kSlots = 64;
   double*                                           d_scalars = nullptr; // kSlots + 1024 partials
   bool                                              autotune  = false;
+  int                                               rank = 0, nranks = 1; // owner-computes share of Mult ops
   std::map<std::string, TuneChoice>                 tune_cache;
   CapturePool*                                      pinned = nullptr; // set while capturing a graph
   void                                              execute(bool profile);

@@ -405,6 +405,20 @@ def mult_info(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor):
     return ng.value, nt.value, fl.value
 
 
+def mult_owned(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor, rank: int, nranks: int):
+    """Output blocks of lhs += a * b that `rank` of `nranks` computes under the
+    FLOP-balanced owner rule: (packed offsets in lhs, FP64 FLOPs).  Host-only."""
+    ids: dict = {}
+    keep: list = []
+    l, x, y = (_to_c_labeled(t, ids, keep) for t in (lhs, a, b))
+    ng, fl = C.c_int64(), C.c_double()
+    call("tb_mult_owned", l, x, y, int(rank), int(nranks), C.byref(ng), C.byref(fl), None, 0)
+    offs = np.zeros(max(ng.value, 1), dtype=np.int64)
+    call("tb_mult_owned", l, x, y, int(rank), int(nranks), C.byref(ng), C.byref(fl),
+         offs.ctypes.data_as(A.i64p), ng.value)
+    return offs[:ng.value].copy(), fl.value
+
+
 class Scheduler:
     """Scheduler{ec}: sch(op)...execute(hw, profile)."""
 
@@ -487,6 +501,11 @@ class Scheduler:
         self._keep += [e, sg]
         call("tb_sched_denom", self.h, self._labeled(t, ids), float(alpha), self._labeled(r, ids),
              e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
+        return self
+
+    def set_owner(self, rank: int, nranks: int):
+        """Mult ops compute only the output blocks `rank` owns (of `nranks`)."""
+        call("tb_sched_set_owner", self.h, int(rank), int(nranks))
         return self
 
     def autotune(self, enable: bool = True):
