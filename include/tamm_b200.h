@@ -306,6 +306,12 @@ int tb_sched_scalars(tb_sched s, double* host, int n);
  * index space shared by t's modes, neps entries; r with t's labels and layout). */
 int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const double* eps, int64_t neps,
                    const double* signs);
+/* slot += alpha * sum w^2 / D over w's stored elements, D as in tb_sched_denom: the
+ * energy reduction of a perturbative-triples-style term, without storing w / D
+ * (no counterpart in TAMM's ops).  tb_sched_set_scalar queues slot = value. */
+int tb_sched_denom_energy(tb_sched s, int slot, double alpha, tb_labeled w, const double* eps, int64_t neps,
+                          const double* signs);
+int tb_sched_set_scalar(tb_sched s, int slot, double value);
 /* Autotuner (no counterpart in TAMM): with enable != 0, the first execution of each
  * contraction under a split-INT8 request times the candidate kernels (FP64; split-
  * INT8 with output tiles 80 / 64 / 48 wide where the slice count allows) on a saved

@@ -355,6 +355,68 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
   return h;
 }
 
+// part[block] = sum over the block's elements of w^2 / D (D as in k_denom), one CTA
+// per block; k_denom_energy_final adds scale * sum(part) to *out.  Deterministic.
+__global__ void __launch_bounds__(kThreads) k_denom_energy(const double* __restrict__ w,
+                                                           const DenomBlock* __restrict__ blocks, int nmodes,
+                                                           const double* __restrict__ eps, DenomSigns sg,
+                                                           double* __restrict__ part) {
+  const DenomBlock b = blocks[blockIdx.x];
+  int64_t          n = 1;
+  for(int m = 0; m < nmodes; m++) n *= b.dims[m];
+  double s = 0.0;
+  for(int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+    int64_t x = e;
+    double  d = 0.0;
+    for(int m = nmodes - 1; m >= 0; m--) {
+      const int64_t q = x / b.dims[m];
+      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
+      x = q;
+    }
+    const double v = w[b.off + e];
+    s += v * v / d;
+  }
+#pragma unroll
+  for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double ws[kThreads / 32];
+  if((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    double t = 0.0;
+    for(int i = 0; i < kThreads / 32; i++) t += ws[i];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_denom_energy_final(const double* __restrict__ part, int np, double scale, double* __restrict__ out) {
+  __shared__ double ws[32];
+  double            s = 0.0;
+  for(int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+#pragma unroll
+  for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    double t = 0.0;
+    for(int w = 0; w < (int) (blockDim.x / 32); w++) t += ws[w];
+    *out += scale * t;
+  }
+}
+
+__global__ void k_set_scalar(double* out, double v) { *out = v; }
+
+void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
+                         const double* eps, DenomSigns signs, double* part, double* out, cudaStream_t stream) {
+  if(nblocks > 0) k_denom_energy<<<nblocks, kThreads, 0, stream>>>(w, blocks, nmodes, eps, signs, part);
+  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, nblocks, scale, out);
+  TB_CUDA(cudaGetLastError());
+}
+
+void launch_set_scalar(double* out, double v, cudaStream_t stream) {
+  k_set_scalar<<<1, 1, 0, stream>>>(out, v);
+  TB_CUDA(cudaGetLastError());
+}
+
 void launch_dot_to(const double* x, const double* y, int64_t n, double scale, int root, double* out, double* part,
                    cudaStream_t stream) {
   if(n <= 0) {

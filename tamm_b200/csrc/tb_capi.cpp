@@ -848,6 +848,39 @@ int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const d
   TB_API_END
 }
 
+int tb_sched_denom_energy(tb_sched s, int slot, double alpha, tb_labeled w, const double* eps, int64_t neps,
+                          const double* signs) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && eps != nullptr && signs != nullptr && neps >= 0);
+  TB_EXPECTS(slot >= 0 && slot < Sched::kSlots, "scalar slot out of range (0..63)");
+  Op op;
+  op.kind  = Op::DenomEnergy;
+  op.lhs   = to_labeled(w);
+  op.alpha = alpha;
+  op.slot  = slot;
+  const Tensor& T = *op.lhs.t;
+  for(int m = 1; m < T.nmodes; m++)
+    TB_EXPECTS(T.tis[m]->root->is == T.tis[0]->root->is, "denominator energy: all modes over one root index space");
+  auto d = std::make_shared<DenomSpec>();
+  d->eps.assign(eps, eps + neps);
+  for(int m = 0; m < T.nmodes; m++) d->signs[m] = signs[m];
+  op.denom = d;
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
+int tb_sched_set_scalar(tb_sched s, int slot, double value) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  TB_EXPECTS(slot >= 0 && slot < Sched::kSlots, "scalar slot out of range (0..63)");
+  Op op;
+  op.kind  = Op::SetScalar;
+  op.slot  = slot;
+  op.value = value;
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
 int tb_sched_autotune(tb_sched s, int enable) {
   TB_API_BEGIN
   REQUIRE_ARG(s != nullptr);

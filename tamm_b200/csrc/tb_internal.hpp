@@ -163,6 +163,10 @@ struct DenomSigns {
 };
 void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
                   const double* eps, DenomSigns signs, cudaStream_t stream);
+// *out += scale * sum w^2 / D over the blocks (part: nblocks doubles of scratch).
+void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
+                         const double* eps, DenomSigns signs, double* part, double* out, cudaStream_t stream);
+void launch_set_scalar(double* out, double v, cudaStream_t stream);
 // Reads and clears the device error word of the split-INT8 launches of a work list;
 // throws TB_ERR_TIMEOUT if a device-side wait gave up.
 void check_int8_errors(const WorkList& wl, cudaStream_t stream);

@@ -582,38 +582,24 @@ void Sched::run(Op& op) {
     op.lhs.t->require_allocated();
     op.a.t->require_allocated();
     DenomSpec& d = *op.denom;
-    if(!d.d_blocks) { // block table of the update: packed offsets, dims, first orbital index
-      const Tensor&           T = *op.lhs.t;
-      std::vector<DenomBlock> blocks;
-      std::vector<int64_t>    id(T.nmodes);
-      for(size_t bi = 0; bi < T.keys.size(); bi++) {
-        int64_t key = T.keys[bi]; // block id in each mode's own tile numbering
-        for(int m = T.nmodes - 1; m >= 0; m--) {
-          const int64_t n = T.tis[m]->ntiles();
-          id[m]           = key % n;
-          key /= n;
-        }
-        DenomBlock b{};
-        b.off = T.offsets[bi];
-        for(int m = 0; m < T.nmodes; m++) {
-          const int64_t r = T.tis[m]->tiles[id[m]]; // root tile
-          b.dims[m]       = T.tis[m]->root->offsets[r + 1] - T.tis[m]->root->offsets[r];
-          b.first[m]      = T.tis[m]->root->offsets[r];
-          TB_EXPECTS(b.first[m] + b.dims[m] <= (int64_t) d.eps.size(), "orbital energies shorter than the index space");
-        }
-        blocks.push_back(b);
-      }
-      d.ctx     = ctx;
-      d.nblocks = (int) blocks.size();
-      TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d.d_eps), sizeof(double) * std::max<size_t>(d.eps.size(), 1)));
-      TB_CUDA(cudaMemcpy(d.d_eps, d.eps.data(), sizeof(double) * d.eps.size(), cudaMemcpyHostToDevice));
-      TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d.d_blocks), sizeof(DenomBlock) * std::max<size_t>(blocks.size(), 1)));
-      if(!blocks.empty())
-        TB_CUDA(cudaMemcpy(d.d_blocks, blocks.data(), sizeof(DenomBlock) * blocks.size(), cudaMemcpyHostToDevice));
-    }
+    if(!d.d_blocks) d.build(*op.lhs.t, ctx);
     DenomSigns sg{};
     for(int m = 0; m < kMaxModes; m++) sg.s[m] = d.signs[m];
     launch_denom(op.lhs.t->data, op.a.t->data, op.alpha, d.d_blocks, d.nblocks, op.lhs.t->nmodes, d.d_eps, sg, st);
+    return;
+  }
+  if(op.kind == Op::DenomEnergy) {
+    op.lhs.t->require_allocated();
+    DenomSpec& d = *op.denom;
+    if(!d.d_blocks) d.build(*op.lhs.t, ctx);
+    DenomSigns sg{};
+    for(int m = 0; m < kMaxModes; m++) sg.s[m] = d.signs[m];
+    launch_denom_energy(op.lhs.t->data, op.alpha, d.d_blocks, d.nblocks, op.lhs.t->nmodes, d.d_eps, sg, d.d_part,
+                        scalars() + op.slot, st);
+    return;
+  }
+  if(op.kind == Op::SetScalar) {
+    launch_set_scalar(scalars() + op.slot, op.value, st);
     return;
   }
   // MultOp
@@ -744,10 +730,43 @@ Sched::~Sched() {
   }
 }
 
+// Block table of a denominator op over t's admitted blocks: packed offset, dims and
+// the root orbital index of each mode's first element (uploaded once).
+void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c) {
+  std::vector<DenomBlock> blocks;
+  std::vector<int64_t>    id(T.nmodes);
+  for(size_t bi = 0; bi < T.keys.size(); bi++) {
+    int64_t key = T.keys[bi]; // block id in each mode's own tile numbering
+    for(int m = T.nmodes - 1; m >= 0; m--) {
+      const int64_t n = T.tis[m]->ntiles();
+      id[m]           = key % n;
+      key /= n;
+    }
+    DenomBlock b{};
+    b.off = T.offsets[bi];
+    for(int m = 0; m < T.nmodes; m++) {
+      const int64_t r = T.tis[m]->tiles[id[m]]; // root tile
+      b.dims[m]       = T.tis[m]->root->offsets[r + 1] - T.tis[m]->root->offsets[r];
+      b.first[m]      = T.tis[m]->root->offsets[r];
+      TB_EXPECTS(b.first[m] + b.dims[m] <= (int64_t) eps.size(), "orbital energies shorter than the index space");
+    }
+    blocks.push_back(b);
+  }
+  ctx     = c;
+  nblocks = (int) blocks.size();
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_eps), sizeof(double) * std::max<size_t>(eps.size(), 1)));
+  TB_CUDA(cudaMemcpy(d_eps, eps.data(), sizeof(double) * eps.size(), cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_blocks), sizeof(DenomBlock) * std::max<size_t>(blocks.size(), 1)));
+  if(!blocks.empty())
+    TB_CUDA(cudaMemcpy(d_blocks, blocks.data(), sizeof(DenomBlock) * blocks.size(), cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_part), sizeof(double) * std::max<size_t>(blocks.size(), 1)));
+}
+
 DenomSpec::~DenomSpec() {
   if(ctx) cudaSetDevice(ctx->device);
   if(d_eps) cudaFree(d_eps);
   if(d_blocks) cudaFree(d_blocks);
+  if(d_part) cudaFree(d_part);
 }
 
 Graph::~Graph() {

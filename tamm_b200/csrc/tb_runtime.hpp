@@ -116,7 +116,8 @@ Labeled labeled_from_c(const tb_labeled& x);
 struct Op {
   // Dot: scalar slot `slot` = alpha * sum a * b (root: alpha * sqrt(sum a * a)), kept on
   // the device; Denom: lhs += alpha * a / D with the orbital-energy denominator D.
-  enum Kind { Set, Add, Mult, Dot, Denom } kind;
+  // DenomEnergy: slot += alpha * sum lhs^2 / D; SetScalar: slot = value.
+  enum Kind { Set, Add, Mult, Dot, Denom, DenomEnergy, SetScalar } kind;
   Labeled lhs, a, b;
   double  alpha = 1.0, value = 0.0;
   int     is_assign = 0;
@@ -143,7 +144,9 @@ struct DenomSpec {
   double                  signs[kMaxModes] = {0};
   double*                 d_eps    = nullptr;
   DenomBlock*             d_blocks = nullptr;
+  double*                 d_part   = nullptr; // per-block partial sums (energy reduction)
   int                     nblocks  = 0;
+  void                    build(const Tensor& t, const std::shared_ptr<Ctx>& ctx);
   std::shared_ptr<Ctx>    ctx;
   ~DenomSpec();
 };

@@ -508,6 +508,19 @@ class Scheduler:
         call("tb_sched_set_owner", self.h, int(rank), int(nranks))
         return self
 
+    def denom_energy(self, slot: int, alpha: float, w: LabeledTensor, eps, signs):
+        """Queue slot += alpha * sum w^2 / D, D = sum_m signs[m] * eps[orbital index of mode m]."""
+        e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+        sg = np.ascontiguousarray(np.asarray(list(signs) + [0.0] * (8 - len(signs)), dtype=np.float64))
+        self._keep += [e, sg]
+        call("tb_sched_denom_energy", self.h, int(slot), float(alpha), self._labeled(w, {}),
+             e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
+        return self
+
+    def set_scalar(self, slot: int, value: float = 0.0):
+        call("tb_sched_set_scalar", self.h, int(slot), float(value))
+        return self
+
     def autotune(self, enable: bool = True):
         call("tb_sched_autotune", self.h, int(bool(enable)))
         return self

@@ -1,0 +1,193 @@
+"""Triples-style 6-index contraction streamed over occupied pairs, reduced into an
+FP64 energy without storing t3:
+
+    W(a,b,c,i,j,k) = sum_d t2(a,d,i,j) v(b,c,d,k) - sum_l t2(a,b,i,l) v(l,c,j,k)
+    E = sum W^2 / (e_i + e_j + e_k - e_a - e_b - e_c)
+
+on the spin-blocked MO space of the ladder (v from Cholesky vectors, t2 from the
+orbital-energy denominators).  TAMM has no (T) code of its own (it lives in the
+applications built on it); the contractions are TAMM MultOps and the reduction is
+the denominator-energy op of this library.
+
+Streaming: a t3 block of one tile tuple holds tile^6 values (4e9 at tile 40), so W
+is formed one occupied pair (i, j) at a time: W(a,b,c,k) for a fixed (i, j) is one
+contraction over d, minus one over l, into a shared buffer, followed by
+slot += sum W^2 / D.  The streamed labels i, j need single-index tiles while the
+summed l keeps the uniform occupied tiles, so t2 is held in two tilings
+(t2(a,d,i,j) with i, j single; t2(a,b,i,l) with l tiled) and v(l,c,j,k) with j
+single; both t2 copies come from one dense array, so they hold the same values.
+v(b,c,d,k) is stored as (b,c,k,d) so that the summed d is the contiguous mode.
+
+    python -m tamm_b200.triples [--oa 25 --va 250 --tile 40 --seed 4 --pairs 8]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import workloads as W
+from .tamm import (ExecutionContext, ExecutionHW, IndexSpace, Precision, Scheduler, Tensor, TiledIndexSpace,
+                   mult_info)
+
+SLOT_E = 2
+
+
+@dataclass
+class TriplesProblem:
+    ec: ExecutionContext
+    V: TiledIndexSpace     # virtual, uniform tiles
+    Ob: TiledIndexSpace    # occupied, uniform tiles (summed l, streamed-in k)
+    O1: TiledIndexSpace    # occupied, one index per tile (streamed i, j)
+    eps: np.ndarray
+    T: dict
+    buffer: object
+    most: int
+
+
+def _dense_t2(oa, va, eps, seed):
+    """t2(a,b,i,j) ~ N(0, 0.1^2) / (e_a + e_b - e_i - e_j) on the full (virt, virt, occ, occ)
+    ranges, zero outside the spin-conserving blocks."""
+    no, nv = 2 * oa, 2 * va
+    rng = np.random.default_rng(seed + 7)
+    eo, ev = eps[:no], eps[no:]
+    so = np.array([0] * oa + [1] * oa)
+    sv = np.array([0] * va + [1] * va)
+    t = rng.normal(0.0, 0.1, size=(nv, nv, no, no))
+    t /= ev[:, None, None, None] + ev[None, :, None, None] - eo[None, None, :, None] - eo[None, None, None, :]
+    ok = (sv[:, None, None, None] + sv[None, :, None, None]) == (so[None, None, :, None] + so[None, None, None, :])
+    return t * ok
+
+
+def build(oa: int, va: int, tile: int = 40, seed: int = 4, nchol=None, ec: ExecutionContext | None = None):
+    import torch
+    is_ = W.mo_index_space(oa, va)
+    MOb = TiledIndexSpace(is_, tile)
+    MO1 = TiledIndexSpace(is_, 1)
+    V, Ob, O1 = MOb("virt"), MOb("occ"), MO1("occ")
+    ec = ec or ExecutionContext(0, 0)
+    e_occ, e_virt = W.orbital_energies(oa, va, seed)
+    eps = np.concatenate([e_occ, e_occ, e_virt, e_virt])
+    no = 2 * oa
+    Q = nchol if nchol is not None else 5 * (2 * oa + 2 * va)
+    CI = TiledIndexSpace(IndexSpace(Q), 1000)
+    T = {}
+
+    def new(name, spaces, **kw):
+        T[name] = Tensor(spaces, **kw).allocate(ec)
+        return T[name]
+
+    def chol(seed_):
+        rng = np.random.default_rng(seed_)
+
+        def f(bid, dims, rg):
+            ip = np.arange(rg[1][0], rg[1][1])[:, None]
+            iq = np.arange(rg[2][0], rg[2][1])[None, :]
+            return rng.normal(0.0, 1.0, size=dims) / math.sqrt(Q) * np.exp(-np.abs(ip - iq) / 50.0)[None]
+        return f
+
+    for name, (s1, s2), sd in (("L_vv", (V, V), 13), ("L_vo", (V, Ob), 11), ("L_oo", (Ob, O1), 12)):
+        t = new(name, [CI, s1, s2], spin_mask=[2, 0, 1])
+        t.write(W.fill_blocks(t, chol(seed + sd)))
+    dense = _dense_t2(oa, va, eps, seed)
+    for name, sp in (("t2x", [V, V, O1, O1]), ("t2y", [V, V, O1, Ob])):
+        t = new(name, sp, spin=(2, 2))
+        t.write(W.fill_blocks(t, lambda bid, dims, rg: dense[rg[0][0] - no:rg[0][1] - no, rg[1][0] - no:rg[1][1] - no,
+                                                            rg[2][0]:rg[2][1], rg[3][0]:rg[3][1]]))
+    del dense
+    new("vx", [V, V, Ob, V], spin=(2, 2))    # v(b,c,d,k) = sum_Q L(Q,b,d) L(Q,c,k), stored (b,c,k,d)
+    new("vy", [Ob, V, O1, Ob], spin=(2, 2))  # v(l,c,j,k) = sum_Q L(Q,l,j) L(Q,c,k)
+    q = CI.label()
+    b, c, d = V.labels(3)
+    k, l = Ob.labels(2)
+    (j,) = O1.labels(1)
+    sch = Scheduler(ec)
+    sch(T["vx"](b, c, k, d).assign(T["L_vv"](q, b, d) * T["L_vo"](q, c, k)))
+    sch(T["vy"](l, c, j, k).assign(T["L_oo"](q, l, j) * T["L_vo"](q, c, k)))
+    sch.execute(ExecutionHW.GPU)
+    most = 0  # the W layout depends only on the spins of i and j
+    for i in (0, oa):
+        for jj in (0, oa):
+            most = max(most, _w_tensor(V, O1, Ob, i, jj).nelems)
+    buf = torch.empty(most * 8 + 256, dtype=torch.uint8, device=f"cuda:{ec.device}")
+    return TriplesProblem(ec, V, Ob, O1, eps, T, buf, most)
+
+
+def _w_tensor(V, O1, Ob, i, j):
+    return Tensor([V, V, V, O1.sub(i, i + 1), O1.sub(j, j + 1), Ob], spin=(3, 3))
+
+
+def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, j: int):
+    """Queues W(a,b,c,k) for the occupied pair (i, j) and slot SLOT_E += sum W^2 / D.
+    Returns (W tensor, FP64 FLOPs of the two contractions)."""
+    Wt = _w_tensor(P.V, P.O1, P.Ob, i, j)
+    Wt.attach(P.ec, (P.buffer.data_ptr() + 255) // 256 * 256, P.most * 8)
+    a, b, c, d = P.V.labels(4)
+    k, l = P.Ob.labels(2)
+    li, lj = Wt.spaces[3].label(), Wt.spaces[4].label()
+    T = P.T
+    w = Wt(a, b, c, li, lj, k)
+    x = (w, T["vx"](b, c, k, d), T["t2x"](a, d, li, lj))
+    y = (w, T["t2y"](a, b, li, l), T["vy"](l, c, lj, k))
+    sch(w.assign(x[1] * x[2]))
+    sch(w.isub(y[1] * y[2]))
+    sch.denom_energy(SLOT_E, 1.0, Wt(a, b, c, li, lj, k), P.eps, [-1, -1, -1, 1, 1, 1])
+    return Wt, mult_info(*x)[2] + mult_info(*y)[2]
+
+
+def energy(P: TriplesProblem, pairs, sch: Scheduler):
+    """E summed over the given occupied pairs; returns (E, FP64 FLOPs, device ms)."""
+    import torch
+    stream = torch.cuda.ExternalStream(P.ec.stream)
+    sch.set_scalar(SLOT_E, 0.0).execute()
+    flops, ms, keep = 0.0, 0.0, []
+    for i, j in pairs:
+        Wt, fl = queue_pair(P, sch, i, j)
+        keep.append(Wt)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sch.execute(ExecutionHW.GPU)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        flops += fl
+        Wt.deallocate()
+    return float(sch.scalars(SLOT_E + 1)[SLOT_E]), flops, ms
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--oa", type=int, default=25)
+    p.add_argument("--va", type=int, default=250)
+    p.add_argument("--tile", type=int, default=40)
+    p.add_argument("--seed", type=int, default=4)
+    p.add_argument("--pairs", type=int, default=8)
+    p.add_argument("--pool-gib", type=int, default=150)
+    args = p.parse_args(argv)
+    ec = ExecutionContext(0, args.pool_gib << 30)
+    P = build(args.oa, args.va, tile=args.tile, seed=args.seed, ec=ec)
+    no = 2 * args.oa
+    rng = np.random.default_rng(args.seed + 5)
+    pairs = [(int(x) // no, int(x) % no) for x in rng.choice(no * no, size=args.pairs, replace=False)]
+    out = {"workload": f"triples_energy_O{no}_V{2 * args.va}_tile{args.tile}", "sampled_pairs": pairs,
+           "pairs_total": no * no}
+    res = {}
+    for name, mode in (("fp64", Precision.FP64), ("int8", Precision.INT8)):
+        ec.set_precision(mode, 1e-11)
+        sch = Scheduler(ec)
+        energy(P, pairs[:1], sch)  # warm-up: kernels, digit layouts
+        e, fl, ms = energy(P, pairs, sch)
+        res[name] = {"energy_sample": e, "flops_sample": fl, "device_ms": ms, "tflops": fl / ms / 1e9,
+                     "full_run_s_extrapolated": ms / len(pairs) * no * no / 1e3}
+    ec.set_precision(Precision.FP64)
+    out.update(res)
+    out["int8_vs_fp64_energy_rel_err"] = abs(res["int8"]["energy_sample"] - res["fp64"]["energy_sample"]) / abs(
+        res["fp64"]["energy_sample"])
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
