@@ -292,6 +292,11 @@ int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64
 int tb_sched_op_stats(tb_sched s, int64_t index, tb_stats* out);
 /* Drops queued ops without running them. */
 int tb_sched_clear(tb_sched s);
+/* Waits for the stream, then frees the plans and work lists (with their device
+ * arrays) cached for executed ops; queued ops stay.  For long streams of
+ * contractions that never repeat (e.g. a triples energy streamed over occupied
+ * indices), call it between steps.  Graphs keep what they use. */
+int tb_sched_release(tb_sched s);
 
 /* Scalar results kept on the device, in 64 slots per Scheduler (read with
  * tb_sched_scalars after execute or a graph launch): slot = alpha * sum a * b over

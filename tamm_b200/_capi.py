@@ -106,6 +106,7 @@ PROTOS = {
     "tb_sched_execute": [h, C.c_int, C.c_int],
     "tb_sched_profile": [h, i64p, dp, dp, C.c_int64],
     "tb_sched_clear": [h],
+    "tb_sched_release": [h],
     "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
     "tb_tensor_attach": [h, h, vp, C.c_int64],
     "tb_sched_set_owner": [h, C.c_int, C.c_int],

@@ -356,32 +356,58 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
 }
 
 // part[block] = sum over the block's elements of w^2 / D (D as in k_denom), one CTA
-// per block; k_denom_energy_final adds scale * sum(part) to *out.  Deterministic.
+// per block, in chunks of 256 rows (a row: all modes but the last).  Each thread forms
+// the row part of D for one row of the chunk into shared memory (the last mode's
+// part is tabulated once per block), then the CTA streams the chunk's elements with
+// coalesced loads.  Deterministic.
+constexpr int kDenCols = 1024; // last-mode extents tabulated in shared memory
+
 __global__ void __launch_bounds__(kThreads) k_denom_energy(const double* __restrict__ w,
                                                            const DenomBlock* __restrict__ blocks, int nmodes,
                                                            const double* __restrict__ eps, DenomSigns sg,
                                                            double* __restrict__ part) {
-  const DenomBlock b = blocks[blockIdx.x];
-  int64_t          n = 1;
-  for(int m = 0; m < nmodes; m++) n *= b.dims[m];
+  __shared__ double drow[kThreads];
+  __shared__ double dcol[kDenCols];
+  const DenomBlock  b    = blocks[blockIdx.x];
+  const int         last = nmodes - 1;
+  const int64_t     ncol = b.dims[last];
+  int64_t           nrow = 1;
+  for(int m = 0; m < last; m++) nrow *= b.dims[m];
+  const int     tid  = threadIdx.x;
+  const bool    tab  = ncol <= kDenCols;
+  const double* el   = eps + b.first[last];
+  if(tab)
+    for(int64_t c = tid; c < ncol; c += kThreads) dcol[c] = sg.s[last] * __ldg(el + c);
   double s = 0.0;
-  for(int64_t e = threadIdx.x; e < n; e += blockDim.x) {
-    int64_t x = e;
-    double  d = 0.0;
-    for(int m = nmodes - 1; m >= 0; m--) {
-      const int64_t q = x / b.dims[m];
-      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
-      x = q;
+  for(int64_t r0 = 0; r0 < nrow; r0 += kThreads) {
+    __syncthreads(); // the previous chunk's rows are no longer read
+    if(r0 + tid < nrow) {
+      int64_t x = r0 + tid;
+      double  d = 0.0;
+      for(int m = last - 1; m >= 0; m--) {
+        const int64_t q = x / b.dims[m];
+        d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
+        x = q;
+      }
+      drow[tid] = d;
     }
-    const double v = w[b.off + e];
-    s += v * v / d;
+    __syncthreads();
+    const int64_t rows = nrow - r0 < kThreads ? nrow - r0 : kThreads;
+    const int32_t nel  = (int32_t) (rows * ncol), nc = (int32_t) ncol;
+    const double* base = w + b.off + r0 * ncol;
+    for(int32_t e = tid; e < nel; e += kThreads) {
+      const int32_t rr = e / nc, cc = e - rr * nc;
+      const double  v  = base[e];
+      s += v * v / (drow[rr] + (tab ? dcol[cc] : sg.s[last] * __ldg(el + cc)));
+    }
   }
 #pragma unroll
   for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   __shared__ double ws[kThreads / 32];
-  if((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
   __syncthreads();
-  if(threadIdx.x == 0) {
+  if((tid & 31) == 0) ws[tid >> 5] = s;
+  __syncthreads();
+  if(tid == 0) {
     double t = 0.0;
     for(int i = 0; i < kThreads / 32; i++) t += ws[i];
     part[blockIdx.x] = t;

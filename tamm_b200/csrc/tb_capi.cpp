@@ -915,11 +915,11 @@ int tb_sched_tune_info(tb_sched s, int64_t index, int* mode, int* tile_n, int* n
 int tb_sched_graph_create(tb_sched s, tb_graph* out) {
   TB_API_BEGIN
   REQUIRE_ARG(s != nullptr && out != nullptr);
-  Sched&       S     = *s->p;
-  const size_t first = S.start;
-  TB_EXPECTS(first < S.ops.size(), "no queued ops to capture");
+  Sched& S = *s->p;
+  TB_EXPECTS(S.start < S.ops.size(), "no queued ops to capture");
   S.execute(false); // warm-up: plans, work lists, split layouts, autotuner choices
   TB_CUDA(cudaStreamSynchronize(S.ctx->stream));
+  const size_t first = S.last_first; // the warm-up ran ops [last_first, end)
   auto g = std::make_unique<Graph>();
   g->ctx        = S.ctx;
   g->pool.arena = S.ctx->arena.get();
@@ -969,6 +969,18 @@ int tb_graph_sync(tb_graph g) {
 int tb_graph_destroy(tb_graph g) {
   delete g;
   return TB_OK;
+}
+
+int tb_sched_release(tb_sched s) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  TB_CUDA(cudaSetDevice(s->p->ctx->device));
+  TB_CUDA(cudaStreamSynchronize(s->p->ctx->stream));
+  s->p->ops.erase(s->p->ops.begin(), s->p->ops.begin() + (long) s->p->start);
+  s->p->start = s->p->last_first = 0;
+  s->p->plan_cache.clear();
+  s->p->wl_cache.clear();
+  TB_API_END
 }
 
 int tb_sched_clear(tb_sched s) {

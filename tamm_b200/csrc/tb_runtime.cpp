@@ -780,7 +780,11 @@ Graph::~Graph() {
 
 void Sched::execute(bool profile) {
   TB_CUDA(cudaSetDevice(ctx->device));
-  last_first = start;
+  // keep only the ops about to run (the history of earlier executes is not needed:
+  // plans and work lists live in the caches)
+  ops.erase(ops.begin(), ops.begin() + (long) start);
+  start      = 0;
+  last_first = 0;
   prof_ms.clear();
   prof_flops.clear();
   prof_stats.clear();

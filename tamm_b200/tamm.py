@@ -503,6 +503,11 @@ class Scheduler:
              e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
         return self
 
+    def release(self):
+        """Free the cached plans and work lists of executed ops (see tb_sched_release)."""
+        call("tb_sched_release", self.h)
+        return self
+
     def set_owner(self, rank: int, nranks: int):
         """Mult ops compute only the output blocks `rank` owns (of `nranks`)."""
         call("tb_sched_set_owner", self.h, int(rank), int(nranks))

@@ -10,15 +10,18 @@ applications built on it); the contractions are TAMM MultOps and the reduction i
 the denominator-energy op of this library.
 
 Streaming: a t3 block of one tile tuple holds tile^6 values (4e9 at tile 40), so W
-is formed one occupied pair (i, j) at a time: W(a,b,c,k) for a fixed (i, j) is one
-contraction over d, minus one over l, into a shared buffer, followed by
-slot += sum W^2 / D.  The streamed labels i, j need single-index tiles while the
-summed l keeps the uniform occupied tiles, so t2 is held in two tilings
-(t2(a,d,i,j) with i, j single; t2(a,b,i,l) with l tiled) and v(l,c,j,k) with j
-single; both t2 copies come from one dense array, so they hold the same values.
-v(b,c,d,k) is stored as (b,c,k,d) so that the summed d is the contiguous mode.
+is formed one step at a time, a step being one occupied index i and one block of
+`jtile` occupied indices j: W(a,b,c,k) for that (i, j-block) is one contraction
+over d, minus one over l, into a shared buffer, followed by slot += sum W^2 / D.
+The streamed labels need finer occupied tiles (i single, j in blocks of jtile)
+while the summed l keeps the uniform tiles, so t2 is held in two tilings
+(t2(a,d,i,j) with i single and j blocked; t2(a,b,i,l) with l uniform) and v(l,c,j,k)
+with j blocked; both t2 copies come from one dense array, so they hold the same
+values.  v(b,c,d,k) is stored as (b,c,k,d) so that the summed d is contiguous, and
+the summed d has its own tiling (`dtile`, default one tile per spin block): a task
+then contracts over the whole spin block instead of one 40-wide tile.
 
-    python -m tamm_b200.triples [--oa 25 --va 250 --tile 40 --seed 4 --pairs 8]
+    python -m tamm_b200.triples [--oa 25 --va 250 --tile 40 --jtile 2 --dtile 250 --seed 4 --steps 8]
 """
 from __future__ import annotations
 
@@ -41,7 +44,9 @@ class TriplesProblem:
     ec: ExecutionContext
     V: TiledIndexSpace     # virtual, uniform tiles
     Ob: TiledIndexSpace    # occupied, uniform tiles (summed l, streamed-in k)
-    O1: TiledIndexSpace    # occupied, one index per tile (streamed i, j)
+    O1: TiledIndexSpace    # occupied, one index per tile (streamed i)
+    Oj: TiledIndexSpace    # occupied, blocks of jtile indices (streamed j)
+    Vd: TiledIndexSpace    # virtual, tiling of the summed d
     eps: np.ndarray
     T: dict
     buffer: object
@@ -62,12 +67,15 @@ def _dense_t2(oa, va, eps, seed):
     return t * ok
 
 
-def build(oa: int, va: int, tile: int = 40, seed: int = 4, nchol=None, ec: ExecutionContext | None = None):
+def build(oa: int, va: int, tile: int = 40, jtile: int = 2, dtile: int = 0, seed: int = 4, nchol=None,
+          ec: ExecutionContext | None = None):
     import torch
     is_ = W.mo_index_space(oa, va)
     MOb = TiledIndexSpace(is_, tile)
     MO1 = TiledIndexSpace(is_, 1)
-    V, Ob, O1 = MOb("virt"), MOb("occ"), MO1("occ")
+    MOj = TiledIndexSpace(is_, jtile)
+    MOd = TiledIndexSpace(is_, dtile if dtile > 0 else va)
+    V, Ob, O1, Oj, Vd = MOb("virt"), MOb("occ"), MO1("occ"), MOj("occ"), MOd("virt")
     ec = ec or ExecutionContext(0, 0)
     e_occ, e_virt = W.orbital_energies(oa, va, seed)
     eps = np.concatenate([e_occ, e_occ, e_virt, e_virt])
@@ -89,43 +97,50 @@ def build(oa: int, va: int, tile: int = 40, seed: int = 4, nchol=None, ec: Execu
             return rng.normal(0.0, 1.0, size=dims) / math.sqrt(Q) * np.exp(-np.abs(ip - iq) / 50.0)[None]
         return f
 
-    for name, (s1, s2), sd in (("L_vv", (V, V), 13), ("L_vo", (V, Ob), 11), ("L_oo", (Ob, O1), 12)):
+    for name, (s1, s2), sd in (("L_vv", (V, Vd), 13), ("L_vo", (V, Ob), 11), ("L_oo", (Ob, Oj), 12)):
         t = new(name, [CI, s1, s2], spin_mask=[2, 0, 1])
         t.write(W.fill_blocks(t, chol(seed + sd)))
     dense = _dense_t2(oa, va, eps, seed)
-    for name, sp in (("t2x", [V, V, O1, O1]), ("t2y", [V, V, O1, Ob])):
+    for name, sp in (("t2x", [V, Vd, O1, Oj]), ("t2y", [V, V, O1, Ob])):
         t = new(name, sp, spin=(2, 2))
         t.write(W.fill_blocks(t, lambda bid, dims, rg: dense[rg[0][0] - no:rg[0][1] - no, rg[1][0] - no:rg[1][1] - no,
                                                             rg[2][0]:rg[2][1], rg[3][0]:rg[3][1]]))
     del dense
-    new("vx", [V, V, Ob, V], spin=(2, 2))    # v(b,c,d,k) = sum_Q L(Q,b,d) L(Q,c,k), stored (b,c,k,d)
-    new("vy", [Ob, V, O1, Ob], spin=(2, 2))  # v(l,c,j,k) = sum_Q L(Q,l,j) L(Q,c,k)
+    new("vx", [V, V, Ob, Vd], spin=(2, 2))   # v(b,c,d,k) = sum_Q L(Q,b,d) L(Q,c,k), stored (b,c,k,d)
+    new("vy", [Ob, V, Oj, Ob], spin=(2, 2))  # v(l,c,j,k) = sum_Q L(Q,l,j) L(Q,c,k)
     q = CI.label()
-    b, c, d = V.labels(3)
+    b, c = V.labels(2)
+    (d,) = Vd.labels(1)
     k, l = Ob.labels(2)
-    (j,) = O1.labels(1)
+    (j,) = Oj.labels(1)
     sch = Scheduler(ec)
     sch(T["vx"](b, c, k, d).assign(T["L_vv"](q, b, d) * T["L_vo"](q, c, k)))
     sch(T["vy"](l, c, j, k).assign(T["L_oo"](q, l, j) * T["L_vo"](q, c, k)))
     sch.execute(ExecutionHW.GPU)
-    most = 0  # the W layout depends only on the spins of i and j
+    most = 0  # the W layout depends on the spin of i and on the j block
     for i in (0, oa):
-        for jj in (0, oa):
-            most = max(most, _w_tensor(V, O1, Ob, i, jj).nelems)
+        for jt in range(Oj.num_tiles):
+            most = max(most, _w_tensor(V, O1, Oj, Ob, i, jt).nelems)
     buf = torch.empty(most * 8 + 256, dtype=torch.uint8, device=f"cuda:{ec.device}")
-    return TriplesProblem(ec, V, Ob, O1, eps, T, buf, most)
+    return TriplesProblem(ec, V, Ob, O1, Oj, Vd, eps, T, buf, most)
 
 
-def _w_tensor(V, O1, Ob, i, j):
-    return Tensor([V, V, V, O1.sub(i, i + 1), O1.sub(j, j + 1), Ob], spin=(3, 3))
+def _w_tensor(V, O1, Oj, Ob, i, jt):
+    return Tensor([V, V, V, O1.sub(i, i + 1), Oj.sub(jt, jt + 1), Ob], spin=(3, 3))
 
 
-def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, j: int):
-    """Queues W(a,b,c,k) for the occupied pair (i, j) and slot SLOT_E += sum W^2 / D.
-    Returns (W tensor, FP64 FLOPs of the two contractions)."""
-    Wt = _w_tensor(P.V, P.O1, P.Ob, i, j)
+def steps(P: TriplesProblem):
+    """All streaming steps: (occupied index i, tile index of the j block)."""
+    return [(i, jt) for i in range(P.O1.num_tiles) for jt in range(P.Oj.num_tiles)]
+
+
+def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int):
+    """Queues W(a,b,c,k) for occupied index i and j block jt, and slot SLOT_E +=
+    sum W^2 / D.  Returns (W tensor, FP64 FLOPs of the two contractions)."""
+    Wt = _w_tensor(P.V, P.O1, P.Oj, P.Ob, i, jt)
     Wt.attach(P.ec, (P.buffer.data_ptr() + 255) // 256 * 256, P.most * 8)
-    a, b, c, d = P.V.labels(4)
+    a, b, c = P.V.labels(3)
+    (d,) = P.Vd.labels(1)
     k, l = P.Ob.labels(2)
     li, lj = Wt.spaces[3].label(), Wt.spaces[4].label()
     T = P.T
@@ -139,7 +154,7 @@ def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, j: int):
 
 
 def energy(P: TriplesProblem, pairs, sch: Scheduler):
-    """E summed over the given occupied pairs; returns (E, FP64 FLOPs, device ms)."""
+    """E summed over the given steps (i, j block); returns (E, FP64 FLOPs, device ms)."""
     import torch
     stream = torch.cuda.ExternalStream(P.ec.stream)
     sch.set_scalar(SLOT_E, 0.0).execute()
@@ -154,34 +169,55 @@ def energy(P: TriplesProblem, pairs, sch: Scheduler):
         e1.synchronize()
         ms += e0.elapsed_time(e1)
         flops += fl
+        sch.release()  # this step's work lists never recur
         Wt.deallocate()
     return float(sch.scalars(SLOT_E + 1)[SLOT_E]), flops, ms
 
 
 def main(argv=None):
+    """Sampled full-size run: FP64 and split-INT8 energies and times over a seeded
+    sample of streaming steps, the full run extrapolated, and the INT8 W of one step
+    compared element by element with the FP64 one on the device."""
+    import torch
     p = argparse.ArgumentParser()
     p.add_argument("--oa", type=int, default=25)
     p.add_argument("--va", type=int, default=250)
     p.add_argument("--tile", type=int, default=40)
+    p.add_argument("--jtile", type=int, default=2)
+    p.add_argument("--dtile", type=int, default=0, help="tiling of the summed d (0: one tile per spin block)")
     p.add_argument("--seed", type=int, default=4)
-    p.add_argument("--pairs", type=int, default=8)
-    p.add_argument("--pool-gib", type=int, default=150)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--pool-gib", type=int, default=80)
     args = p.parse_args(argv)
     ec = ExecutionContext(0, args.pool_gib << 30)
-    P = build(args.oa, args.va, tile=args.tile, seed=args.seed, ec=ec)
-    no = 2 * args.oa
+    P = build(args.oa, args.va, tile=args.tile, jtile=args.jtile, dtile=args.dtile, seed=args.seed, ec=ec)
+    allsteps = steps(P)
     rng = np.random.default_rng(args.seed + 5)
-    pairs = [(int(x) // no, int(x) % no) for x in rng.choice(no * no, size=args.pairs, replace=False)]
-    out = {"workload": f"triples_energy_O{no}_V{2 * args.va}_tile{args.tile}", "sampled_pairs": pairs,
-           "pairs_total": no * no}
-    res = {}
+    sample = [allsteps[int(x)] for x in rng.choice(len(allsteps), size=min(args.steps, len(allsteps)), replace=False)]
+    out = {"workload": f"triples_energy_O{2 * args.oa}_V{2 * args.va}_tile{args.tile}_jtile{args.jtile}_dtile{args.dtile}",
+           "sampled_steps": sample, "steps_total": len(allsteps)}
+    res, wref = {}, None
+    base = (P.buffer.data_ptr() + 255) // 256 * 256 - P.buffer.data_ptr()
     for name, mode in (("fp64", Precision.FP64), ("int8", Precision.INT8)):
         ec.set_precision(mode, 1e-11)
         sch = Scheduler(ec)
-        energy(P, pairs[:1], sch)  # warm-up: kernels, digit layouts
-        e, fl, ms = energy(P, pairs, sch)
-        res[name] = {"energy_sample": e, "flops_sample": fl, "device_ms": ms, "tflops": fl / ms / 1e9,
-                     "full_run_s_extrapolated": ms / len(pairs) * no * no / 1e3}
+        energy(P, sample[:1], sch)  # warm-up: kernels, digit layouts
+        e, fl, ms = energy(P, sample, sch)
+        res[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9,
+                     "full_run_s_extrapolated": ms / len(sample) * len(allsteps) / 1e3}
+        # W of the first sampled step, kept on the device for the comparison
+        Wt, _ = queue_pair(P, sch, *sample[0])
+        sch.execute(ExecutionHW.GPU)
+        wv = P.buffer[base:base + 8 * Wt.nelems].view(torch.float64)
+        if wref is None:
+            wref = wv.clone()
+        else:  # chunked, to keep temporaries small
+            dmax, rmax, ch = 0.0, 0.0, 1 << 27
+            for o in range(0, wv.numel(), ch):
+                dmax = max(dmax, float((wv[o:o + ch] - wref[o:o + ch]).abs().max()))
+                rmax = max(rmax, float(wref[o:o + ch].abs().max()))
+            out["int8_vs_fp64_W_max_rel_err"] = dmax / rmax
+        Wt.deallocate()
     ec.set_precision(Precision.FP64)
     out.update(res)
     out["int8_vs_fp64_energy_rel_err"] = abs(res["int8"]["energy_sample"] - res["fp64"]["energy_sample"]) / abs(

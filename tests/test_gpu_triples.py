@@ -1,6 +1,6 @@
 """Streamed triples energy (tamm_b200.triples) against a dense restatement of its
-formula, on a small spin-blocked MO space (O=6, V=16, tile 4), summed over every
-occupied pair:
+formula, on a small spin-blocked MO space (O=6, V=16, tile 4, j streamed in blocks of 2),
+summed over every streaming step:
 
     W(a,b,c,i,j,k) = sum_d t2(a,d,i,j) v(b,c,d,k) - sum_l t2(a,b,i,l) v(l,c,j,k)
     E = sum W^2 / (e_i + e_j + e_k - e_a - e_b - e_c)
@@ -53,15 +53,16 @@ def _reference(P, oa, va, seed):
     return float(np.sum(Wd * Wd / D))
 
 
+@pytest.mark.parametrize("dtile", [4, 0])
 @pytest.mark.parametrize("mode,tol", [(tb.Precision.FP64, 1e-12), (tb.Precision.INT8, 1e-10)])
-def test_streamed_triples_energy(ec, mode, tol):
+def test_streamed_triples_energy(ec, mode, tol, dtile):
     oa, va, seed = 3, 8, 4
-    P = triples.build(oa, va, tile=4, seed=seed, ec=ec)
+    # j blocks of 2, 1 (ragged); d on the output tiling (4) or one tile per spin block (0)
+    P = triples.build(oa, va, tile=4, jtile=2, dtile=dtile, seed=seed, ec=ec)
     want = _reference(P, oa, va, seed)
-    no = 2 * oa
     ec.set_precision(mode, 1e-11)
     try:
-        e, flops, _ = triples.energy(P, [(i, j) for i in range(no) for j in range(no)], tb.Scheduler(ec))
+        e, flops, _ = triples.energy(P, triples.steps(P), tb.Scheduler(ec))
     finally:
         ec.set_precision(tb.Precision.FP64)
     assert flops > 0 and want < 0
