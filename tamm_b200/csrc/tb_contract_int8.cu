@@ -152,15 +152,12 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
           const int      np = (b.K - p0) >> 1;
           const double2* s2 = reinterpret_cast<const double2*>(s + p0);
           int            k  = lane;
-          for(; k + 96 < np; k += 128) {
-            double2 t[4];
+          for(; k + 224 < np; k += 256) {
+            double2 t[8];
 #pragma unroll
-            for(int x = 0; x < 4; x++) t[x] = __ldg(s2 + k + 32 * x);
+            for(int x = 0; x < 8; x++) t[x] = __ldg(s2 + k + 32 * x);
 #pragma unroll
-            for(int x = 0; x < 4; x++) {
-              m[2 * x]     = fmax(m[2 * x], fabs(t[x].x));
-              m[2 * x + 1] = fmax(m[2 * x + 1], fabs(t[x].y));
-            }
+            for(int x = 0; x < 8; x++) m[x] = fmax(m[x], fmax(fabs(t[x].x), fabs(t[x].y)));
           }
           for(; k < np; k += 32) {
             const double2 t = __ldg(s2 + k);
@@ -226,29 +223,33 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
       uint8_t* out = dst + b.dst_off + (int64_t) (ch.y / b.tile_rows) * nkc * S * b.tile_rows * KC + g8 * 128 + r * 16 +
                      q * 4;
       const bool vec = live && b.kcontig && !(reinterpret_cast<uintptr_t>(s) & 15);
-      for(int k16 = warp; k16 < b.K_pad / 16; k16 += 8) {
+      // loads of one 16-value column (this thread's row and quad) and the conversion
+      // of it into S 4-byte digit words; two columns per iteration keep the second
+      // column's loads in flight while the first converts
+      auto load4 = [&](int k16, double (&v)[4]) {
         const int k0 = k16 * 16 + q * 4;
-        double    v[4];
         if(vec && k0 + 3 < b.K) {
           const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
           const double2 v23 = __ldg(reinterpret_cast<const double2*>(s + k0 + 2));
           v[0] = v01.x, v[1] = v01.y, v[2] = v23.x, v[3] = v23.y;
         }
         else
-  #pragma unroll
+#pragma unroll
           for(int x = 0; x < 4; x++) {
             const int k = k0 + x;
             v[x]        = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
           }
+      };
+      auto emit = [&](int k16, const double (&v)[4]) {
         uint32_t lo[4], hi[4];
-  #pragma unroll
+#pragma unroll
         for(int x = 0; x < 4; x++) {
           const uint64_t Y = (uint64_t) __double2ll_rn(v[x] * f1 * f2) + bias;
           lo[x]            = (uint32_t) Y;
           hi[x]            = (uint32_t) (Y >> 32);
         }
         uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
-  #pragma unroll
+#pragma unroll
         for(int i = 0; i < S; i++) {
           const int p = S - 1 - i; // byte of Y holding digit i
           uint32_t  w;
@@ -264,6 +265,15 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
           }
           *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * 16) = w ^ 0x80808080u;
         }
+      };
+      const int n16 = b.K_pad / 16;
+      for(int k16 = warp; k16 < n16; k16 += 16) {
+        double v0[4], v1[4];
+        load4(k16, v0);
+        const bool two = k16 + 8 < n16;
+        if(two) load4(k16 + 8, v1);
+        emit(k16, v0);
+        if(two) emit(k16 + 8, v1);
       }
     }
     __syncthreads(); // s_sh / s_off are rewritten for the next chunk
