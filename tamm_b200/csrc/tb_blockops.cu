@@ -173,28 +173,6 @@ __global__ void k_dot_final(const double* __restrict__ part, int np, double* __r
   }
 }
 
-// t += scale * r / D over the admitted blocks of t (r has t's layout), with
-// D = sum over modes of sign_m * eps[first_m + index_m]: the orbital-energy
-// denominator of a CC amplitude update (D = e_a + e_b - e_i - e_j for t2(a,b,i,j)).
-// One CTA per block, threads over its elements.
-__global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, const double* __restrict__ r,
-                                                    double scale, const DenomBlock* __restrict__ blocks,
-                                                    int nmodes, const double* __restrict__ eps, DenomSigns sg) {
-  const DenomBlock b = blocks[blockIdx.x];
-  int64_t          n = 1;
-  for(int m = 0; m < nmodes; m++) n *= b.dims[m];
-  for(int64_t e = threadIdx.x; e < n; e += blockDim.x) {
-    int64_t x = e;
-    double  d = 0.0;
-    for(int m = nmodes - 1; m >= 0; m--) {
-      const int64_t q = x / b.dims[m];
-      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
-      x = q;
-    }
-    t[b.off + e] += scale * r[b.off + e] / d;
-  }
-}
-
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -355,62 +333,71 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
   return h;
 }
 
-// part[block] = sum over the block's elements of w^2 / D (D as in k_denom), one CTA
-// per block, in chunks of 256 rows (a row: all modes but the last).  Each thread forms
-// the row part of D for one row of the chunk into shared memory (the last mode's
-// part is tabulated once per block), then the CTA streams the chunk's elements with
-// coalesced loads.  Deterministic.
+// Orbital-energy denominators over the admitted blocks of a tensor: for element
+// (x_0, ..., x_last) of a block, D = sum_m s_m * eps[first_m + x_m].  The work is
+// cut into units of up to 256 rows of one block (a row: all modes but the last), one
+// CTA per unit: each thread forms the row part of D for one row into shared memory
+// (the last mode's part is tabulated once per unit), then the CTA streams the unit's
+// elements with coalesced loads.
+//   ENERGY:  part[unit] = sum w^2 / D  (w = t; deterministic, summed by
+//            k_denom_energy_final)
+//   update:  t += scale * r / D
 constexpr int kDenCols = 1024; // last-mode extents tabulated in shared memory
 
-__global__ void __launch_bounds__(kThreads) k_denom_energy(const double* __restrict__ w,
-                                                           const DenomBlock* __restrict__ blocks, int nmodes,
-                                                           const double* __restrict__ eps, DenomSigns sg,
-                                                           double* __restrict__ part) {
+template<bool ENERGY>
+__global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, const double* __restrict__ r, double scale,
+                                                    const DenomBlock* __restrict__ blocks,
+                                                    const DenomUnit* __restrict__ units, int nmodes,
+                                                    const double* __restrict__ eps, DenomSigns sg,
+                                                    double* __restrict__ part) {
   __shared__ double drow[kThreads];
   __shared__ double dcol[kDenCols];
-  const DenomBlock  b    = blocks[blockIdx.x];
+  const DenomUnit   u    = units[blockIdx.x];
+  const DenomBlock  b    = blocks[u.block];
   const int         last = nmodes - 1;
   const int64_t     ncol = b.dims[last];
   int64_t           nrow = 1;
   for(int m = 0; m < last; m++) nrow *= b.dims[m];
-  const int     tid  = threadIdx.x;
-  const bool    tab  = ncol <= kDenCols;
-  const double* el   = eps + b.first[last];
+  const int     tid = threadIdx.x;
+  const bool    tab = ncol <= kDenCols;
+  const double* el  = eps + b.first[last];
   if(tab)
     for(int64_t c = tid; c < ncol; c += kThreads) dcol[c] = sg.s[last] * __ldg(el + c);
-  double s = 0.0;
-  for(int64_t r0 = 0; r0 < nrow; r0 += kThreads) {
-    __syncthreads(); // the previous chunk's rows are no longer read
-    if(r0 + tid < nrow) {
-      int64_t x = r0 + tid;
-      double  d = 0.0;
-      for(int m = last - 1; m >= 0; m--) {
-        const int64_t q = x / b.dims[m];
-        d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
-        x = q;
-      }
-      drow[tid] = d;
+  const int64_t rows = nrow - u.r0 < kThreads ? nrow - u.r0 : kThreads;
+  if(tid < rows) {
+    int64_t x = u.r0 + tid;
+    double  d = 0.0;
+    for(int m = last - 1; m >= 0; m--) {
+      const int64_t q = x / b.dims[m];
+      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
+      x = q;
     }
-    __syncthreads();
-    const int64_t rows = nrow - r0 < kThreads ? nrow - r0 : kThreads;
-    const int32_t nel  = (int32_t) (rows * ncol), nc = (int32_t) ncol;
-    const double* base = w + b.off + r0 * ncol;
-    for(int32_t e = tid; e < nel; e += kThreads) {
-      const int32_t rr = e / nc, cc = e - rr * nc;
-      const double  v  = base[e];
-      s += v * v / (drow[rr] + (tab ? dcol[cc] : sg.s[last] * __ldg(el + cc)));
-    }
+    drow[tid] = d;
   }
+  __syncthreads();
+  const int32_t nel = (int32_t) (rows * ncol), nc = (int32_t) ncol;
+  const int64_t base = b.off + u.r0 * ncol;
+  double        s    = 0.0;
+  for(int32_t e = tid; e < nel; e += kThreads) {
+    const int32_t rr = e / nc, cc = e - rr * nc;
+    const double  D  = drow[rr] + (tab ? dcol[cc] : sg.s[last] * __ldg(el + cc));
+    if constexpr(ENERGY) {
+      const double v = t[base + e];
+      s += v * v / D;
+    }
+    else t[base + e] += scale * r[base + e] / D;
+  }
+  if constexpr(ENERGY) {
 #pragma unroll
-  for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  __shared__ double ws[kThreads / 32];
-  __syncthreads();
-  if((tid & 31) == 0) ws[tid >> 5] = s;
-  __syncthreads();
-  if(tid == 0) {
-    double t = 0.0;
-    for(int i = 0; i < kThreads / 32; i++) t += ws[i];
-    part[blockIdx.x] = t;
+    for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double ws[kThreads / 32];
+    if((tid & 31) == 0) ws[tid >> 5] = s;
+    __syncthreads();
+    if(tid == 0) {
+      double v = 0.0;
+      for(int i = 0; i < kThreads / 32; i++) v += ws[i];
+      part[blockIdx.x] = v;
+    }
   }
 }
 
@@ -431,10 +418,13 @@ __global__ void k_denom_energy_final(const double* __restrict__ part, int np, do
 
 __global__ void k_set_scalar(double* out, double v) { *out = v; }
 
-void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
-                         const double* eps, DenomSigns signs, double* part, double* out, cudaStream_t stream) {
-  if(nblocks > 0) k_denom_energy<<<nblocks, kThreads, 0, stream>>>(w, blocks, nmodes, eps, signs, part);
-  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, nblocks, scale, out);
+void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, const DenomUnit* units,
+                         int nunits, int nmodes, const double* eps, DenomSigns signs, double* part, double* out,
+                         cudaStream_t stream) {
+  if(nunits > 0)
+    k_denom<true><<<nunits, kThreads, 0, stream>>>(const_cast<double*>(w), nullptr, 0.0, blocks, units, nmodes, eps,
+                                                   signs, part);
+  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, nunits, scale, out);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -454,10 +444,10 @@ void launch_dot_to(const double* x, const double* y, int64_t n, double scale, in
   TB_CUDA(cudaGetLastError());
 }
 
-void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
-                  const double* eps, DenomSigns signs, cudaStream_t stream) {
-  if(nblocks <= 0) return;
-  k_denom<<<nblocks, kThreads, 0, stream>>>(t, r, scale, blocks, nmodes, eps, signs);
+void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, const DenomUnit* units,
+                  int nunits, int nmodes, const double* eps, DenomSigns signs, cudaStream_t stream) {
+  if(nunits <= 0) return;
+  k_denom<false><<<nunits, kThreads, 0, stream>>>(t, r, scale, blocks, units, nmodes, eps, signs, nullptr);
   TB_CUDA(cudaGetLastError());
 }
 

@@ -836,6 +836,7 @@ int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const d
   op.a     = to_labeled(r);
   op.alpha = alpha;
   const Tensor& T = *op.lhs.t;
+  TB_EXPECTS(T.nmodes >= 1, "denominator update of a scalar tensor");
   TB_EXPECTS(op.lhs.labels == op.a.labels && T.keys == op.a.t->keys && T.offsets == op.a.t->offsets,
              "denominator update: r needs t's labels and block layout");
   for(int m = 1; m < T.nmodes; m++)
@@ -859,6 +860,7 @@ int tb_sched_denom_energy(tb_sched s, int slot, double alpha, tb_labeled w, cons
   op.alpha = alpha;
   op.slot  = slot;
   const Tensor& T = *op.lhs.t;
+  TB_EXPECTS(T.nmodes >= 1, "denominator energy of a scalar tensor");
   for(int m = 1; m < T.nmodes; m++)
     TB_EXPECTS(T.tis[m]->root->is == T.tis[0]->root->is, "denominator energy: all modes over one root index space");
   auto d = std::make_shared<DenomSpec>();

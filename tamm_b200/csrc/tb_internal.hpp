@@ -161,11 +161,17 @@ struct DenomBlock {
 struct DenomSigns {
   double s[kMaxModes];
 };
-void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
-                  const double* eps, DenomSigns signs, cudaStream_t stream);
-// *out += scale * sum w^2 / D over the blocks (part: nblocks doubles of scratch).
-void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, int nblocks, int nmodes,
-                         const double* eps, DenomSigns signs, double* part, double* out, cudaStream_t stream);
+// A unit of denominator work: up to 256 consecutive rows of one block.
+struct DenomUnit {
+  int32_t block, pad;
+  int64_t r0;
+};
+void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, const DenomUnit* units,
+                  int nunits, int nmodes, const double* eps, DenomSigns signs, cudaStream_t stream);
+// *out += scale * sum w^2 / D over the blocks (part: nunits doubles of scratch).
+void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, const DenomUnit* units,
+                         int nunits, int nmodes, const double* eps, DenomSigns signs, double* part, double* out,
+                         cudaStream_t stream);
 void launch_set_scalar(double* out, double v, cudaStream_t stream);
 // Reads and clears the device error word of the split-INT8 launches of a work list;
 // throws TB_ERR_TIMEOUT if a device-side wait gave up.

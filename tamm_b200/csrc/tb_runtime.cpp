@@ -585,7 +585,8 @@ void Sched::run(Op& op) {
     if(!d.d_blocks) d.build(*op.lhs.t, ctx);
     DenomSigns sg{};
     for(int m = 0; m < kMaxModes; m++) sg.s[m] = d.signs[m];
-    launch_denom(op.lhs.t->data, op.a.t->data, op.alpha, d.d_blocks, d.nblocks, op.lhs.t->nmodes, d.d_eps, sg, st);
+    launch_denom(op.lhs.t->data, op.a.t->data, op.alpha, d.d_blocks, d.d_units, d.nunits, op.lhs.t->nmodes, d.d_eps,
+                 sg, st);
     return;
   }
   if(op.kind == Op::DenomEnergy) {
@@ -594,8 +595,8 @@ void Sched::run(Op& op) {
     if(!d.d_blocks) d.build(*op.lhs.t, ctx);
     DenomSigns sg{};
     for(int m = 0; m < kMaxModes; m++) sg.s[m] = d.signs[m];
-    launch_denom_energy(op.lhs.t->data, op.alpha, d.d_blocks, d.nblocks, op.lhs.t->nmodes, d.d_eps, sg, d.d_part,
-                        scalars() + op.slot, st);
+    launch_denom_energy(op.lhs.t->data, op.alpha, d.d_blocks, d.d_units, d.nunits, op.lhs.t->nmodes, d.d_eps, sg,
+                        d.d_part, scalars() + op.slot, st);
     return;
   }
   if(op.kind == Op::SetScalar) {
@@ -752,14 +753,25 @@ void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c) {
     }
     blocks.push_back(b);
   }
+  std::vector<DenomUnit> units;
+  for(size_t bi = 0; bi < blocks.size(); bi++) {
+    int64_t nrow = 1;
+    for(int m = 0; m + 1 < T.nmodes; m++) nrow *= blocks[bi].dims[m];
+    for(int64_t r0 = 0; r0 < nrow; r0 += 256) units.push_back(DenomUnit{(int32_t) bi, 0, r0});
+  }
+  TB_EXPECTS(units.size() < (1ull << 31), "too many denominator work units");
   ctx     = c;
   nblocks = (int) blocks.size();
+  nunits  = (int) units.size();
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_eps), sizeof(double) * std::max<size_t>(eps.size(), 1)));
   TB_CUDA(cudaMemcpy(d_eps, eps.data(), sizeof(double) * eps.size(), cudaMemcpyHostToDevice));
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_blocks), sizeof(DenomBlock) * std::max<size_t>(blocks.size(), 1)));
   if(!blocks.empty())
     TB_CUDA(cudaMemcpy(d_blocks, blocks.data(), sizeof(DenomBlock) * blocks.size(), cudaMemcpyHostToDevice));
-  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_part), sizeof(double) * std::max<size_t>(blocks.size(), 1)));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_units), sizeof(DenomUnit) * std::max<size_t>(units.size(), 1)));
+  if(!units.empty())
+    TB_CUDA(cudaMemcpy(d_units, units.data(), sizeof(DenomUnit) * units.size(), cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_part), sizeof(double) * std::max<size_t>(units.size(), 1)));
 }
 
 DenomSpec::~DenomSpec() {
@@ -767,6 +779,7 @@ DenomSpec::~DenomSpec() {
   if(d_eps) cudaFree(d_eps);
   if(d_blocks) cudaFree(d_blocks);
   if(d_part) cudaFree(d_part);
+  if(d_units) cudaFree(d_units);
 }
 
 Graph::~Graph() {

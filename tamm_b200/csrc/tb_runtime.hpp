@@ -144,8 +144,9 @@ struct DenomSpec {
   double                  signs[kMaxModes] = {0};
   double*                 d_eps    = nullptr;
   DenomBlock*             d_blocks = nullptr;
-  double*                 d_part   = nullptr; // per-block partial sums (energy reduction)
-  int                     nblocks  = 0;
+  DenomUnit*              d_units  = nullptr; // 256-row work units
+  double*                 d_part   = nullptr; // per-unit partial sums (energy reduction)
+  int                     nblocks  = 0, nunits = 0;
   void                    build(const Tensor& t, const std::shared_ptr<Ctx>& ctx);
   std::shared_ptr<Ctx>    ctx;
   ~DenomSpec();
