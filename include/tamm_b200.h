@@ -243,6 +243,12 @@ int tb_tensor_add(tb_tensor t, const int64_t* blockid, const double* host, int64
 int tb_tensor_write(tb_tensor t, const double* host, int64_t n);
 int tb_tensor_read(tb_tensor t, double* host, int64_t n);
 int tb_tensor_norm(tb_tensor t, double* out);
+/* Checkpoint / restart (TAMM's write_to_disk / read_from_disk, tamm_io.hpp:230-465,
+ * in its tammio element order: admitted blocks in row-major tile order, each block
+ * row-major — a raw file instead of an HDF5 dataset).  The file records the spaces'
+ * tiles, spins and the spin mask; load checks them against the tensor. */
+int tb_tensor_save(tb_tensor t, const char* path);
+int tb_tensor_load(tb_tensor t, const char* path);
 
 /* A labelled operand: tensor, per-mode int label, per-mode label space (NULL array
  * or NULL entry: the tensor's own tiled space; else a sub-space of it, as for

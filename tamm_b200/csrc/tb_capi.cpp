@@ -3,6 +3,7 @@
 #include "tb_runtime.hpp"
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 
@@ -631,6 +632,83 @@ int tb_tensor_read(tb_tensor t, double* host, int64_t n) {
   TB_CUDA(cudaSetDevice(t->p->ctx->device));
   TB_CUDA(cudaMemcpyAsync(host, t->p->data, sizeof(double) * n, cudaMemcpyDeviceToHost, t->p->ctx->stream));
   TB_CUDA(cudaStreamSynchronize(t->p->ctx->stream));
+  TB_API_END
+}
+
+// Checkpoint file: header (magic, version, structure) + block keys + the packed store.
+// The payload is the tensor's admitted blocks in row-major tile order, each block
+// row-major: the element order of TAMM's tammio dataset (tamm_io.hpp:230-330, the
+// file_offset of a block = sizes of the admitted blocks before it), without HDF5.
+namespace {
+constexpr char    kCkptMagic[8] = {'T', 'B', 'T', 'E', 'N', 'S', '0', '1'};
+struct CkptFile {
+  FILE* f = nullptr;
+  ~CkptFile() {
+    if(f) fclose(f);
+  }
+};
+std::vector<int64_t> ckpt_structure(const Tensor& T) {
+  std::vector<int64_t> h{T.nmodes, T.has_spin ? 1 : 0};
+  for(int m = 0; m < T.nmodes; m++) {
+    h.push_back(T.mask[m]);
+    h.push_back(T.tis[m]->ntiles());
+    for(int64_t x = 0; x < T.tis[m]->ntiles(); x++) {
+      h.push_back(T.tis[m]->size(x));
+      h.push_back(T.tis[m]->spin(x));
+    }
+  }
+  h.push_back((int64_t) T.keys.size());
+  h.push_back(T.nelems);
+  return h;
+}
+} // namespace
+
+int tb_tensor_save(tb_tensor t, const char* path) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && path != nullptr);
+  const Tensor& T = *t->p;
+  T.require_allocated();
+  std::vector<double> host(std::max<int64_t>(T.nelems, 1));
+  TB_CUDA(cudaSetDevice(T.ctx->device));
+  TB_CUDA(cudaMemcpyAsync(host.data(), T.data, sizeof(double) * T.nelems, cudaMemcpyDeviceToHost, T.ctx->stream));
+  TB_CUDA(cudaStreamSynchronize(T.ctx->stream));
+  const std::vector<int64_t> h = ckpt_structure(T);
+  const int64_t              nh = (int64_t) h.size();
+  CkptFile                   cf;
+  cf.f = fopen(path, "wb");
+  TB_EXPECTS(cf.f != nullptr, std::string("cannot open for writing: ") + path);
+  bool ok = fwrite(kCkptMagic, 1, 8, cf.f) == 8 && fwrite(&nh, 8, 1, cf.f) == 1 &&
+            fwrite(h.data(), 8, h.size(), cf.f) == h.size() &&
+            fwrite(T.keys.data(), 8, T.keys.size(), cf.f) == T.keys.size() &&
+            (T.nelems == 0 || fwrite(host.data(), 8, T.nelems, cf.f) == (size_t) T.nelems);
+  ok = (fclose(cf.f) == 0) && ok;
+  cf.f = nullptr;
+  TB_EXPECTS(ok, std::string("write failed: ") + path);
+  TB_API_END
+}
+
+int tb_tensor_load(tb_tensor t, const char* path) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && path != nullptr);
+  Tensor& T = *t->p;
+  T.require_allocated();
+  CkptFile cf;
+  cf.f = fopen(path, "rb");
+  TB_EXPECTS(cf.f != nullptr, std::string("cannot open for reading: ") + path);
+  char    magic[8];
+  int64_t nh = 0;
+  TB_EXPECTS(fread(magic, 1, 8, cf.f) == 8 && std::memcmp(magic, kCkptMagic, 8) == 0, "not a tensor checkpoint");
+  TB_EXPECTS(fread(&nh, 8, 1, cf.f) == 1 && nh > 0 && nh < (1ll << 32), "corrupt checkpoint header");
+  std::vector<int64_t> h(nh), keys;
+  TB_EXPECTS(fread(h.data(), 8, h.size(), cf.f) == h.size(), "truncated checkpoint header");
+  TB_EXPECTS(h == ckpt_structure(T), "checkpoint structure (spaces, tiles, spins, spin mask) differs from the tensor's");
+  keys.resize(T.keys.size());
+  TB_EXPECTS(fread(keys.data(), 8, keys.size(), cf.f) == keys.size() && keys == T.keys, "checkpoint block table differs");
+  std::vector<double> host(std::max<int64_t>(T.nelems, 1));
+  TB_EXPECTS(T.nelems == 0 || fread(host.data(), 8, T.nelems, cf.f) == (size_t) T.nelems, "truncated checkpoint data");
+  TB_CUDA(cudaSetDevice(T.ctx->device));
+  TB_CUDA(cudaMemcpyAsync(T.data, host.data(), sizeof(double) * T.nelems, cudaMemcpyHostToDevice, T.ctx->stream));
+  TB_CUDA(cudaStreamSynchronize(T.ctx->stream));
   TB_API_END
 }
 

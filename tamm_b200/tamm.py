@@ -238,6 +238,16 @@ class Tensor:
         call("tb_tensor_deallocate", self.h)
         self.ec = None
 
+    def save(self, path: str):
+        """Checkpoint (TAMM's write_to_disk element order, raw file)."""
+        call("tb_tensor_save", self.h, str(path).encode())
+        return self
+
+    def load(self, path: str):
+        """Restart from a checkpoint of a tensor with the same spaces and spin mask."""
+        call("tb_tensor_load", self.h, str(path).encode())
+        return self
+
     def attach(self, ec: ExecutionContext, device_ptr: int, nbytes: int):
         """Caller-owned device storage (>= 8 * nelems bytes, 16-byte aligned), e.g. one
         buffer shared by tensors used one after another in stream order."""
