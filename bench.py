@@ -373,7 +373,9 @@ def main():
             "max_rel_err_vs_fp64": max_rel_err,
             "e2e": {"value": e2e_val, "unit": "TFLOP/s", "h2d_bytes_per_step": 8 * lad.t2.nelems,
                     "d2h_bytes_per_step": 8 * lad.r2.nelems, "ms_per_step": e2e_ms},
-            "gpu_launches": args.steps * (3 if headline == "int8" else 1),
+            # our kernels per step: INT8 = split A, split B, k_task_slices, GEMM; BF16x3 =
+            # split A, split B, GEMM (its digit counts come from a memset); FP64 = one kernel
+            "gpu_launches": args.steps * {"int8": 4, "bf16x3": 3, "fp64": 1}[headline],
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
