@@ -179,7 +179,10 @@ int tb_ctx_create(int device, int64_t pool_bytes, tb_ctx* out);
 int tb_ctx_destroy(tb_ctx ctx);
 int tb_ctx_set_precision(tb_ctx ctx, int mode, double err_target, int nslices);
 int tb_ctx_stream(tb_ctx ctx, void** stream);
-int tb_ctx_synchronize(tb_ctx ctx);
+int tb_ctx_synchronize(tb_ctx ctx); /* compute and copy streams */
+/* Makes later work on the compute stream wait for everything enqueued so far on the
+ * context's copy streams (e.g. to time transfers with events on the compute stream). */
+int tb_ctx_join(tb_ctx ctx);
 /* Arena occupancy: bytes in use, high-water mark, capacity. */
 int tb_ctx_arena_info(tb_ctx ctx, int64_t* used, int64_t* peak, int64_t* capacity);
 
@@ -239,6 +242,14 @@ int tb_tensor_attach(tb_tensor t, tb_ctx ctx, void* device_ptr, int64_t bytes);
 int tb_tensor_get(tb_tensor t, const int64_t* blockid, double* host, int64_t n);
 int tb_tensor_put(tb_tensor t, const int64_t* blockid, const double* host, int64_t n);
 int tb_tensor_add(tb_tensor t, const int64_t* blockid, const double* host, int64_t n);
+/* Asynchronous whole-store transfers with pinned host memory (no counterpart in
+ * TAMM): they run on the context's copy streams, a write after the compute work
+ * already enqueued on the tensor and before any compute enqueued later, a read after
+ * the compute work enqueued on the tensor.  With two sets of tensors used in turn,
+ * the transfers of one step overlap the contraction of the next.  The host buffer
+ * must stay untouched until tb_ctx_synchronize / tb_sched_wait returns. */
+int tb_tensor_write_async(tb_tensor t, const double* host, int64_t n);
+int tb_tensor_read_async(tb_tensor t, double* host, int64_t n);
 /* Whole packed store <-> host (n == nelems). */
 int tb_tensor_write(tb_tensor t, const double* host, int64_t n);
 int tb_tensor_read(tb_tensor t, double* host, int64_t n);
@@ -292,6 +303,11 @@ int tb_mult_owned(tb_labeled lhs, tb_labeled a, tb_labeled b, int rank, int nran
  * runs on the GPU (there is no host execution path); profile records per-op device
  * times readable with tb_sched_profile. */
 int tb_sched_execute(tb_sched s, int hw, int profile);
+/* Scheduler::execute without waiting: the ops are enqueued on the context's stream
+ * and the call returns; split-INT8 device error words are checked by tb_sched_wait,
+ * which waits for the compute and copy streams. */
+int tb_sched_execute_async(tb_sched s);
+int tb_sched_wait(tb_sched s);
 /* Number of ops in the last execute; per op: device milliseconds and FP64 FLOPs. */
 int tb_sched_profile(tb_sched s, int64_t* nops, double* ms, double* flops, int64_t cap);
 /* Kernel statistics of op `index` of the last profiled execute (zeros for Set/Add ops). */

@@ -110,6 +110,11 @@ PROTOS = {
     "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
     "tb_tensor_attach": [h, h, vp, C.c_int64],
     "tb_tensor_save": [h, C.c_char_p],
+    "tb_ctx_join": [h],
+    "tb_tensor_write_async": [h, dp, C.c_int64],
+    "tb_tensor_read_async": [h, dp, C.c_int64],
+    "tb_sched_execute_async": [h],
+    "tb_sched_wait": [h],
     "tb_tensor_load": [h, C.c_char_p],
     "tb_sched_set_owner": [h, C.c_int, C.c_int],
     "tb_mult_owned": [tb_labeled, tb_labeled, tb_labeled, C.c_int, C.c_int, i64p, dp, i64p, C.c_int64],

@@ -327,7 +327,26 @@ int tb_ctx_stream(tb_ctx ctx, void** stream) {
 int tb_ctx_synchronize(tb_ctx ctx) {
   TB_API_BEGIN
   REQUIRE_ARG(ctx != nullptr);
+  TB_CUDA(cudaSetDevice(ctx->p->device));
   TB_CUDA(cudaStreamSynchronize(ctx->p->stream));
+  if(ctx->p->h2d) TB_CUDA(cudaStreamSynchronize(ctx->p->h2d));
+  if(ctx->p->d2h) TB_CUDA(cudaStreamSynchronize(ctx->p->d2h));
+  TB_API_END
+}
+
+int tb_ctx_join(tb_ctx ctx) {
+  TB_API_BEGIN
+  REQUIRE_ARG(ctx != nullptr);
+  Ctx& c = *ctx->p;
+  TB_CUDA(cudaSetDevice(c.device));
+  for(cudaStream_t x: {c.h2d, c.d2h}) {
+    if(!x) continue;
+    cudaEvent_t e;
+    TB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TB_CUDA(cudaEventRecord(e, x));
+    TB_CUDA(cudaStreamWaitEvent(c.stream, e, 0));
+    TB_CUDA(cudaEventDestroy(e)); // released once the wait is resolved
+  }
   TB_API_END
 }
 
@@ -712,6 +731,47 @@ int tb_tensor_load(tb_tensor t, const char* path) {
   TB_API_END
 }
 
+// Asynchronous host transfers on the context's copy streams, ordered against the
+// compute stream by events: a write waits until the compute work enqueued so far that
+// touched the tensor is done, and later compute work waits for the write; a read
+// waits for that compute work.  Host buffers must be pinned and stay untouched until
+// tb_ctx_synchronize (or tb_sched_wait) returns.
+int tb_tensor_write_async(tb_tensor t, const double* host, int64_t n) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && host != nullptr);
+  Tensor& T = *t->p;
+  TB_EXPECTS(n == T.nelems, "host buffer length must equal the stored element count");
+  T.require_allocated();
+  Ctx& c = *T.ctx;
+  TB_CUDA(cudaSetDevice(c.device));
+  if(!c.h2d) TB_CUDA(cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking));
+  if(T.used) TB_CUDA(cudaStreamWaitEvent(c.h2d, T.used, 0));
+  TB_CUDA(cudaMemcpyAsync(T.data, host, sizeof(double) * n, cudaMemcpyHostToDevice, c.h2d));
+  if(!T.filled) TB_CUDA(cudaEventCreateWithFlags(&T.filled, cudaEventDisableTiming));
+  TB_CUDA(cudaEventRecord(T.filled, c.h2d));
+  TB_CUDA(cudaStreamWaitEvent(c.stream, T.filled, 0));
+  TB_API_END
+}
+
+int tb_tensor_read_async(tb_tensor t, double* host, int64_t n) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && host != nullptr);
+  Tensor& T = *t->p;
+  TB_EXPECTS(n == T.nelems, "host buffer length must equal the stored element count");
+  T.require_allocated();
+  Ctx& c = *T.ctx;
+  TB_CUDA(cudaSetDevice(c.device));
+  if(!c.d2h) TB_CUDA(cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking));
+  if(!T.used) { // nothing computed on it yet: order after everything enqueued so far
+    TB_CUDA(cudaEventCreateWithFlags(&T.used, cudaEventDisableTiming));
+    TB_CUDA(cudaEventRecord(T.used, c.stream));
+  }
+  TB_CUDA(cudaStreamWaitEvent(c.d2h, T.used, 0));
+  if(T.filled) TB_CUDA(cudaStreamWaitEvent(c.d2h, T.filled, 0));
+  TB_CUDA(cudaMemcpyAsync(host, T.data, sizeof(double) * n, cudaMemcpyDeviceToHost, c.d2h));
+  TB_API_END
+}
+
 int tb_tensor_norm(tb_tensor t, double* out) {
   TB_API_BEGIN
   REQUIRE_ARG(t != nullptr && out != nullptr);
@@ -838,6 +898,34 @@ int tb_sched_execute(tb_sched s, int hw, int profile) {
   TB_EXPECTS(hw >= 0 && hw <= 2, "hw must be 0 (DEFAULT), 1 (CPU) or 2 (GPU)");
   s->p->execute(profile != 0);
   TB_CUDA(cudaStreamSynchronize(s->p->ctx->stream));
+  TB_API_END
+}
+
+int tb_sched_execute_async(tb_sched s) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  s->p->deferred_checks = true;
+  try {
+    s->p->execute(false);
+  } catch(...) {
+    s->p->deferred_checks = false;
+    throw;
+  }
+  s->p->deferred_checks = false;
+  TB_API_END
+}
+
+int tb_sched_wait(tb_sched s) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  Ctx& c = *s->p->ctx;
+  TB_CUDA(cudaSetDevice(c.device));
+  TB_CUDA(cudaStreamSynchronize(c.stream));
+  if(c.h2d) TB_CUDA(cudaStreamSynchronize(c.h2d));
+  if(c.d2h) TB_CUDA(cudaStreamSynchronize(c.d2h));
+  auto pending = std::move(s->p->pending);
+  s->p->pending.clear();
+  for(const auto& wl: pending) check_int8_errors(*wl, c.stream);
   TB_API_END
 }
 

@@ -115,9 +115,29 @@ Ctx::~Ctx() {
   if(stream) {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
+    for(cudaStream_t x: {h2d, d2h})
+      if(x) {
+        cudaStreamSynchronize(x);
+        cudaStreamDestroy(x);
+      }
     arena.reset();
     cudaStreamDestroy(stream);
   }
+}
+
+Tensor::~Tensor() {
+  if(used || filled) {
+    if(ctx) cudaSetDevice(ctx->device);
+    if(used) cudaEventDestroy(used);
+    if(filled) cudaEventDestroy(filled);
+  }
+}
+
+// marks the end of the compute work enqueued so far that touched t
+static void mark_used(Tensor* t, cudaStream_t st) {
+  if(!t || !t->data) return;
+  if(!t->used) TB_CUDA(cudaEventCreateWithFlags(&t->used, cudaEventDisableTiming));
+  TB_CUDA(cudaEventRecord(t->used, st));
 }
 
 // ------------------------------------------------------------------ index spaces
@@ -649,7 +669,7 @@ void Sched::run(Op& op) {
   }
   op.plan->profile      = profiling;
   op.plan->pinned       = pinned;
-  op.plan->check_errors = pinned == nullptr;
+  op.plan->check_errors = pinned == nullptr && !deferred_checks;
   op.flops              = op.wl->flops;
   run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
                ctx->arena.get());
@@ -810,6 +830,9 @@ void Sched::execute(bool profile) {
   for(size_t i = start; i < ops.size(); i++) {
     if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start)], ctx->stream));
     run(ops[i]);
+    if(ops[i].kind == Op::Mult && deferred_checks && ops[i].wl) pending.push_back(ops[i].wl);
+    if(!pinned) // (a captured graph orders its own ops)
+      for(Tensor* t: {ops[i].lhs.t, ops[i].a.t, ops[i].b.t}) mark_used(t, ctx->stream);
     if(profile) {
       TB_CUDA(cudaEventRecord(ev[2 * (i - start) + 1], ctx->stream));
       prof_stats.push_back(ops[i].kind == Op::Mult && ops[i].plan ? ops[i].plan->last : tb_stats{});

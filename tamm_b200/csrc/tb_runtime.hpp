@@ -41,7 +41,8 @@ private:
 
 struct Ctx {
   int                    device = 0;
-  cudaStream_t           stream = nullptr;
+  cudaStream_t           stream = nullptr;          // compute
+  cudaStream_t           h2d = nullptr, d2h = nullptr; // asynchronous host transfers (created on first use)
   std::unique_ptr<Arena> arena;
   int                    mode       = TB_MODE_FP64;
   double                 err_target = 1e-11;
@@ -91,6 +92,9 @@ struct Tensor {
   std::shared_ptr<Ctx>              ctx;
   double*                           data   = nullptr;
   bool                              owns   = true; // false: storage attached by the caller
+  cudaEvent_t                       used   = nullptr; // end of the last compute op that touched it
+  cudaEvent_t                       filled = nullptr; // end of the last asynchronous host write
+  ~Tensor();
 
   void    build_table(); // Distribution_NW (distribution.hpp:201-243)
   bool    is_non_zero(const int64_t* blockid) const;
@@ -175,6 +179,8 @@ struct Sched {
   int                                               rank = 0, nranks = 1; // owner-computes share of Mult ops
   std::map<std::string, TuneChoice>                 tune_cache;
   CapturePool*                                      pinned = nullptr; // set while capturing a graph
+  bool                                              deferred_checks = false; // execute_async
+  std::vector<std::shared_ptr<WorkList>>            pending;         // INT8 lists to check at wait()
   void                                              execute(bool profile);
   void                                              run(Op& op);
   void                                              tune(Op& op, const std::string& key);

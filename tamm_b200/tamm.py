@@ -61,6 +61,11 @@ class ExecutionContext:
         call("tb_ctx_stream", self.h, C.byref(s))
         return s.value
 
+    def join(self):
+        """Later compute-stream work waits for the copy streams (tb_ctx_join)."""
+        call("tb_ctx_join", self.h)
+        return self
+
     def synchronize(self):
         call("tb_ctx_synchronize", self.h)
 
@@ -237,6 +242,16 @@ class Tensor:
     def deallocate(self):
         call("tb_tensor_deallocate", self.h)
         self.ec = None
+
+    def write_async(self, host_ptr: int):
+        """Asynchronous copy of the packed store from pinned host memory at host_ptr."""
+        call("tb_tensor_write_async", self.h, C.cast(host_ptr, A.dp), self.nelems)
+        return self
+
+    def read_async(self, host_ptr: int):
+        """Asynchronous copy of the packed store into pinned host memory at host_ptr."""
+        call("tb_tensor_read_async", self.h, C.cast(host_ptr, A.dp), self.nelems)
+        return self
 
     def save(self, path: str):
         """Checkpoint (TAMM's write_to_disk element order, raw file)."""
@@ -476,6 +491,15 @@ class Scheduler:
 
     def execute(self, hw=ExecutionHW.DEFAULT, profile=False):
         call("tb_sched_execute", self.h, int(hw), int(bool(profile)))
+        return self
+
+    def execute_async(self):
+        """Enqueue the queued ops without waiting (see tb_sched_execute_async)."""
+        call("tb_sched_execute_async", self.h)
+        return self
+
+    def wait(self):
+        call("tb_sched_wait", self.h)
         return self
 
     def profile(self):
