@@ -183,6 +183,11 @@ int tb_ctx_synchronize(tb_ctx ctx); /* compute and copy streams */
 /* Makes later work on the compute stream wait for everything enqueued so far on the
  * context's copy streams (e.g. to time transfers with events on the compute stream). */
 int tb_ctx_join(tb_ctx ctx);
+/* Sub-allocation from the context's stream-ordered arena (TAMM's RMM pool,
+ * rmm_memory_pool.hpp:50-263): 256-byte aligned device memory, reusable by any
+ * later work on the context's stream as soon as it is freed. */
+int tb_ctx_alloc(tb_ctx ctx, int64_t bytes, void** out);
+int tb_ctx_free(tb_ctx ctx, void* p);
 /* Arena occupancy: bytes in use, high-water mark, capacity. */
 int tb_ctx_arena_info(tb_ctx ctx, int64_t* used, int64_t* peak, int64_t* capacity);
 

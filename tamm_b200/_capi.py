@@ -111,6 +111,8 @@ PROTOS = {
     "tb_tensor_attach": [h, h, vp, C.c_int64],
     "tb_tensor_save": [h, C.c_char_p],
     "tb_ctx_join": [h],
+    "tb_ctx_alloc": [h, C.c_int64, C.POINTER(vp)],
+    "tb_ctx_free": [h, vp],
     "tb_tensor_write_async": [h, dp, C.c_int64],
     "tb_tensor_read_async": [h, dp, C.c_int64],
     "tb_sched_execute_async": [h],

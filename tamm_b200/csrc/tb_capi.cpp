@@ -334,6 +334,21 @@ int tb_ctx_synchronize(tb_ctx ctx) {
   TB_API_END
 }
 
+int tb_ctx_alloc(tb_ctx ctx, int64_t bytes, void** out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(ctx != nullptr && out != nullptr);
+  TB_EXPECTS(bytes >= 0, "negative allocation size");
+  *out = ctx->p->arena->allocate(std::max<int64_t>(bytes, 1));
+  TB_API_END
+}
+
+int tb_ctx_free(tb_ctx ctx, void* p) {
+  TB_API_BEGIN
+  REQUIRE_ARG(ctx != nullptr);
+  if(p) ctx->p->arena->deallocate(p);
+  TB_API_END
+}
+
 int tb_ctx_join(tb_ctx ctx) {
   TB_API_BEGIN
   REQUIRE_ARG(ctx != nullptr);

@@ -61,6 +61,16 @@ class ExecutionContext:
         call("tb_ctx_stream", self.h, C.byref(s))
         return s.value
 
+    def alloc(self, nbytes: int) -> int:
+        """Device memory from the context's arena (256-byte aligned); returns the address."""
+        p = A.vp()
+        call("tb_ctx_alloc", self.h, int(nbytes), C.byref(p))
+        return p.value
+
+    def free(self, ptr: int):
+        call("tb_ctx_free", self.h, C.c_void_p(ptr))
+        return self
+
     def join(self):
         """Later compute-stream work waits for the copy streams (tb_ctx_join)."""
         call("tb_ctx_join", self.h)
