@@ -369,7 +369,7 @@ def main():
         peak = measured_peak(torch, "fp64")
         achieved = lad.flops / (st["gemm_ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_contract_fp64 (DMMA m8n8k4)",
+                "traffic": None, "kernel": "k_contract_fp64 (DMMA m16n8k8)",
                 "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU; "
                                "MEASURED_PEAKS.json has no FP64 figure"}
     if world > 1:

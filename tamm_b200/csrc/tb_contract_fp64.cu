@@ -1,4 +1,4 @@
-// Grouped FP64 block contraction on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64).
+// Grouped FP64 block contraction on the FP64 tensor cores (DMMA, mma.sync m16n8k8 f64).
 //
 // One launch runs a whole MultOp::execute_bufacc (src/tamm/multop.hpp:576-893): every
 // CTA owns one 128x64 tile of one output block (a "group") and loops over the
@@ -7,7 +7,7 @@
 // registers.  Operands are gathered straight from the block store with the label
 // permutation folded into per-row / per-k offset tables (no Ainter/Binter copies as in
 // kernels::block_multiply's transpose_inputs, multiply.hpp:159-194), staged through a
-// 3-deep cp.async pipeline, and the result is written once into C in C's own label
+// 4-deep cp.async pipeline, and the result is written once into C in C's own label
 // order (transpose_output, multiply.hpp:196-210, fused into the epilogue).
 #include "tb_internal.hpp"
 
@@ -16,9 +16,13 @@
 namespace tb {
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, NSLOT = STAGES + 1, NTHREADS = 256;
-constexpr int AS_LD = BK + 4; // padded row strides (doubles) against bank conflicts
-constexpr int BS_LD = BN + 4;
+constexpr int BM = 128, BN = 64, BK = 32, STAGES = 2, NSLOT = STAGES + 1, NTHREADS = 256;
+
+// Shared-memory tiles are stored unpadded with the column XOR-swizzled by the row's two
+// low bits (in units of 4 doubles), so that the DMMA fragment loads (8 rows x 4 columns per
+// half warp) hit 16 distinct bank pairs.  Dropping the padding lets 4 stages fit at 2 CTAs
+// per SM.
+__device__ __forceinline__ int swz(int row, int col) { return col ^ ((row & 3) << 2); }
 
 struct TaskInfo {
   int64_t a_blk, b_blk; // block offset + batch offset, elements
@@ -36,8 +40,8 @@ struct ChunkDesc {
 };
 
 struct Smem {
-  double    As[STAGES][BM][AS_LD];
-  double    Bs[STAGES][BK][BS_LD];
+  double    As[STAGES][BM][BK]; // [m][k ^ swz]
+  double    Bs[STAGES][BK][BN]; // [k][n ^ swz]
   int32_t   rowA[2][BM];
   int32_t   colB[2][BN];
   int32_t   rowC[BM];
@@ -58,9 +62,8 @@ struct Params {
   int             is_assign;
 };
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int bytes) {
-  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void* gmem, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gmem), "r"(bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template<int N>
@@ -68,10 +71,14 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
+// D(16x8) += A(16x8) * B(8x8) in FP64.  Fragments (g = lane / 4, t = lane % 4):
+// a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]}, b = {B[t][g], B[t+4][g]},
+// c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+               "{%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // Row-major strides of a block with `n` modes.
@@ -228,51 +235,76 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
     }
   };
 
+  // Per-thread constants of the gather.  With K contiguous in an operand each thread
+  // keeps one k column and walks rows; otherwise it keeps one row (column) and walks k,
+  // so that consecutive threads read consecutive addresses either way.  The row / column
+  // / k offset tables hold 0 past the block's edge, so every source address stays inside
+  // the task's block; out-of-range elements are zero-filled (source size 0).
+  const bool     a_kfast = lc.a_contig == 1, b_kfast = lc.b_contig == 1;
+  const int      a_fix = a_kfast ? tid % BK : tid % BM, a_walk0 = a_kfast ? tid / BK : tid / BM;
+  const int      b_fix = b_kfast ? tid % BK : tid % BN, b_walk0 = b_kfast ? tid / BK : tid / BN;
+  const int      m_lim = Mtot - it.m0, n_lim = Ntot - it.n0;
+  const uint32_t sA0   = static_cast<uint32_t>(__cvta_generic_to_shared(&s.As[0][0][0]));
+  const uint32_t sB0   = static_cast<uint32_t>(__cvta_generic_to_shared(&s.Bs[0][0][0]));
+
   auto issue = [&](int q) {
     const ChunkDesc& d = s.desc[q % NSLOT];
     if(!d.valid) return;
-    const int stage = q % STAGES, buf = d.buf;
-    const double* Ab = p.A + d.a_base;
-    const double* Bb = p.B + d.b_base;
+    const int      stage = q % STAGES, buf = d.buf, kvalid = d.kvalid;
+    const uint32_t sA    = sA0 + stage * (BM * BK * 8), sB = sB0 + stage * (BK * BN * 8);
+    constexpr int  EA = (BM * BK) / NTHREADS, EB = (BK * BN) / NTHREADS;
+    if(a_kfast) { // thread: k = a_fix, rows a_walk0 + e * (NTHREADS / BK)
+      const bool    kok = a_fix < kvalid;
+      const double* src = p.A + d.a_base + d.kA[a_fix];
 #pragma unroll
-    for(int e = 0; e < (BM * BK) / NTHREADS; e++) {
-      int m, kk;
-      if(lc.a_contig == 1) {
-        kk = tid % BK;
-        m  = tid / BK + e * (NTHREADS / BK);
+      for(int e = 0; e < EA; e++) {
+        const int  m  = a_walk0 + e * (NTHREADS / BK);
+        const bool ok = kok && m < m_lim;
+        cp_async8(sA + (m * BK + swz(m, a_fix)) * 8, src + s.rowA[buf][m], ok ? 8 : 0);
       }
-      else {
-        m  = tid % BM;
-        kk = tid / BM + e * (NTHREADS / BM);
-      }
-      const bool ok = (it.m0 + m < Mtot) && (kk < d.kvalid);
-      cp_async8(&s.As[stage][m][kk], ok ? (const void*) (Ab + s.rowA[buf][m] + d.kA[kk]) : (const void*) p.A,
-                ok ? 8 : 0);
     }
+    else { // thread: row = a_fix, k = a_walk0 + e * (NTHREADS / BM)
+      const bool    mok = a_fix < m_lim;
+      const double* src = p.A + d.a_base + s.rowA[buf][a_fix];
 #pragma unroll
-    for(int e = 0; e < (BK * BN) / NTHREADS; e++) {
-      int n, kk;
-      if(lc.b_contig == 1) {
-        kk = tid % BK;
-        n  = tid / BK + e * (NTHREADS / BK);
+      for(int e = 0; e < EA; e++) {
+        const int  kk = a_walk0 + e * (NTHREADS / BM);
+        const bool ok = mok && kk < kvalid;
+        cp_async8(sA + (a_fix * BK + swz(a_fix, kk)) * 8, src + d.kA[kk], ok ? 8 : 0);
       }
-      else {
-        n  = tid % BN;
-        kk = tid / BN + e * (NTHREADS / BN);
+    }
+    if(b_kfast) { // thread: k = b_fix, columns b_walk0 + e * (NTHREADS / BK)
+      const bool    kok = b_fix < kvalid;
+      const double* src = p.B + d.b_base + d.kB[b_fix];
+#pragma unroll
+      for(int e = 0; e < EB; e++) {
+        const int  n  = b_walk0 + e * (NTHREADS / BK);
+        const bool ok = kok && n < n_lim;
+        cp_async8(sB + (b_fix * BN + swz(b_fix, n)) * 8, src + s.colB[buf][n], ok ? 8 : 0);
       }
-      const bool ok = (it.n0 + n < Ntot) && (kk < d.kvalid);
-      cp_async8(&s.Bs[stage][kk][n], ok ? (const void*) (Bb + d.kB[kk] + s.colB[buf][n]) : (const void*) p.B,
-                ok ? 8 : 0);
+    }
+    else { // thread: column = b_fix, k = b_walk0 + e * (NTHREADS / BN)
+      const bool    nok = b_fix < n_lim;
+      const double* src = p.B + d.b_base + s.colB[buf][b_fix];
+#pragma unroll
+      for(int e = 0; e < EB; e++) {
+        const int  kk = b_walk0 + e * (NTHREADS / BN);
+        const bool ok = nok && kk < kvalid;
+        cp_async8(sB + (kk * BN + swz(kk, b_fix)) * 8, src + d.kB[kk], ok ? 8 : 0);
+      }
     }
   };
 
-  const int warp = tid >> 5, lane = tid & 31;
+  // each warp owns a 32x32 piece of the tile: 2 (m16) x 4 (n8) DMMA tiles
+  const int warp = tid >> 5, lane = tid & 31, lg = lane >> 2, lt = lane & 3;
   const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
-  double    acc[4][4][2];
+  double    acc[2][4][4];
 #pragma unroll
-  for(int i = 0; i < 4; i++)
+  for(int i = 0; i < 2; i++)
 #pragma unroll
-    for(int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for(int j = 0; j < 4; j++)
+#pragma unroll
+      for(int h = 0; h < 4; h++) acc[i][j][h] = 0.0;
 
   // ---- prologue: chunks 0..STAGES-2 in flight, chunk STAGES-1 prepared ----
   prepare(0);
@@ -297,44 +329,55 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
     prepare(q + STAGES);
     if(scale_acc) { // beta chaining of A-only x B-only reduction steps (gemm_wrapper)
 #pragma unroll
-      for(int i = 0; i < 4; i++)
+      for(int i = 0; i < 2; i++)
 #pragma unroll
-        for(int j = 0; j < 4; j++) {
-          acc[i][j][0] *= p.beta;
-          acc[i][j][1] *= p.beta;
-        }
+        for(int j = 0; j < 4; j++)
+#pragma unroll
+          for(int h = 0; h < 4; h++) acc[i][j][h] *= p.beta;
     }
     const int stage = q % STAGES;
 #pragma unroll
-    for(int k4 = 0; k4 < BK; k4 += 4) {
-      double a[4], b[4];
+    for(int k8 = 0; k8 < BK; k8 += 8) {
+      double a[2][4], b[4][2];
 #pragma unroll
-      for(int i = 0; i < 4; i++) a[i] = s.As[stage][wm + 8 * i + (lane >> 2)][k4 + (lane & 3)];
+      for(int i = 0; i < 2; i++) {
+        const int r = wm + 16 * i + lg;
+        a[i][0]     = s.As[stage][r][swz(r, k8 + lt)];
+        a[i][1]     = s.As[stage][r + 8][swz(r, k8 + lt)];
+        a[i][2]     = s.As[stage][r][swz(r, k8 + lt + 4)];
+        a[i][3]     = s.As[stage][r + 8][swz(r, k8 + lt + 4)];
+      }
 #pragma unroll
-      for(int j = 0; j < 4; j++) b[j] = s.Bs[stage][k4 + (lane & 3)][wn + 8 * j + (lane >> 2)];
+      for(int j = 0; j < 4; j++) {
+        b[j][0] = s.Bs[stage][k8 + lt][swz(lt, wn + 8 * j + lg)];
+        b[j][1] = s.Bs[stage][k8 + lt + 4][swz(lt, wn + 8 * j + lg)];
+      }
 #pragma unroll
-      for(int i = 0; i < 4; i++)
+      for(int i = 0; i < 2; i++)
 #pragma unroll
-        for(int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for(int j = 0; j < 4; j++) dmma16(acc[i][j], a[i], b[j]);
     }
   }
   cp_async_wait<0>();
 
   // ---- epilogue: C (=|+=) alpha * acc in C's own layout ----
 #pragma unroll
-  for(int i = 0; i < 4; i++) {
-    const int m = wm + 8 * i + (lane >> 2);
-    if(it.m0 + m >= Mtot) continue;
-    const int64_t rbase = c_base + s.rowC[m];
+  for(int i = 0; i < 2; i++) {
 #pragma unroll
-    for(int j = 0; j < 4; j++) {
+    for(int hr = 0; hr < 2; hr++) {
+      const int m = wm + 16 * i + 8 * hr + lg;
+      if(it.m0 + m >= Mtot) continue;
+      const int64_t rbase = c_base + s.rowC[m];
 #pragma unroll
-      for(int h = 0; h < 2; h++) {
-        const int n = wn + 8 * j + 2 * (lane & 3) + h;
-        if(it.n0 + n >= Ntot) continue;
-        double*      cp = p.C + rbase + s.colC[n];
-        const double v  = p.alpha * acc[i][j][h];
-        *cp             = p.is_assign ? v : *cp + v;
+      for(int j = 0; j < 4; j++) {
+#pragma unroll
+        for(int h = 0; h < 2; h++) {
+          const int n = wn + 8 * j + 2 * lt + h;
+          if(it.n0 + n >= Ntot) continue;
+          double*      cp = p.C + rbase + s.colC[n];
+          const double v  = p.alpha * acc[i][j][2 * hr + h];
+          *cp             = p.is_assign ? v : *cp + v;
+        }
       }
     }
   }
