@@ -385,9 +385,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
 
 } // namespace
 
+static void build_items_fp64(const LabelClasses& lc, const WorkList& wl);
+
 void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,
                           int is_assign, const double* A, const double* B, double* C,
                           cudaStream_t stream) {
+  if(!wl.items_built) build_items_fp64(plan.lc, wl);
   if(wl.items_fp64.empty()) return;
   Params p;
   p.lc        = plan.lc;
@@ -416,20 +419,15 @@ void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, do
 }
 
 // Work items of the FP64 kernel: one per (group, batch index, 128-row tile, 64-col
-// tile), longest first so the hardware block scheduler balances uneven groups.
-void build_items_fp64(const LabelClasses& lc, WorkList& wl) {
-  struct Cost {
-    int64_t cost;
-    DevItem item;
-  };
-  std::vector<Cost> v;
+// tile), longest group first so the hardware block scheduler balances uneven groups
+// (every tile of a group costs the same, so ordering the groups orders the tiles).
+static void build_items_fp64(const LabelClasses& lc, const WorkList& wl) {
+  std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
+  order.reserve(wl.groups.size());
+  int64_t nitems = 0;
   for(size_t gi = 0; gi < wl.groups.size(); gi++) {
     const DevGroup& g = wl.groups[gi];
     if(g.task_begin == g.task_end) continue;
-    int64_t nbatch = 1, M = 1, N = 1;
-    for(int j = 0; j < lc.nbatch; j++) nbatch *= g.cdims[lc.batch_c[j]];
-    for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
-    for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
     int64_t work = 0;
     for(int t = g.task_begin; t < g.task_end; t++) {
       const DevTask& tk = wl.tasks[t];
@@ -439,14 +437,37 @@ void build_items_fp64(const LabelClasses& lc, WorkList& wl) {
       for(int j = 0; j < lc.nbr; j++) k *= tk.bdims[lc.br_b[j]];
       work += (k + BK - 1) / BK;
     }
+    order.emplace_back(work, (int32_t) gi);
+  }
+  std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  auto extents = [&](const DevGroup& g, int64_t& nbatch, int64_t& M, int64_t& N) {
+    nbatch = M = N = 1;
+    for(int j = 0; j < lc.nbatch; j++) nbatch *= g.cdims[lc.batch_c[j]];
+    for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
+    for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
+  };
+  for(const auto& o: order) {
+    int64_t nbatch, M, N;
+    extents(wl.groups[o.second], nbatch, M, N);
+    nitems += nbatch * ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  }
+  TB_EXPECTS(nitems < (1ll << 31), "work list too large");
+  wl.items_fp64.clear();
+  wl.items_fp64.reserve((size_t) nitems);
+  for(const auto& o: order) {
+    int64_t nbatch, M, N;
+    extents(wl.groups[o.second], nbatch, M, N);
     for(int64_t b = 0; b < nbatch; b++)
       for(int64_t m0 = 0; m0 < M; m0 += BM)
         for(int64_t n0 = 0; n0 < N; n0 += BN)
-          v.push_back({work, DevItem{(int32_t) gi, (int32_t) b, (int32_t) m0, (int32_t) n0}});
+          wl.items_fp64.push_back(DevItem{o.second, (int32_t) b, (int32_t) m0, (int32_t) n0});
   }
-  std::stable_sort(v.begin(), v.end(), [](const Cost& a, const Cost& b) { return a.cost > b.cost; });
-  wl.items_fp64.resize(v.size());
-  for(size_t i = 0; i < v.size(); i++) wl.items_fp64[i] = v[i].item;
+  if(!wl.items_fp64.empty()) {
+    TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&wl.d_items), sizeof(DevItem) * wl.items_fp64.size()));
+    TB_CUDA(cudaMemcpy(wl.d_items, wl.items_fp64.data(), sizeof(DevItem) * wl.items_fp64.size(),
+                       cudaMemcpyHostToDevice));
+  }
+  wl.items_built = true;
 }
 
 } // namespace tb

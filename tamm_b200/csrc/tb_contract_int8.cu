@@ -820,28 +820,35 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   L->a_nexp      = aexp;
   L->nexp        = aexp + bexp;
   auto chunks    = [](const std::vector<SplitBlock>& bl, std::vector<int2>& out) {
+    size_t n = 0;
+    for(const auto& b: bl) n += (size_t) b.rows_pad / 8;
+    out.reserve(n);
     for(size_t i = 0; i < bl.size(); i++)
       for(int r = 0; r < bl[i].rows_pad; r += 8) out.push_back(make_int2((int) i, r));
   };
   chunks(L->a_blocks, L->a_chunks);
   chunks(L->b_blocks, L->b_chunks);
-  // output tiles, longest first
-  std::vector<std::pair<int64_t, I8Item>> v;
+  // output tiles, longest group first (every tile of a group costs the same, so
+  // ordering the groups orders the tiles)
+  std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
   for(size_t gi = 0; gi < wl.groups.size(); gi++) {
     const DevGroup& g = wl.groups[gi];
     if(g.task_begin == g.task_end) continue;
-    int64_t M = 1, N = 1, work = 0;
+    int64_t work = 0;
+    for(int t = g.task_begin; t < g.task_end; t++) work += L->tasks[t].nkc;
+    order.emplace_back(work, (int32_t) gi);
+  }
+  std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  for(const auto& o: order) {
+    const DevGroup& g = wl.groups[o.second];
+    int64_t         M = 1, N = 1;
     for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
     for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
-    for(int t = g.task_begin; t < g.task_end; t++) work += L->tasks[t].nkc;
-    for(int64_t mt = 0; mt < (M + MT - 1) / MT; mt++)
-      for(int64_t nt = 0; nt < (N + L->NT - 1) / L->NT; nt++) {
-        v.push_back({work, I8Item{(int32_t) gi, (int32_t) mt, (int32_t) nt, 0}});
-        L->int8_ops += 2.0 * MT * L->NT * kstep * work * (S * (S + 1) / 2);
-      }
+    const int64_t mts = (M + MT - 1) / MT, nts = (N + L->NT - 1) / L->NT;
+    for(int64_t mt = 0; mt < mts; mt++)
+      for(int64_t nt = 0; nt < nts; nt++) L->items.push_back(I8Item{o.second, (int32_t) mt, (int32_t) nt, 0});
+    L->int8_ops += 2.0 * MT * L->NT * kstep * o.first * (S * (S + 1) / 2) * (double) (mts * nts);
   }
-  std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-  for(auto& x: v) L->items.push_back(x.second);
   TB_CUDA(cudaGetDevice(&L->device));
   auto up = [](auto*& dptr, const auto& vec) {
     using T = std::remove_reference_t<decltype(vec[0])>;

@@ -81,12 +81,15 @@ struct DevItem {
 struct WorkList {
   std::vector<DevGroup> groups;
   std::vector<DevTask>  tasks;
-  std::vector<DevItem>  items_fp64; // tile items for the FP64 kernel
   double                flops = 0;
   DevGroup*             d_groups = nullptr;
   DevTask*              d_tasks  = nullptr;
-  DevItem*              d_items  = nullptr;
   int                   device   = -1;
+  // tile items of the FP64 kernel, built (and uploaded) on its first launch over this
+  // work list: contractions that run split-INT8 or BF16x3 never need them
+  mutable std::vector<DevItem> items_fp64;
+  mutable DevItem*             d_items     = nullptr;
+  mutable bool                 items_built = false;
   ~WorkList();
 };
 

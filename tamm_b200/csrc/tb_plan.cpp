@@ -9,7 +9,6 @@
 
 namespace tb {
 
-void build_items_fp64(const LabelClasses& lc, WorkList& wl); // tb_contract_fp64.cu
 
 namespace {
 thread_local std::string g_last_error;
@@ -166,7 +165,6 @@ void finalize_worklist(const LabelClasses& lc, WorkList& wl, bool upload) {
       wl.flops += task_flops(lc, g, wl.tasks[t]);
     }
   }
-  build_items_fp64(lc, wl);
   if(!upload) return;
   TB_CUDA(cudaGetDevice(&wl.device));
   auto up = [](auto*& dptr, const auto& vec) {
@@ -177,7 +175,6 @@ void finalize_worklist(const LabelClasses& lc, WorkList& wl, bool upload) {
   };
   up(wl.d_groups, wl.groups);
   up(wl.d_tasks, wl.tasks);
-  up(wl.d_items, wl.items_fp64);
 }
 
 WorkList* single_block_worklist(const LabelClasses& lc, const int64_t* adims, const int64_t* bdims,
