@@ -126,16 +126,41 @@ __device__ __forceinline__ int row_exponent(double mx) {
 // (row r, pair q) converts k = 2q, 2q+1 of an 8-value column.
 template<int S, bool BF>
 __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restrict__ blocks,
-                                                     const int2* __restrict__ chunks, int nchunks,
+                                                     const int32_t* __restrict__ chunk_begin, int nblocks,
+                                                     int nchunks,
                                                      const double* __restrict__ src, uint8_t* __restrict__ dst,
                                                      int32_t* __restrict__ exps, int32_t* __restrict__ blockmax) {
   __shared__ int     s_sh[8];
   __shared__ int32_t s_off[8];
   const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t     bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
+  // Block of chunk c: the last block whose first chunk is <= c (empty blocks skipped).
+  // The next chunk of a CTA is usually a few blocks on, so each lane holds the first
+  // chunk of one of the 32 blocks after the current one, loaded one chunk ahead (the
+  // load is in flight while the current chunk is split); past them, a 32-way search
+  // with one ballot per step keeps chunk_begin[lo] <= c < chunk_begin[hi], the lanes
+  // probing lo + step .. lo + 32 step, of which those at or below c form a prefix.
+  auto probe = [&](int from) {
+    return from + 1 + lane < nblocks ? __ldg(chunk_begin + from + 1 + lane) : 0x7fffffff;
+  };
+  int lo = 0, next_first = probe(0); // chunk_begin[lo] <= c holds for every later c
   for(int c = blockIdx.x; c < nchunks; c += gridDim.x) {
-    const int2       ch = chunks[c];
+    int hi;
+    {
+      const int cnt = __popc(__ballot_sync(0xffffffffu, next_first <= c));
+      lo += cnt;
+      hi = cnt < 32 ? lo + 1 : nblocks; // a failed probe at lo + 1 bounds the block
+    }
+    while(hi - lo > 1) {
+      const int      step = (hi - lo + 31) >> 5, idx = lo + (lane + 1) * step;
+      const unsigned le   = __ballot_sync(0xffffffffu, idx < hi && __ldg(chunk_begin + idx) <= c);
+      const int      cnt  = __popc(le);
+      hi                  = min(hi, lo + (cnt + 1) * step);
+      lo += cnt * step;
+    }
+    const int2       ch = make_int2(lo, 8 * (c - __ldg(chunk_begin + lo)));
     const SplitBlock b  = blocks[ch.x];
+    next_first          = probe(lo);
     {
       const int     row    = ch.y + warp;
       const bool    live   = row < b.rows;
@@ -660,7 +685,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 struct I8Layout {
   int                     S = 0, NT = 0, esize = 1; // digits, output tile width, bytes per digit
   std::vector<SplitBlock> a_blocks, b_blocks;
-  std::vector<int2>       a_chunks, b_chunks;
+  std::vector<int32_t>    a_cbegin, b_cbegin; // first 8-row chunk of each block, then the total
   std::vector<I8Task>     tasks;
   std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
@@ -669,8 +694,8 @@ struct I8Layout {
   double                  int8_ops = 0;
   SplitBlock*             d_ablocks = nullptr;
   SplitBlock*             d_bblocks = nullptr;
-  int2*                   d_achunks = nullptr;
-  int2*                   d_bchunks = nullptr;
+  int32_t*                d_acbegin = nullptr;
+  int32_t*                d_bcbegin = nullptr;
   I8Task*                 d_tasks   = nullptr;
   I8Item*                 d_items   = nullptr;
   I8TaskMeta*             d_meta    = nullptr;
@@ -684,8 +709,8 @@ struct I8Layout {
       cudaSetDevice(device);
       cudaFree(d_ablocks);
       cudaFree(d_bblocks);
-      cudaFree(d_achunks);
-      cudaFree(d_bchunks);
+      cudaFree(d_acbegin);
+      cudaFree(d_bcbegin);
       cudaFree(d_tasks);
       cudaFree(d_items);
       cudaFree(d_meta);
@@ -819,15 +844,17 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   L->slice_bytes = abytes + bbytes;
   L->a_nexp      = aexp;
   L->nexp        = aexp + bexp;
-  auto chunks    = [](const std::vector<SplitBlock>& bl, std::vector<int2>& out) {
-    size_t n = 0;
-    for(const auto& b: bl) n += (size_t) b.rows_pad / 8;
-    out.reserve(n);
-    for(size_t i = 0; i < bl.size(); i++)
-      for(int r = 0; r < bl[i].rows_pad; r += 8) out.push_back(make_int2((int) i, r));
+  auto chunks    = [](const std::vector<SplitBlock>& bl, std::vector<int32_t>& out) {
+    out.resize(bl.size() + 1);
+    int64_t n = 0;
+    for(size_t i = 0; i < bl.size(); i++) {
+      out[i] = (int32_t) n;
+      n += bl[i].rows_pad / 8;
+    }
+    out[bl.size()] = (int32_t) n;
   };
-  chunks(L->a_blocks, L->a_chunks);
-  chunks(L->b_blocks, L->b_chunks);
+  chunks(L->a_blocks, L->a_cbegin);
+  chunks(L->b_blocks, L->b_cbegin);
   // output tiles, longest group first (every tile of a group costs the same, so
   // ordering the groups orders the tiles)
   std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
@@ -858,8 +885,8 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   up(L->d_ablocks, L->a_blocks);
   up(L->d_bblocks, L->b_blocks);
-  up(L->d_achunks, L->a_chunks);
-  up(L->d_bchunks, L->b_chunks);
+  up(L->d_acbegin, L->a_cbegin);
+  up(L->d_bcbegin, L->b_cbegin);
   up(L->d_tasks, L->tasks);
   up(L->d_items, L->items);
   up(L->d_meta, L->meta);
@@ -885,13 +912,15 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
   const int grid_cap = sm_count() * 8;
   // 0x80808080: below every exponent sum, marks blocks without a nonzero row
   TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
-  auto one = [&](const SplitBlock* blocks, const int2* chunks, size_t nchunks, const double* src) {
+  auto one = [&](const SplitBlock* blocks, const int32_t* cbegin, const std::vector<int32_t>& hbegin,
+                 const double* src) {
+    const int nblocks = (int) hbegin.size() - 1, nchunks = hbegin.back();
     if(nchunks == 0) return;
-    const int grid = (int) std::min<int64_t>((int64_t) nchunks, grid_cap);
-    k_split_fused<S, BF><<<grid, 256, 0, st>>>(blocks, chunks, (int) nchunks, src, slices, exps, L.d_blockmax);
+    const int grid = std::min(nchunks, grid_cap);
+    k_split_fused<S, BF><<<grid, 256, 0, st>>>(blocks, cbegin, nblocks, nchunks, src, slices, exps, L.d_blockmax);
   };
-  one(L.d_ablocks, L.d_achunks, L.a_chunks.size(), A);
-  one(L.d_bblocks, L.d_bchunks, L.b_chunks.size(), B);
+  one(L.d_ablocks, L.d_acbegin, L.a_cbegin, A);
+  one(L.d_bblocks, L.d_bcbegin, L.b_cbegin, B);
   const int ng = (int) wl.groups.size();
   if constexpr(BF) { // both bf16 pieces in every task
     if(!L.tasks.empty()) TB_CUDA(cudaMemsetAsync(L.d_tslices, S, L.tasks.size(), st));
@@ -1134,9 +1163,10 @@ __global__ void k_noalloc_setup(NoAllocDesc d, unsigned char* base) {
   }
   I8Item* items = reinterpret_cast<I8Item*>(base + kCtlItems);
   for(int i = tid; i < d.mtiles * d.ntiles; i += nth) items[i] = I8Item{0, i / d.ntiles, i % d.ntiles, 0};
-  int2* chunks = reinterpret_cast<int2*>(base + d.chunks_off);
-  for(int i = tid; i < d.nchunk_a + d.nchunk_b; i += nth)
-    chunks[i] = i < d.nchunk_a ? make_int2(0, 8 * i) : make_int2(1, 8 * (i - d.nchunk_a));
+  if(tid == 0) { // one block per operand: first chunk 0, then the chunk count
+    int32_t* cb = reinterpret_cast<int32_t*>(base + d.chunks_off);
+    cb[0] = 0, cb[1] = d.nchunk_a, cb[2] = 0, cb[3] = d.nchunk_b;
+  }
 }
 
 template<int S>
@@ -1148,15 +1178,15 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   DevGroup*     grp  = reinterpret_cast<DevGroup*>(sb + 2);
   I8Task*       tsk  = reinterpret_cast<I8Task*>(grp + 1);
   I8TaskMeta*   meta = reinterpret_cast<I8TaskMeta*>(tsk + 1);
-  int2*         ch   = reinterpret_cast<int2*>(base + d.chunks_off);
+  const int32_t* cb  = reinterpret_cast<const int32_t*>(base + d.chunks_off);
   int32_t*      bmax = reinterpret_cast<int32_t*>(base + kCtlBlockMax);
   uint8_t*      tsl  = base + kCtlSlices;
   int32_t*      exps = reinterpret_cast<int32_t*>(base + exps_off);
   uint8_t*      sl   = base + slices_off;
   k_noalloc_setup<<<8, 256, 0, st>>>(d, base);
   const int cap = sm_count() * 8;
-  k_split_fused<S, false><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, ch, d.nchunk_a, A, sl, exps, bmax);
-  k_split_fused<S, false><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb, ch + d.nchunk_a, d.nchunk_b, B, sl, exps, bmax);
+  k_split_fused<S, false><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, cb, 1, d.nchunk_a, A, sl, exps, bmax);
+  k_split_fused<S, false><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb + 1, cb + 2, 1, d.nchunk_b, B, sl, exps, bmax);
   k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
   I8Params p{};
   p.slices  = sl;
@@ -1243,7 +1273,7 @@ extern "C" int tb_block_multiply_int8_noalloc(double alpha, const double* a, con
     const int64_t abytes = S * Mp * Kp, bbytes = S * Np * Kp;
     const int64_t mtiles = Mp / MT, ntiles = Np / NT;
     const int64_t chunks_off = rup(kCtlItems + 16 * mtiles * ntiles, 256);
-    const int64_t exps_off   = rup(chunks_off + 8 * (Mp / 8 + Np / 8), 256);
+    const int64_t exps_off   = rup(chunks_off + 16, 256);
     const int64_t sl_off     = rup(exps_off + 4 * (Mp + Np), 256);
     const int64_t need       = sl_off + abytes + bbytes;
     if(need > kNoAllocBytes)
