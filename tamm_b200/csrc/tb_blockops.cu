@@ -333,59 +333,129 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
   return h;
 }
 
+// 1/D by Newton-Raphson refinement of the hardware approximation rcp.approx.ftz.f64:
+// each step x <- x + x (1 - D x) squares the relative error (quadratic convergence), so
+// two steps take the approximation's error e to e^4, below double rounding; the result
+// is within a unit or two in the last place of the correctly rounded 1/D.  D must be a
+// normal, nonzero double (denormals are flushed to zero).
+__device__ __forceinline__ double recip_nr(double D) {
+  double x;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(D));
+  double e = fma(-D, x, 1.0);
+  x        = fma(x, e, x);
+  e        = fma(-D, x, 1.0);
+  return fma(x, e, x);
+}
+
 // Orbital-energy denominators over the admitted blocks of a tensor: for element
 // (x_0, ..., x_last) of a block, D = sum_m s_m * eps[first_m + x_m].  The work is
-// cut into units of up to 256 rows of one block (a row: all modes but the last), one
-// CTA per unit: each thread forms the row part of D for one row into shared memory
-// (the last mode's part is tabulated once per unit), then the CTA streams the unit's
-// elements with coalesced loads.
-//   ENERGY:  part[unit] = sum w^2 / D  (w = t; deterministic, summed by
-//            k_denom_energy_final)
+// cut into units of consecutive rows of one block (a row: all modes but the last;
+// up to kDenRows rows, about kDenomUnitElems elements), and a persistent grid walks
+// the units: the CTA forms the row part of D for each of the unit's rows in shared
+// memory (the last mode's part is tabulated once per unit), then streams the unit's
+// elements with coalesced loads, eight in flight per thread.  A last mode of at most
+// kThreads columns gives each thread one fixed column (its part of D in a register)
+// and floor(kThreads / columns) rows per pass; a longer one steps (row, column)
+// through the unit without divisions.
+//   ENERGY:  part[cta] = sum w^2 / D  (w = t; each CTA sums its units in a fixed
+//            order, k_denom_energy_final sums the CTAs in a fixed order)
 //   update:  t += scale * r / D
 constexpr int kDenCols = 1024; // last-mode extents tabulated in shared memory
+constexpr int kDenRows = kDenomUnitRows; // rows of one unit (row parts of D in shared memory)
 
 template<bool ENERGY>
 __global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, const double* __restrict__ r, double scale,
                                                     const DenomBlock* __restrict__ blocks,
-                                                    const DenomUnit* __restrict__ units, int nmodes,
+                                                    const DenomUnit* __restrict__ units, int nunits, int nmodes,
                                                     const double* __restrict__ eps, DenomSigns sg,
                                                     double* __restrict__ part) {
-  __shared__ double drow[kThreads];
+  __shared__ double drow[kDenRows];
   __shared__ double dcol[kDenCols];
-  const DenomUnit   u    = units[blockIdx.x];
-  const DenomBlock  b    = blocks[u.block];
+  constexpr int     U    = 8; // loads in flight per thread
+  const int         tid  = threadIdx.x;
   const int         last = nmodes - 1;
-  const int64_t     ncol = b.dims[last];
-  int64_t           nrow = 1;
-  for(int m = 0; m < last; m++) nrow *= b.dims[m];
-  const int     tid = threadIdx.x;
-  const bool    tab = ncol <= kDenCols;
-  const double* el  = eps + b.first[last];
-  if(tab)
-    for(int64_t c = tid; c < ncol; c += kThreads) dcol[c] = sg.s[last] * __ldg(el + c);
-  const int64_t rows = nrow - u.r0 < kThreads ? nrow - u.r0 : kThreads;
-  if(tid < rows) {
-    int64_t x = u.r0 + tid;
-    double  d = 0.0;
-    for(int m = last - 1; m >= 0; m--) {
-      const int64_t q = x / b.dims[m];
-      d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * b.dims[m]));
-      x = q;
+  double            s    = 0.0;
+  // one element: its value(s) and its denominator
+  auto elem = [&](int64_t i, double v, double w, double D) {
+    if constexpr(ENERGY) s += v * v * recip_nr(D);
+    else t[i] = v + scale * w * recip_nr(D);
+  };
+  auto load = [&](int64_t i, double& v, double& w) {
+    if constexpr(ENERGY) v = __ldg(t + i);
+    else {
+      v = t[i];
+      w = __ldg(r + i);
     }
-    drow[tid] = d;
-  }
-  __syncthreads();
-  const int32_t nel = (int32_t) (rows * ncol), nc = (int32_t) ncol;
-  const int64_t base = b.off + u.r0 * ncol;
-  double        s    = 0.0;
-  for(int32_t e = tid; e < nel; e += kThreads) {
-    const int32_t rr = e / nc, cc = e - rr * nc;
-    const double  D  = drow[rr] + (tab ? dcol[cc] : sg.s[last] * __ldg(el + cc));
-    if constexpr(ENERGY) {
-      const double v = t[base + e];
-      s += v * v / D;
+  };
+  for(int ui = blockIdx.x; ui < nunits; ui += gridDim.x) {
+    const DenomUnit  u    = units[ui];
+    const DenomBlock b    = blocks[u.block];
+    const int32_t    nc   = (int32_t) b.dims[last];
+    const bool       tab  = nc <= kDenCols;
+    const double*    el   = eps + b.first[last];
+    const double     slst = sg.s[last];
+    __syncthreads(); // the previous unit is done with drow / dcol
+    if(tab)
+      for(int c = tid; c < nc; c += kThreads) dcol[c] = slst * __ldg(el + c);
+    for(int i = tid; i < u.rows; i += kThreads) {
+      int32_t x = (int32_t) (u.r0 + i); // a block holds fewer than 2^31 elements
+      double  d = 0.0;
+      for(int m = last - 1; m >= 0; m--) {
+        const int32_t n = (int32_t) b.dims[m], q = x / n;
+        d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * n));
+        x = q;
+      }
+      drow[i] = d;
     }
-    else t[base + e] += scale * r[base + e] / D;
+    __syncthreads();
+    const int64_t base = b.off + u.r0 * (int64_t) nc;
+    if(nc <= kThreads) { // fixed column per thread, P rows per pass of A elements
+      const int P = kThreads / nc, A = P * nc;
+      if(tid < A) {
+        const int     ro = tid / nc;
+        const double  dc = dcol[tid - ro * nc];
+        const int     nk = (u.rows - ro + P - 1) / P; // rows ro, ro + P, ... of the unit
+        const int64_t e0 = base + tid;
+        int           k  = 0;
+        for(; k + U <= nk; k += U) {
+          double v[U], w[U];
+#pragma unroll
+          for(int j = 0; j < U; j++) load(e0 + (int64_t) (k + j) * A, v[j], w[j]);
+#pragma unroll
+          for(int j = 0; j < U; j++) elem(e0 + (int64_t) (k + j) * A, v[j], w[j], drow[ro + (k + j) * P] + dc);
+        }
+        for(; k < nk; k++) {
+          double v, w;
+          load(e0 + (int64_t) k * A, v, w);
+          elem(e0 + (int64_t) k * A, v, w, drow[ro + k * P] + dc);
+        }
+      }
+    }
+    else { // long rows: step (row, column) by kThreads elements, no divisions
+      const int32_t nel = u.rows * nc;
+      int32_t       rr = 0, cc = tid, e = tid;
+      auto          den = [&]() {
+        const double D = drow[rr] + (tab ? dcol[cc] : slst * __ldg(el + cc));
+        cc += kThreads;
+        if(cc >= nc) {
+          cc -= nc;
+          rr++;
+        }
+        return D;
+      };
+      for(; e + (U - 1) * kThreads < nel; e += U * kThreads) {
+        double v[U], w[U];
+#pragma unroll
+        for(int j = 0; j < U; j++) load(base + e + j * kThreads, v[j], w[j]);
+#pragma unroll
+        for(int j = 0; j < U; j++) elem(base + e + j * kThreads, v[j], w[j], den());
+      }
+      for(; e < nel; e += kThreads) {
+        double v, w;
+        load(base + e, v, w);
+        elem(base + e, v, w, den());
+      }
+    }
   }
   if constexpr(ENERGY) {
 #pragma unroll
@@ -399,6 +469,23 @@ __global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, cons
       part[blockIdx.x] = v;
     }
   }
+}
+
+// Persistent grid of the denominator kernels: as many CTAs as fit on the GPU at once,
+// at most one per unit.
+template<bool ENERGY>
+int denom_grid(int nunits) {
+  static int per_sm[64] = {0};
+  int        dev        = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  int& k = per_sm[dev < 64 ? dev : 63];
+  if(k == 0) {
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, k_denom<ENERGY>, kThreads, 0));
+    k = std::max(k, 1);
+  }
+  int nsm = 0;
+  TB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  return std::min(nunits, nsm * k);
 }
 
 __global__ void k_denom_energy_final(const double* __restrict__ part, int np, double scale, double* __restrict__ out) {
@@ -421,10 +508,11 @@ __global__ void k_set_scalar(double* out, double v) { *out = v; }
 void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks, const DenomUnit* units,
                          int nunits, int nmodes, const double* eps, DenomSigns signs, double* part, double* out,
                          cudaStream_t stream) {
-  if(nunits > 0)
-    k_denom<true><<<nunits, kThreads, 0, stream>>>(const_cast<double*>(w), nullptr, 0.0, blocks, units, nmodes, eps,
-                                                   signs, part);
-  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, nunits, scale, out);
+  const int grid = nunits > 0 ? denom_grid<true>(nunits) : 0;
+  if(grid > 0)
+    k_denom<true><<<grid, kThreads, 0, stream>>>(const_cast<double*>(w), nullptr, 0.0, blocks, units, nunits, nmodes,
+                                                 eps, signs, part);
+  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, grid, scale, out);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -447,7 +535,8 @@ void launch_dot_to(const double* x, const double* y, int64_t n, double scale, in
 void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, const DenomUnit* units,
                   int nunits, int nmodes, const double* eps, DenomSigns signs, cudaStream_t stream) {
   if(nunits <= 0) return;
-  k_denom<false><<<nunits, kThreads, 0, stream>>>(t, r, scale, blocks, units, nmodes, eps, signs, nullptr);
+  k_denom<false><<<denom_grid<false>(nunits), kThreads, 0, stream>>>(t, r, scale, blocks, units, nunits, nmodes, eps,
+                                                                    signs, nullptr);
   TB_CUDA(cudaGetLastError());
 }
 

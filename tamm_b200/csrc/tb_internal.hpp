@@ -164,11 +164,14 @@ struct DenomBlock {
 struct DenomSigns {
   double s[kMaxModes];
 };
-// A unit of denominator work: up to 256 consecutive rows of one block.
+// A unit of denominator work: `rows` consecutive rows (all modes but the last) of one
+// block, from row r0.
 struct DenomUnit {
-  int32_t block, pad;
+  int32_t block, rows;
   int64_t r0;
 };
+constexpr int kDenomUnitRows  = 2048;  // at most, so that the row parts fit in shared memory
+constexpr int kDenomUnitElems = 16384; // about, per unit
 void launch_denom(double* t, const double* r, double scale, const DenomBlock* blocks, const DenomUnit* units,
                   int nunits, int nmodes, const double* eps, DenomSigns signs, cudaStream_t stream);
 // *out += scale * sum w^2 / D over the blocks (part: nunits doubles of scratch).

@@ -777,7 +777,11 @@ void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c) {
   for(size_t bi = 0; bi < blocks.size(); bi++) {
     int64_t nrow = 1;
     for(int m = 0; m + 1 < T.nmodes; m++) nrow *= blocks[bi].dims[m];
-    for(int64_t r0 = 0; r0 < nrow; r0 += 256) units.push_back(DenomUnit{(int32_t) bi, 0, r0});
+    const int64_t ncol = blocks[bi].dims[T.nmodes - 1];
+    const int64_t step = std::min<int64_t>(kDenomUnitRows, std::max<int64_t>(1, kDenomUnitElems / ncol));
+    TB_EXPECTS(step * ncol < (1ll << 31), "denominator unit too large");
+    for(int64_t r0 = 0; r0 < nrow; r0 += step)
+      units.push_back(DenomUnit{(int32_t) bi, (int32_t) std::min(step, nrow - r0), r0});
   }
   TB_EXPECTS(units.size() < (1ull << 31), "too many denominator work units");
   ctx     = c;
