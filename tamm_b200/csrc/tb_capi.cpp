@@ -32,7 +32,7 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
         TB_CUDA(cudaEventCreate(&e0));
         TB_CUDA(cudaEventCreate(&e1));
         TB_CUDA(cudaEventRecord(e0, stream));
-        launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+        launch_contract_fp64(plan, wl, alpha, 1.0, plan.store ? 1 : 0, A, B, C, stream);
         TB_CUDA(cudaEventRecord(e1, stream));
         TB_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
@@ -41,7 +41,7 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
       }
-      else launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+      else launch_contract_fp64(plan, wl, alpha, 1.0, plan.store ? 1 : 0, A, B, C, stream);
       break;
     case TB_MODE_INT8: contract_int8(plan, wl, alpha, A, B, C, stream); break;
     case TB_MODE_BF16X3: contract_bf16x3(plan, wl, alpha, A, B, C, stream); break;

@@ -119,6 +119,11 @@ struct Plan {
   // pool, which keeps it allocated for the graph's replays
   struct CapturePool* pinned = nullptr;
   bool         profile      = false;   // time the phases with CUDA events (synchronises)
+  // C = alpha * A * B instead of C += alpha * A * B on the output blocks of groups with
+  // tasks: the FP64 kernel stores its result without reading C (each element of C
+  // belongs to exactly one output tile); blocks of groups without tasks are left
+  // untouched
+  bool         store        = false;
 };
 
 void forget_int8_layout(const WorkList* wl);

@@ -358,6 +358,14 @@ bool next_tuple(std::vector<int64_t>& it, const std::vector<int64_t>& nt) {
   return false;
 }
 
+// Same tensor, labels and label spaces.
+bool same_target(const Labeled& x, const Labeled& y) {
+  if(x.t != y.t || x.labels != y.labels || x.ltis.size() != y.ltis.size()) return false;
+  for(size_t i = 0; i < x.ltis.size(); i++)
+    if(x.ltis[i].get() != y.ltis[i].get()) return false;
+  return true;
+}
+
 std::string signature(const Op& op) {
   std::ostringstream os;
   auto               put = [&](const Labeled& x) {
@@ -504,6 +512,7 @@ void Sched::run(Op& op) {
   cudaStream_t st = ctx->stream;
   if(op.kind == Op::Set) {
     op.lhs.t->require_allocated();
+    if(op.fill_none) return;
     if(!op.set_blocks) {
       auto blocks = std::make_shared<std::vector<int64_t>>();
       bool whole  = true;
@@ -627,27 +636,12 @@ void Sched::run(Op& op) {
   op.lhs.t->require_allocated();
   op.a.t->require_allocated();
   op.b.t->require_allocated();
-  if(!op.wl) {
-    const std::string sig = signature(op) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks);
-    auto              pit = plan_cache.find(sig);
-    if(pit == plan_cache.end()) {
-      auto plan        = std::make_shared<Plan>();
-      plan->lc         = classify(op.lhs.labels.data(), (int) op.lhs.labels.size(), op.a.labels.data(),
-                                  (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
-      plan->mode       = ctx->mode;
-      plan->err_target = ctx->err_target;
-      plan->nslices    = ctx->nslices;
-      plan_cache[sig]  = plan;
-      wl_cache[sig]    = build_mult_worklist(op, plan->lc, true, rank, nranks);
-      pit              = plan_cache.find(sig);
-    }
-    op.plan = pit->second;
-    op.wl   = wl_cache[sig];
-  }
+  prepare_mult(op);
   op.plan->mode       = ctx->mode;
   op.plan->err_target = ctx->err_target;
   op.plan->nslices    = ctx->nslices;
   op.plan->tile_n     = 0;
+  op.plan->store      = op.store;
   if(autotune && ctx->mode == TB_MODE_INT8 && !pinned) {
     const std::string key = signature(op) + "|" + std::to_string(ctx->err_target) + "|" + std::to_string(ctx->nslices);
     auto              it  = tune_cache.find(key);
@@ -676,6 +670,51 @@ void Sched::run(Op& op) {
   op.plan->profile      = false;
   op.plan->pinned       = nullptr;
   op.plan->check_errors = true;
+  op.plan->store        = false;
+}
+
+// Plan and work list of a MultOp, from the caches (keyed by the op's signature and
+// this rank's share).
+void Sched::prepare_mult(Op& op) {
+  if(op.wl) return;
+  const std::string sig = signature(op) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks);
+  auto              pit = plan_cache.find(sig);
+  if(pit == plan_cache.end()) {
+    auto plan        = std::make_shared<Plan>();
+    plan->lc         = classify(op.lhs.labels.data(), (int) op.lhs.labels.size(), op.a.labels.data(),
+                                (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
+    plan->mode       = ctx->mode;
+    plan->err_target = ctx->err_target;
+    plan->nslices    = ctx->nslices;
+    plan_cache[sig]  = plan;
+    wl_cache[sig]    = build_mult_worklist(op, plan->lc, true, rank, nranks);
+    pit              = plan_cache.find(sig);
+  }
+  op.plan = pit->second;
+  op.wl   = wl_cache[sig];
+}
+
+// Assignment C = alpha * A * B, queued as Set(0) + Mult (MultOp::canonicalize,
+// multop.hpp:255-269), on one rank under an FP64 request: the FP64 kernel stores its
+// result into the output blocks of groups with tasks (every element of those blocks is
+// written once), and the Set zeroes only the blocks of groups without tasks.  Saves
+// the fill of C and the read of every C element.  (The split kernels keep the fill
+// and their one atomic add per element: plain stores from their epilogue measured
+// slower on large outputs.)
+void Sched::fuse_assign(Op& set, Op& mult) {
+  prepare_mult(mult);
+  mult.store = true;
+  if(set.set_blocks) return; // decided when this op first ran
+  auto blocks = std::make_shared<std::vector<int64_t>>();
+  for(const auto& g: mult.wl->groups) {
+    if(g.task_begin != g.task_end) continue;
+    int64_t n = 1;
+    for(int i = 0; i < mult.lhs.t->nmodes; i++) n *= g.cdims[i];
+    blocks->push_back(g.c_off);
+    blocks->push_back(n);
+  }
+  set.fill_none  = blocks->empty();
+  set.set_blocks = blocks;
 }
 
 // Autotuner: each candidate (the FP64 kernel, the split-INT8 kernel at output tile
@@ -833,6 +872,11 @@ void Sched::execute(bool profile) {
   }
   for(size_t i = start; i < ops.size(); i++) {
     if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start)], ctx->stream));
+    if(nranks == 1 && ctx->mode == TB_MODE_FP64 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
+       ops[i].is_assign && ops[i].value == 0.0 &&
+       ops[i + 1].kind == Op::Mult && same_target(ops[i].lhs, ops[i + 1].lhs) &&
+       ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t) // C read as an operand needs the fill
+      fuse_assign(ops[i], ops[i + 1]);
     run(ops[i]);
     if(ops[i].kind == Op::Mult && deferred_checks && ops[i].wl) pending.push_back(ops[i].wl);
     if(!pinned) // (a captured graph orders its own ops)

@@ -138,6 +138,10 @@ struct Op {
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
   bool                                   flat = false;
   std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
+  // an assignment C = alpha * A * B queued as Set(0) + Mult runs fused on one rank in
+  // FP64: the Mult stores its result (store), the Set zeroes only the output blocks the
+  // Mult's work list leaves without tasks (fill_none: there are none)
+  bool                                   store = false, fill_none = false;
   double                                 flops = 0;
 };
 
@@ -183,6 +187,8 @@ struct Sched {
   std::vector<std::shared_ptr<WorkList>>            pending;         // INT8 lists to check at wait()
   void                                              execute(bool profile);
   void                                              run(Op& op);
+  void                                              prepare_mult(Op& op);
+  void                                              fuse_assign(Op& set, Op& mult);
   void                                              tune(Op& op, const std::string& key);
   double*                                           scalars();
   ~Sched();
