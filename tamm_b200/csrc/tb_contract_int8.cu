@@ -345,6 +345,7 @@ struct I8Params {
   int*            err;
   const uint8_t*  tslices; // digit count of each task (1..S)
   int*            ctr;     // next output tile to hand out (zero at launch)
+  int             xpose;   // C is contiguous along the tile's columns: transposed reductions
 };
 
 template<int S, int NT>
@@ -361,9 +362,19 @@ __host__ __device__ constexpr int stages() {
   return (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) < 6 ? (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) : 6;
 }
 
+// Epilogue transpose buffer behind the tail, where it fits: per epilogue warp kXCols
+// columns x 32 rows of doubles, rows kXStride apart (34: the transposed reads of a half
+// warp, 8 columns x 2 rows, fall on 16 distinct bank pairs).
+constexpr int kXCols = 8, kXStride = 34;
+constexpr int kXBytes = (NEPI / 32) * kXCols * kXStride * 8;
+template<int S, int NT>
+__host__ __device__ constexpr bool xpose_fits() {
+  return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail + kXBytes <= kMaxSmem;
+}
+
 template<int S, int NT>
 constexpr size_t smem_bytes() {
-  return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail;
+  return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail + (xpose_fits<S, NT>() ? kXBytes : 0);
 }
 
 // BF: the BF16x3 mode (S = 2 bf16 pieces, kind::f16 MMAs with FP32 accumulators; both
@@ -661,7 +672,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       if(!ok) break;
       // C (+)= alpha * result: one reduction per element (c + alpha * r, rounded once,
       // as a load-add-store would be; every element of C belongs to exactly one output
-      // tile), performed at L2, so the epilogue does not wait for C's memory
+      // tile), performed at L2, so the epilogue does not wait for C's memory.
+      // A thread holds one row of the tile; when C is contiguous along the columns
+      // instead, the warp passes its values through shared memory kXCols columns at a
+      // time so that each reduction instruction covers 4 rows x 8 adjacent columns.
+      if constexpr(xpose_fits<S, NT>()) {
+        if(p.xpose) {
+          static_assert(NH % kXCols == 0, "tile half width must be a multiple of the transpose width");
+          double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * kXCols * kXStride;
+          const int rsub = lane / kXCols, csub = lane % kXCols;
+#pragma unroll
+          for(int x0 = 0; x0 < NH; x0 += kXCols) {
+#pragma unroll
+            for(int j = 0; j < kXCols; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
+            __syncwarp();
+            const int o = nof[col0 + x0 + csub];
+#pragma unroll
+            for(int it = 0; it < kXCols; it++) { // rows it * 4 + rsub
+              const int     r  = it * (32 / kXCols) + rsub;
+              const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
+              if(ro >= 0 && o >= 0) atomicAdd(p.C + ro + o, xb[csub * kXStride + r]);
+            }
+            __syncwarp(); // the next columns overwrite the buffer
+          }
+          continue;
+        }
+      }
       if(rowoff >= 0) {
         double* crow = p.C + rowoff;
 #pragma unroll
@@ -947,6 +983,8 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   p.err     = L.d_err;
   p.tslices = L.d_tslices;
   p.ctr     = L.d_ctr;
+  // transposed reductions when C's last mode (stride 1) is a column label of the tile
+  p.xpose = xpose_fits<S, NT>() && lc.nn > 0 && lc.n_c[lc.nn - 1] == lc.nc - 1 ? 1 : 0;
   TB_CUDA(cudaMemsetAsync(L.d_ctr, 0, sizeof(int), st));
   const size_t smem = smem_bytes<S, NT>();
   static bool  configured[64] = {false};
