@@ -106,8 +106,9 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return e;
 }
 
-// Split in one pass over HBM: one CTA per 8-row group.  Phase 1, warp w streams row w
-// (16-byte loads from the row's first 16-byte boundary, four in flight per lane) for
+// Split in one pass over HBM: persistent CTAs, each taking 8-row groups ("chunks") in
+// turn.  Phase 1, warp w streams row w
+// (16-byte loads from the row's first 16-byte boundary, eight in flight per lane) for
 // its max |x| and row exponent; phase 2 re-reads the 8 rows, now resident in L2, one
 // 8-row x 16-k core matrix per warp and step: thread (row r, quad q) turns k =
 // 4q..4q+3 into Y = round(x * 2^(8S-1-e)) + 0x80..80, whose plain base-256 bytes are
@@ -116,7 +117,7 @@ __device__ __forceinline__ int row_exponent(double mx) {
 // contiguous 128-byte core matrix.
 // Slice layout per 32-byte K chunk of a tile: [K half (16 bytes)][digit][row][16 bytes],
 // i.e. the S digits' core matrices of one K half follow each other, so that the digits
-// j0..j1 of a B tile form one UMMA operand of (j1 - j0 + 1) x NT rows.  Residency (four CTAs per SM at 60 registers)
+// j0..j1 of a B tile form one UMMA operand of (j1 - j0 + 1) x NT rows.  Residency (four CTAs per SM at 64 registers)
 // bounds the rows held in L2 between the phases to 4 x 148 x 8 rows (87 MB at K =
 // 2304, within the 126 MB L2).
 //

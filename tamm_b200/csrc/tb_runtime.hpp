@@ -152,8 +152,9 @@ struct DenomSpec {
   double                  signs[kMaxModes] = {0};
   double*                 d_eps    = nullptr;
   DenomBlock*             d_blocks = nullptr;
-  DenomUnit*              d_units  = nullptr; // 256-row work units
-  double*                 d_part   = nullptr; // per-unit partial sums (energy reduction)
+  DenomUnit*              d_units  = nullptr; // row work units (kDenomUnitRows / kDenomUnitElems)
+  double*                 d_part   = nullptr; // per-CTA partial sums of the energy reduction
+                                              // (nunits entries: the grid is never larger)
   int                     nblocks  = 0, nunits = 0;
   void                    build(const Tensor& t, const std::shared_ptr<Ctx>& ctx);
   std::shared_ptr<Ctx>    ctx;
