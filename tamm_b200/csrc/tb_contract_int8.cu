@@ -114,7 +114,8 @@ __device__ __forceinline__ int row_exponent(double mx) {
 // 4q..4q+3 into Y = round(x * 2^(8S-1-e)) + 0x80..80, whose plain base-256 bytes are
 // the balanced digits + 128.  The bytes of 4 values are gathered per slice with PRMT,
 // flipped back with one XOR and stored as one 4-byte word, so every warp store is a
-// contiguous 128-byte core matrix.
+// contiguous 128-byte core matrix.  Phase 2's re-reads and the digit stores are marked
+// evict-first (streaming), so that the rows still waiting for their phase 2 keep L2.
 // Slice layout per 32-byte K chunk of a tile: [K half (16 bytes)][digit][row][16 bytes],
 // i.e. the S digits' core matrices of one K half follow each other, so that the digits
 // j0..j1 of a B tile form one UMMA operand of (j1 - j0 + 1) x NT rows.  Residency (four CTAs per SM at 64 registers)
@@ -224,12 +225,12 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
         const int k0 = k8 * 8 + q * 2;
         double    v[2];
         if(vec && k0 + 1 < b.K) {
-          const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
+          const double2 v01 = __ldcs(reinterpret_cast<const double2*>(s + k0));
           v[0] = v01.x, v[1] = v01.y;
         }
         else
 #pragma unroll
-          for(int x = 0; x < 2; x++) v[x] = (live && k0 + x < b.K) ? __ldg(s + koff(b, k0 + x)) : 0.0;
+          for(int x = 0; x < 2; x++) v[x] = (live && k0 + x < b.K) ? __ldcs(s + koff(b, k0 + x)) : 0.0;
         uint32_t hi = 0, lo = 0;
 #pragma unroll
         for(int x = 0; x < 2; x++) {
@@ -240,8 +241,8 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
           lo |= (uint32_t) __bfloat16_as_ushort(t) << (16 * x);
         }
         uint8_t* o = out + (int64_t) (k8 >> 1) * S * b.tile_rows * KC + (k8 & 1) * S * b.tile_rows * 16;
-        *reinterpret_cast<uint32_t*>(o)                      = hi;
-        *reinterpret_cast<uint32_t*>(o + b.tile_rows * 16) = lo;
+        __stcs(reinterpret_cast<unsigned int*>(o), hi);
+        __stcs(reinterpret_cast<unsigned int*>(o + b.tile_rows * 16), lo);
       }
     }
     else {
@@ -255,15 +256,15 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
       auto load4 = [&](int k16, double (&v)[4]) {
         const int k0 = k16 * 16 + q * 4;
         if(vec && k0 + 3 < b.K) {
-          const double2 v01 = __ldg(reinterpret_cast<const double2*>(s + k0));
-          const double2 v23 = __ldg(reinterpret_cast<const double2*>(s + k0 + 2));
+          const double2 v01 = __ldcs(reinterpret_cast<const double2*>(s + k0));
+          const double2 v23 = __ldcs(reinterpret_cast<const double2*>(s + k0 + 2));
           v[0] = v01.x, v[1] = v01.y, v[2] = v23.x, v[3] = v23.y;
         }
         else
 #pragma unroll
           for(int x = 0; x < 4; x++) {
             const int k = k0 + x;
-            v[x]        = (live && k < b.K) ? __ldg(s + koff(b, k)) : 0.0;
+            v[x]        = (live && k < b.K) ? __ldcs(s + koff(b, k)) : 0.0;
           }
       };
       auto emit = [&](int k16, const double (&v)[4]) {
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
             const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
             w                 = __byte_perm(t0, t1, 0x5410);
           }
-          *reinterpret_cast<uint32_t*>(o + (int64_t) i * b.tile_rows * 16) = w ^ 0x80808080u;
+          __stcs(reinterpret_cast<unsigned int*>(o + (int64_t) i * b.tile_rows * 16), w ^ 0x80808080u);
         }
       };
       const int n16 = b.K_pad / 16;
