@@ -313,6 +313,40 @@ void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t
   TB_CUDA(cudaGetLastError());
 }
 
+// SetOp over a list of blocks in one launch: blocks (offset, element count) pairs in
+// device memory; CTA (x, y) fills blocks y, y + gridDim.y, ... with gridDim.x CTAs per
+// block, two elements per thread and step (16-byte stores where aligned).
+__global__ void __launch_bounds__(kThreads) k_fill_blocks(double* __restrict__ x, const int64_t* __restrict__ pairs,
+                                                          int nblocks, double v, int is_assign) {
+  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
+    double* const xb     = x + pairs[2 * blk];
+    const int64_t n      = pairs[2 * blk + 1];
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 2;
+    for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
+      if(i + 1 < n && ((reinterpret_cast<uintptr_t>(xb + i) & 15) == 0)) {
+        double2 d;
+        if(is_assign) d = make_double2(v, v);
+        else {
+          d = *reinterpret_cast<double2*>(xb + i);
+          d.x += v;
+          d.y += v;
+        }
+        *reinterpret_cast<double2*>(xb + i) = d;
+      }
+      else
+        for(int64_t j = i; j < i + 2 && j < n; j++) xb[j] = is_assign ? v : xb[j] + v;
+    }
+  }
+}
+
+void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double value, int is_assign,
+                        cudaStream_t stream) {
+  if(nblocks <= 0) return;
+  const dim3 grid(4, (unsigned) std::min(nblocks, 2048));
+  k_fill_blocks<<<grid, kThreads, 0, stream>>>(x, pairs, nblocks, value, is_assign);
+  TB_CUDA(cudaGetLastError());
+}
+
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream) {
   if(n <= 0) return;

@@ -152,6 +152,9 @@ AssignLoop plan_assign(const int64_t* ddims, const int* dlabels, int nd, const i
 void launch_assign(const AssignLoop& lp, double* dst, double scale, const double* src,
                    int is_assign, cudaStream_t stream);
 void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream);
+// x[off .. off + n) (=|+=) value for each (off, n) pair of a device array
+void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double value, int is_assign,
+                        cudaStream_t stream);
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream);
 double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream);

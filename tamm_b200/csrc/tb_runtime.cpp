@@ -534,10 +534,25 @@ void Sched::run(Op& op) {
       op.set_blocks = blocks;
     }
     if(op.set_blocks->empty()) launch_fill(op.lhs.t->data, op.lhs.t->nelems, op.value, op.is_assign, st);
-    else
-      for(size_t i = 0; i < op.set_blocks->size(); i += 2)
-        launch_fill(op.lhs.t->data + (*op.set_blocks)[i], (*op.set_blocks)[i + 1], op.value,
-                    op.is_assign, st);
+    else {
+      const size_t nb = op.set_blocks->size() / 2;
+      TB_EXPECTS(nb < (1u << 31), "too many blocks in one fill");
+      if(!op.set_dev) { // one list upload per op; a captured graph replays the same list
+        int64_t*  d   = nullptr;
+        const int dev = ctx->device;
+        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * op.set_blocks->size()));
+        op.set_dev = std::shared_ptr<int64_t>(d, [dev](int64_t* p) {
+          int cur = -1;
+          cudaGetDevice(&cur);
+          cudaSetDevice(dev);
+          cudaFree(p);
+          if(cur >= 0) cudaSetDevice(cur);
+        });
+        TB_CUDA(cudaMemcpy(d, op.set_blocks->data(), sizeof(int64_t) * op.set_blocks->size(),
+                           cudaMemcpyHostToDevice));
+      }
+      launch_fill_blocks(op.lhs.t->data, op.set_dev.get(), (int) nb, op.value, op.is_assign, st);
+    }
     return;
   }
   if(op.kind == Op::Add) {

@@ -138,6 +138,7 @@ struct Op {
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
   bool                                   flat = false;
   std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
+  std::shared_ptr<int64_t>               set_dev;    // device copy of set_blocks (uploaded on first use)
   // an assignment C = alpha * A * B queued as Set(0) + Mult runs fused on one rank in
   // FP64: the Mult stores its result (store), the Set zeroes only the output blocks the
   // Mult's work list leaves without tasks (fill_none: there are none)
