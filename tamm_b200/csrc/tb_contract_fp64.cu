@@ -16,7 +16,8 @@
 namespace tb {
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 32, STAGES = 2, NSLOT = STAGES + 1, NTHREADS = 256;
+constexpr int BM = 128, BK = 32, STAGES = 2, NSLOT = STAGES + 1, NTHREADS = 256;
+// output tile width BN: 64, or 80 where that pads the work list's output blocks less
 
 // Shared-memory tiles are stored unpadded with the column XOR-swizzled by the row's two
 // low bits (in units of 4 doubles), so that the DMMA fragment loads (8 rows x 4 columns per
@@ -39,6 +40,7 @@ struct ChunkDesc {
   int32_t kA[BK], kB[BK];
 };
 
+template<int BN>
 struct Smem {
   double    As[STAGES][BM][BK]; // [m][k ^ swz]
   double    Bs[STAGES][BK][BN]; // [k][n ^ swz]
@@ -103,9 +105,10 @@ __device__ __forceinline__ int32_t decompose(int32_t x, int n, const int32_t* di
   return off;
 }
 
+template<int BN>
 __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem&               s   = *reinterpret_cast<Smem*>(smem_raw);
+  Smem<BN>&           s   = *reinterpret_cast<Smem<BN>*>(smem_raw);
   const LabelClasses& lc  = p.lc;
   const int           tid = threadIdx.x;
   const DevItem       it  = p.items[blockIdx.x];
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
         cp_async8(sB + (b_fix * BN + swz(b_fix, n)) * 8, src + s.colB[buf][n], ok ? 8 : 0);
       }
     }
-    else { // thread: column = b_fix, k = b_walk0 + e * (NTHREADS / BN)
+    else if constexpr(NTHREADS % BN == 0) { // thread: column = b_fix, k = b_walk0 + e * (NTHREADS / BN)
       const bool    nok = b_fix < n_lim;
       const double* src = p.B + d.b_base + s.colB[buf][b_fix];
 #pragma unroll
@@ -293,16 +296,32 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
         cp_async8(sB + (kk * BN + swz(kk, b_fix)) * 8, src + d.kB[kk], ok ? 8 : 0);
       }
     }
+    else { // a width that does not divide the thread count: P = NTHREADS / BN rows of BN
+           // columns per pass on the first P * BN threads, each keeping its column
+      constexpr int P = NTHREADS / BN, NE = (BK + P - 1) / P;
+      if(tid < P * BN) {
+        const int     n   = tid % BN, k0 = tid / BN;
+        const bool    nok = n < n_lim;
+        const double* src = p.B + d.b_base + s.colB[buf][n];
+#pragma unroll
+        for(int e = 0; e < NE; e++) {
+          const int kk = k0 + e * P;
+          if(kk < BK) cp_async8(sB + (kk * BN + swz(kk, n)) * 8, src + d.kB[kk], nok && kk < kvalid ? 8 : 0);
+        }
+      }
+    }
   };
 
-  // each warp owns a 32x32 piece of the tile: 2 (m16) x 4 (n8) DMMA tiles
+  // each warp owns a 32 x BN/2 piece of the tile: 2 (m16) x NJ (n8) DMMA tiles
+  constexpr int NJ = BN / 16;
+  static_assert(BN % 16 == 0, "tile width must be a multiple of 16");
   const int warp = tid >> 5, lane = tid & 31, lg = lane >> 2, lt = lane & 3;
-  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
-  double    acc[2][4][4];
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * (BN / 2);
+  double    acc[2][NJ][4];
 #pragma unroll
   for(int i = 0; i < 2; i++)
 #pragma unroll
-    for(int j = 0; j < 4; j++)
+    for(int j = 0; j < NJ; j++)
 #pragma unroll
       for(int h = 0; h < 4; h++) acc[i][j][h] = 0.0;
 
@@ -331,14 +350,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
 #pragma unroll
       for(int i = 0; i < 2; i++)
 #pragma unroll
-        for(int j = 0; j < 4; j++)
+        for(int j = 0; j < NJ; j++)
 #pragma unroll
           for(int h = 0; h < 4; h++) acc[i][j][h] *= p.beta;
     }
     const int stage = q % STAGES;
 #pragma unroll
     for(int k8 = 0; k8 < BK; k8 += 8) {
-      double a[2][4], b[4][2];
+      double a[2][4];
 #pragma unroll
       for(int i = 0; i < 2; i++) {
         const int r = wm + 16 * i + lg;
@@ -348,14 +367,13 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
         a[i][3]     = s.As[stage][r + 8][swz(r, k8 + lt + 4)];
       }
 #pragma unroll
-      for(int j = 0; j < 4; j++) {
-        b[j][0] = s.Bs[stage][k8 + lt][swz(lt, wn + 8 * j + lg)];
-        b[j][1] = s.Bs[stage][k8 + lt + 4][swz(lt, wn + 8 * j + lg)];
+      for(int j = 0; j < NJ; j++) { // one B fragment live at a time
+        double b[2];
+        b[0] = s.Bs[stage][k8 + lt][swz(lt, wn + 8 * j + lg)];
+        b[1] = s.Bs[stage][k8 + lt + 4][swz(lt, wn + 8 * j + lg)];
+        dmma16(acc[0][j], a[0], b);
+        dmma16(acc[1][j], a[1], b);
       }
-#pragma unroll
-      for(int i = 0; i < 2; i++)
-#pragma unroll
-        for(int j = 0; j < 4; j++) dmma16(acc[i][j], a[i], b[j]);
     }
   }
   cp_async_wait<0>();
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
       if(it.m0 + m >= Mtot) continue;
       const int64_t rbase = c_base + s.rowC[m];
 #pragma unroll
-      for(int j = 0; j < 4; j++) {
+      for(int j = 0; j < NJ; j++) {
 #pragma unroll
         for(int h = 0; h < 2; h++) {
           const int n = wn + 8 * j + 2 * lt + h;
@@ -387,6 +405,20 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
 
 static void build_items_fp64(const LabelClasses& lc, const WorkList& wl);
 
+template<int BN>
+static void launch_k(const Params& p, unsigned nitems, cudaStream_t stream) {
+  const size_t smem = sizeof(Smem<BN>);
+  static bool  configured[64] = {false};
+  int          dev            = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  if(dev < 64 && !configured[dev]) {
+    TB_CUDA(cudaFuncSetAttribute(k_contract_fp64<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    configured[dev] = true;
+  }
+  k_contract_fp64<BN><<<nitems, NTHREADS, smem, stream>>>(p);
+  TB_CUDA(cudaGetLastError());
+}
+
 void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, double beta,
                           int is_assign, const double* A, const double* B, double* C,
                           cudaStream_t stream) {
@@ -403,24 +435,17 @@ void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, do
   p.alpha     = alpha;
   p.beta      = beta;
   p.is_assign = is_assign;
-  const size_t smem = sizeof(Smem);
-  static bool  configured[64] = {false};
-  int          dev            = 0;
-  TB_CUDA(cudaGetDevice(&dev));
-  if(dev < 64 && !configured[dev]) {
-    TB_CUDA(cudaFuncSetAttribute(k_contract_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int) smem));
-    configured[dev] = true;
-  }
   const int64_t nitems = (int64_t) wl.items_fp64.size();
   TB_EXPECTS(nitems < (1ll << 31), "work list too large");
-  k_contract_fp64<<<(unsigned) nitems, NTHREADS, smem, stream>>>(p);
-  TB_CUDA(cudaGetLastError());
+  if(wl.items_bn == 80) launch_k<80>(p, (unsigned) nitems, stream);
+  else launch_k<64>(p, (unsigned) nitems, stream);
 }
 
-// Work items of the FP64 kernel: one per (group, batch index, 128-row tile, 64-col
+// Work items of the FP64 kernel: one per (group, batch index, 128-row tile, BN-column
 // tile), longest group first so the hardware block scheduler balances uneven groups
 // (every tile of a group costs the same, so ordering the groups orders the tiles).
+// BN is 80 where that pads the output columns of the work list less than 64 does
+// (N = 400 or 80, say), else 64.
 static void build_items_fp64(const LabelClasses& lc, const WorkList& wl) {
   std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
   order.reserve(wl.groups.size());
@@ -446,6 +471,15 @@ static void build_items_fp64(const LabelClasses& lc, const WorkList& wl) {
     for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
     for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
   };
+  double padded64 = 0, padded80 = 0; // MMA work of each width, tile padding included
+  for(const auto& o: order) {
+    int64_t nbatch, M, N;
+    extents(wl.groups[o.second], nbatch, M, N);
+    const double w = (double) o.first * nbatch * ((M + BM - 1) / BM);
+    padded64 += w * ((N + 63) / 64) * 64;
+    padded80 += w * ((N + 79) / 80) * 80;
+  }
+  const int BN = padded80 < padded64 ? 80 : 64;
   for(const auto& o: order) {
     int64_t nbatch, M, N;
     extents(wl.groups[o.second], nbatch, M, N);
@@ -467,6 +501,7 @@ static void build_items_fp64(const LabelClasses& lc, const WorkList& wl) {
     TB_CUDA(cudaMemcpy(wl.d_items, wl.items_fp64.data(), sizeof(DevItem) * wl.items_fp64.size(),
                        cudaMemcpyHostToDevice));
   }
+  wl.items_bn    = BN;
   wl.items_built = true;
 }
 

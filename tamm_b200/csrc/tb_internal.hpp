@@ -90,6 +90,7 @@ struct WorkList {
   mutable std::vector<DevItem> items_fp64;
   mutable DevItem*             d_items     = nullptr;
   mutable bool                 items_built = false;
+  mutable int                  items_bn    = 64; // output tile width of those items
   ~WorkList();
 };
 
