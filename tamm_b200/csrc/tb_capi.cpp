@@ -1163,6 +1163,7 @@ int tb_sched_release(tb_sched s) {
   s->p->start = s->p->last_first = 0;
   s->p->plan_cache.clear();
   s->p->wl_cache.clear();
+  s->p->fill_cache.clear();
   TB_API_END
 }
 

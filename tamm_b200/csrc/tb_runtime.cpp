@@ -537,19 +537,24 @@ void Sched::run(Op& op) {
     else {
       const size_t nb = op.set_blocks->size() / 2;
       TB_EXPECTS(nb < (1u << 31), "too many blocks in one fill");
-      if(!op.set_dev) { // one list upload per op; a captured graph replays the same list
-        int64_t*  d   = nullptr;
-        const int dev = ctx->device;
-        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * op.set_blocks->size()));
-        op.set_dev = std::shared_ptr<int64_t>(d, [dev](int64_t* p) {
-          int cur = -1;
-          cudaGetDevice(&cur);
-          cudaSetDevice(dev);
-          cudaFree(p);
-          if(cur >= 0) cudaSetDevice(cur);
-        });
-        TB_CUDA(cudaMemcpy(d, op.set_blocks->data(), sizeof(int64_t) * op.set_blocks->size(),
-                           cudaMemcpyHostToDevice));
+      if(!op.set_dev) { // one upload per signature; later ops and graph replays reuse it
+        if(op.fill_key.empty()) op.fill_key = "S|" + signature(op);
+        auto& cached = fill_cache[op.fill_key];
+        if(!cached) {
+          int64_t*  d   = nullptr;
+          const int dev = ctx->device;
+          TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * op.set_blocks->size()));
+          cached = std::shared_ptr<int64_t>(d, [dev](int64_t* p) {
+            int cur = -1;
+            cudaGetDevice(&cur);
+            cudaSetDevice(dev);
+            cudaFree(p);
+            if(cur >= 0) cudaSetDevice(cur);
+          });
+          TB_CUDA(cudaMemcpy(d, op.set_blocks->data(), sizeof(int64_t) * op.set_blocks->size(),
+                             cudaMemcpyHostToDevice));
+        }
+        op.set_dev = cached;
       }
       launch_fill_blocks(op.lhs.t->data, op.set_dev.get(), (int) nb, op.value, op.is_assign, st);
     }
@@ -720,6 +725,7 @@ void Sched::fuse_assign(Op& set, Op& mult) {
   prepare_mult(mult);
   mult.store = true;
   if(set.set_blocks) return; // decided when this op first ran
+  set.fill_key = "F|" + signature(mult) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks);
   auto blocks = std::make_shared<std::vector<int64_t>>();
   for(const auto& g: mult.wl->groups) {
     if(g.task_begin != g.task_end) continue;

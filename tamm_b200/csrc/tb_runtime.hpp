@@ -138,7 +138,8 @@ struct Op {
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
   bool                                   flat = false;
   std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
-  std::shared_ptr<int64_t>               set_dev;    // device copy of set_blocks (uploaded on first use)
+  std::shared_ptr<int64_t>               set_dev;    // device copy of set_blocks (from the scheduler's cache)
+  std::string                            fill_key;   // its key in that cache
   // an assignment C = alpha * A * B queued as Set(0) + Mult runs fused on one rank in
   // FP64: the Mult stores its result (store), the Set zeroes only the output blocks the
   // Mult's work list leaves without tasks (fill_none: there are none)
@@ -179,6 +180,9 @@ struct Sched {
   bool                                              profiling = false;
   std::map<std::string, std::shared_ptr<Plan>>     plan_cache;
   std::map<std::string, std::shared_ptr<WorkList>> wl_cache;
+  // device block lists of SetOps over some of a tensor's blocks, by the op's signature
+  // (or, for the fill of a fused assignment, its contraction's), uploaded once
+  std::map<std::string, std::shared_ptr<int64_t>>  fill_cache;
   static constexpr int                              kSlots = 64;
   double*                                           d_scalars = nullptr; // kSlots + 1024 partials
   bool                                              autotune  = false;
