@@ -2,11 +2,17 @@
 #include "tb_runtime.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <numeric>
 #include <sstream>
 
 namespace tb {
+
+uint64_t next_serial() {
+  static std::atomic<uint64_t> n{0};
+  return ++n;
+}
 
 // ------------------------------------------------------------------------- arena
 
@@ -369,8 +375,9 @@ bool same_target(const Labeled& x, const Labeled& y) {
 std::string signature(const Op& op) {
   std::ostringstream os;
   auto               put = [&](const Labeled& x) {
-    os << x.t << ":";
-    for(size_t i = 0; i < x.labels.size(); i++) os << x.labels[i] << "@" << x.ltis[i].get() << ",";
+    os << x.t << "#" << x.t->serial.v << ":";
+    for(size_t i = 0; i < x.labels.size(); i++)
+      os << x.labels[i] << "@" << x.ltis[i].get() << "#" << x.ltis[i]->serial.v << ",";
     os << "|";
   };
   os << (int) op.kind << "|";

@@ -71,7 +71,19 @@ struct RootTiling {
 
 // A tiled index space: a list of root tiles (all of them for the root space,
 // a subset for named subspaces and tile sub-ranges).
+// Identity of a runtime object for the scheduler's caches: a number no other object
+// of this process has had, so that an object created at the address of a destroyed
+// one never matches the cache entries of its predecessor.  A copy is a new object.
+uint64_t next_serial();
+struct Serial {
+  uint64_t v;
+  Serial() : v(next_serial()) {}
+  Serial(const Serial&) : v(next_serial()) {}
+  Serial& operator=(const Serial&) { return *this; }
+};
+
 struct TIS {
+  Serial                      serial;
   std::shared_ptr<RootTiling> root;
   std::vector<int64_t>        tiles;
   int64_t                     ntiles() const { return (int64_t) tiles.size(); }
@@ -82,6 +94,7 @@ struct TIS {
 };
 
 struct Tensor {
+  Serial                            serial;
   int                               nmodes = 0;
   std::vector<std::shared_ptr<TIS>> tis;
   bool                              has_spin = false;
