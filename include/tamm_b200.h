@@ -96,15 +96,16 @@ int tb_axpby(double alpha, const double* x, double beta, double* y, int64_t n, v
  * allocators (TAMM's RMM pool takes 80% of the free memory at start-up, a caching
  * allocator the rest), or code that must not trigger the device-wide
  * synchronisation cudaMalloc / cudaFree can cause.  It makes no cudaMalloc,
- * cudaMallocAsync, cudaFree or host-heap call: its scratch (digit slices,
- * exponents, the one-task work list) is a file-scope device array of 64 MiB that
- * every GPU loading the library holds until exit.  A triple needing more scratch
+ * cudaMallocAsync or cudaFree call and, when it succeeds, allocates no host memory
+ * either (a failure builds its tb_last_error message string): its scratch (digit
+ * slices, exponents, the one-task work list) is a file-scope device array of 64 MiB
+ * that every GPU loading the library holds until exit.  A triple needing more scratch
  * (about 6 * K * (M + N) bytes at the default 6 digits) is rejected with
  * TB_ERR_INVALID and a message giving the size.  Labels as in tb_block_multiply
  * (plain contractions only: no Hadamard or one-sided reduction labels); nslices 0
  * picks the digit count for a 1e-11 target, 3..8 forces it.  The first call on a
- * device looks up the array's device address once for that device (make it before
- * any stream capture).  Every call reuses the same array and leaves its contents
+ * device looks up the array's device address for that device, once; make that first
+ * call before any stream capture on the device.  Every call reuses the same array and leaves its contents
  * behind; each call resets what it needs to start from a known value, and calls
  * that overlap on the GPU (other streams, other threads) race on the array.  The
  * call returns after the stream has drained. */
@@ -161,6 +162,8 @@ typedef struct tb_stats {
   double gemm_ms;         /* device time of the tensor-core contraction kernel (profiled runs) */
   int    mode;            /* kernel that ran: TB_MODE_FP64 or TB_MODE_INT8 (autotuner's choice) */
   int    tile_n;          /* split-INT8 output tile width (0: the default for the slice count) */
+  double flops_run;       /* FP64 FLOPs of the tasks that ran: admitted minus the tasks skipped
+                             over exactly-zero blocks of read-only operands */
 } tb_stats;
 
 /* C += alpha * sum over tasks of A * B, all groups, one stream-ordered pass.
@@ -232,6 +235,23 @@ int tb_tensor_info(tb_tensor t, int* nmodes, int64_t* nblocks, int64_t* nelems);
 /* Packed block table in storage order: keys and element offsets (nblocks each). */
 int tb_tensor_block_table(tb_tensor t, int64_t* keys, int64_t* offsets);
 int tb_tensor_data(tb_tensor t, double** device_ptr);
+/* Read-only mark (no counterpart in TAMM): on != 0 declares the tensor's contents
+ * constant until the mark is cleared, e.g. the two-electron integrals of a
+ * coupled-cluster iteration.  While it is set, every library call that would write
+ * the tensor fails with TB_ERR_STATE (tb_tensor_put / add / write / write_async /
+ * load, and Set / Add / Mult / denominator ops with it on the left-hand side, at
+ * execute time); writes through the pointer of tb_tensor_data are the caller's to
+ * avoid.  Setting the mark scans the stored blocks once on the device (after the work
+ * already enqueued on the context's stream) for blocks whose elements are all zero
+ * (+0.0 or -0.0).  Contractions then skip every admitted task over such a block: its
+ * product is exactly zero, so the result is the same up to the sign of zero entries
+ * of C (non-finite values in the other operand's block are not propagated through a
+ * skipped task, as with BLAS implementations that skip zero operands).  The skipped
+ * tasks still count in the admitted FLOPs (tb_stats.flops) and not in
+ * tb_stats.flops_run.  Deallocating the tensor clears the mark; on == 0 clears it. */
+int tb_tensor_set_read_only(tb_tensor t, int on);
+/* Whether the mark is set, and how many stored blocks / elements the scan found zero. */
+int tb_tensor_read_only_info(tb_tensor t, int* on, int64_t* zero_blocks, int64_t* zero_elems);
 int tb_tensor_is_non_zero(tb_tensor t, const int64_t* blockid, int* out);
 int tb_tensor_block_size(tb_tensor t, const int64_t* blockid, int64_t* out);
 int tb_tensor_block_dims(tb_tensor t, const int64_t* blockid, int64_t* dims);
@@ -290,7 +310,8 @@ int tb_sched_mult(tb_sched s, tb_labeled lhs, double alpha, tb_labeled a, tb_lab
                   int is_assign);
 /* Work of lhs += a * b without running it: admitted output blocks, admitted
  * (C, A, B) block triples and their FP64 FLOPs, from the same enumeration the
- * MultOp uses (multop.hpp:645-893).  Needs no GPU and no allocation. */
+ * MultOp uses (multop.hpp:645-893).  Needs no GPU and no allocation.  Triples over
+ * zero blocks of read-only operands are counted (they are admitted). */
 int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, int64_t* ntasks,
                  double* flops);
 /* Owner-computes share for one of nranks processes (TAMM's rule, multop.hpp:880-891,

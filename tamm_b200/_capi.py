@@ -35,7 +35,7 @@ h = C.c_void_p  # opaque handles
 class tb_stats(C.Structure):
     _fields_ = [("flops", C.c_double), ("int8_ops", C.c_double), ("slices_min", C.c_int),
                 ("slices_max", C.c_int), ("scratch_bytes", C.c_int64), ("split_ms", C.c_double),
-                ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int)]
+                ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int), ("flops_run", C.c_double)]
 
 
 class tb_labeled(C.Structure):
@@ -87,6 +87,8 @@ PROTOS = {
     "tb_tensor_info": [h, ip, i64p, i64p],
     "tb_tensor_block_table": [h, i64p, i64p],
     "tb_tensor_data": [h, C.POINTER(vp)],
+    "tb_tensor_set_read_only": [h, C.c_int],
+    "tb_tensor_read_only_info": [h, ip, i64p, i64p],
     "tb_tensor_is_non_zero": [h, i64p, ip],
     "tb_tensor_block_size": [h, i64p, i64p],
     "tb_tensor_block_dims": [h, i64p, i64p],

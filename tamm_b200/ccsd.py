@@ -131,6 +131,11 @@ def build(oa: int, va: int, seed: int = 2, tile_lo: int = 20, tile_hi: int = 64,
     base = (buf.data_ptr() + 255) // 256 * 256
     for _, vb in batches:
         vb.attach(ec, base, max(most, 1) * 8)
+    # the integrals and Fock matrices stay constant through the iterations: marked
+    # read-only, their exactly-zero spin blocks (e.g. v(a,b,i,j) with spin(a) != spin(i))
+    # are skipped by the contractions that read them
+    for name in ("L_vo", "L_oo", "L_vv", "f_oo", "f_vv", "v_vvoo", "v_oooo", "v_ovvo"):
+        T[name].set_read_only(True)
     P = CCSDProblem(ec, MO, O, V, CI, eps, T, batches, buf)
     P.flops = iteration_flops(P)
     return P
@@ -212,27 +217,18 @@ def tune_report(sch: Scheduler) -> list:
         x += 1
 
 
-def main(argv=None):
-    """Config of the full doubles iteration: eager and graph-replayed iterations in the
-    plain FP64 and split-INT8 (autotuned) modes; prints one JSON line."""
+def measure(P: CCSDProblem, iters: int = 3, modes=("fp64", "int8")) -> dict:
+    """Eager and graph-replayed iterations in the plain FP64 and split-INT8 (autotuned)
+    modes, timed by CUDA events on the context's stream; t2 is restored before each
+    mode so every mode iterates from the same amplitudes."""
     import torch
-    p = argparse.ArgumentParser()
-    p.add_argument("--oa", type=int, default=30)
-    p.add_argument("--va", type=int, default=240)
-    p.add_argument("--seed", type=int, default=2)
-    p.add_argument("--tile-lo", type=int, default=20)
-    p.add_argument("--tile-hi", type=int, default=64)
-    p.add_argument("--iters", type=int, default=3)
-    p.add_argument("--pool-gib", type=int, default=150)
-    args = p.parse_args(argv)
-    ec = ExecutionContext(0, args.pool_gib << 30)
-    P = build(args.oa, args.va, seed=args.seed, tile_lo=args.tile_lo, tile_hi=args.tile_hi, ec=ec)
+    ec = P.ec
     t2_0 = P.T["t2"].read().copy()
     stream = torch.cuda.ExternalStream(ec.stream)
-    out = {"workload": f"ccsd_doubles_iteration_O{2 * args.oa}_V{2 * args.va}", "flops": P.flops,
-           "ops_per_iteration": len(_ops(P)) + 3, "ladder_batches": len(P.batches)}
-    results = {}
-    for name, mode, tune in (("fp64", Precision.FP64, False), ("int8", Precision.INT8, True)):
+    results, r2s = {}, {}
+    table = {"fp64": (Precision.FP64, False), "int8": (Precision.INT8, True), "bf16x3": (Precision.BF16X3, False)}
+    for name in modes:
+        mode, tune = table[name]
         ec.set_precision(mode, 1e-11)
         P.T["t2"].write(t2_0)
         sch = Scheduler(ec)
@@ -243,7 +239,7 @@ def main(argv=None):
         sch.execute(ExecutionHW.GPU)  # first iteration: plans, work lists, autotuning
         first_s = time.perf_counter() - t0
         e_first, n_first = sch.scalars(2)
-        # eager iterations (host-driven op launches)
+        # eager iteration (host-driven op launches), profiled per op
         P.T["t2"].write(t2_0)
         queue_iteration(P, sch)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -260,16 +256,16 @@ def main(argv=None):
         P.T["t2"].write(t2_0)
         g.launch().sync()
         e_graph, n_graph = sch.scalars(2)
-        r2 = P.T["r2"].read().copy()
+        r2s[name] = P.T["r2"].read().copy()
         e0.record(stream)
-        for _ in range(args.iters):
+        for _ in range(iters):
             g.launch()
         e1.record(stream)
         g.sync()
-        graph_ms = e0.elapsed_time(e1) / args.iters
+        graph_ms = e0.elapsed_time(e1) / iters
         results[name] = {"energy_first": e_first, "residual_norm_first": n_first, "energy_graph": e_graph,
                          "first_iteration_s": first_s, "eager_ms": eager_ms, "graph_ms": graph_ms,
-                         "tflops_graph": P.flops["contractions"] / graph_ms / 1e9}
+                         "graph_replays": iters, "tflops_graph": P.flops["contractions"] / graph_ms / 1e9}
         if tune:
             choices = {}
             for ti in tune_report(sch):
@@ -277,12 +273,36 @@ def main(argv=None):
                     key = "fp64" if ti["mode"] == Precision.FP64 else f"int8_nt{ti['tile_n']}"
                     choices[key] = choices.get(key, 0) + 1
             results[name]["autotune_choices"] = choices
-        results[name]["r2"] = r2
         del g
     ec.set_precision(Precision.FP64)
-    d = results["int8"].pop("r2") - results["fp64"].pop("r2")
-    out.update(results)
-    out["int8_vs_fp64_r2_max_rel_err"] = float(np.max(np.abs(d)) / max(np.max(np.abs(P.T["v_vvoo"].read())), 1e-300))
+    P.T["t2"].write(t2_0)
+    if "fp64" in r2s:
+        scale = max(float(np.max(np.abs(r2s["fp64"]))), 1e-300)
+        for name in r2s:
+            if name != "fp64":
+                results[name]["r2_max_rel_err_vs_fp64"] = float(np.max(np.abs(r2s[name] - r2s["fp64"]))) / scale
+                results[name]["speedup_vs_fp64"] = results["fp64"]["graph_ms"] / results[name]["graph_ms"]
+    return results
+
+
+def main(argv=None):
+    """Config of the full doubles iteration: eager and graph-replayed iterations in the
+    plain FP64 and split-INT8 (autotuned) modes; prints one JSON line."""
+    p = argparse.ArgumentParser()
+    p.add_argument("--oa", type=int, default=30)
+    p.add_argument("--va", type=int, default=240)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--tile-lo", type=int, default=20)
+    p.add_argument("--tile-hi", type=int, default=64)
+    p.add_argument("--iters", type=int, default=3)
+    p.add_argument("--pool-gib", type=int, default=150)
+    p.add_argument("--modes", default="fp64,int8")
+    args = p.parse_args(argv)
+    ec = ExecutionContext(0, args.pool_gib << 30)
+    P = build(args.oa, args.va, seed=args.seed, tile_lo=args.tile_lo, tile_hi=args.tile_hi, ec=ec)
+    out = {"workload": f"ccsd_doubles_iteration_O{2 * args.oa}_V{2 * args.va}", "flops": P.flops,
+           "ops_per_iteration": len(_ops(P)) + 3, "ladder_batches": len(P.batches)}
+    out.update(measure(P, args.iters, tuple(args.modes.split(","))))
     print(json.dumps(out))
 
 

@@ -347,6 +347,37 @@ void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double val
   TB_CUDA(cudaGetLastError());
 }
 
+// One pass over the blocks of a read-only tensor: a CTA row (blockIdx.y) per block,
+// 16-byte loads where aligned, one OR per CTA that saw a nonzero element.
+__global__ void __launch_bounds__(kThreads) k_block_nonzero(const double* __restrict__ x,
+                                                            const int64_t* __restrict__ pairs, int nblocks,
+                                                            uint32_t* __restrict__ nonzero) {
+  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
+    const double* const xb     = x + pairs[2 * blk];
+    const int64_t       n      = pairs[2 * blk + 1];
+    const int64_t       stride = (int64_t) gridDim.x * blockDim.x * 2;
+    int                 any    = 0;
+    for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n && !any; i += stride) {
+      if(i + 1 < n && ((reinterpret_cast<uintptr_t>(xb + i) & 15) == 0)) {
+        const double2 d = __ldcs(reinterpret_cast<const double2*>(xb + i));
+        any             = (d.x != 0.0) | (d.y != 0.0);
+      }
+      else
+        for(int64_t j = i; j < i + 2 && j < n; j++) any |= (xb[j] != 0.0);
+    }
+    if(__syncthreads_or(any) && threadIdx.x == 0) atomicOr(nonzero + blk, 1u);
+  }
+}
+
+void launch_block_nonzero(const double* x, const int64_t* pairs, int nblocks, uint32_t* nonzero,
+                          cudaStream_t stream) {
+  if(nblocks <= 0) return;
+  TB_CUDA(cudaMemsetAsync(nonzero, 0, sizeof(uint32_t) * nblocks, stream));
+  const dim3 grid(16, (unsigned) std::min(nblocks, 4096));
+  k_block_nonzero<<<grid, kThreads, 0, stream>>>(x, pairs, nblocks, nonzero);
+  TB_CUDA(cudaGetLastError());
+}
+
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream) {
   if(n <= 0) return;

@@ -15,13 +15,15 @@ std::shared_ptr<TIS> tis_named(const TIS& parent, const std::string& name);
 std::shared_ptr<TIS> tis_subrange(const TIS& parent, int64_t first, int64_t last);
 std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bool upload, int rank = 0,
                                         int nranks = 1);
+void set_read_only(Tensor& T, bool on);
 
 // Mode dispatch of one grouped contraction.
 void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
                   double* C, cudaStream_t stream, Arena* arena) {
   plan.last          = tb_stats{};
-  plan.last.flops    = wl.flops;
-  plan.last.mode     = plan.mode;
+  plan.last.flops     = wl.flops;
+  plan.last.flops_run = wl.flops_run;
+  plan.last.mode      = plan.mode;
   plan.last.tile_n   = plan.tile_n;
   plan.arena      = arena;
   if(wl.tasks.empty()) return;
@@ -530,6 +532,7 @@ int tb_tensor_deallocate(tb_tensor t) {
   TB_API_BEGIN
   REQUIRE_ARG(t != nullptr);
   if(t->p->data && t->p->ctx && t->p->owns) t->p->ctx->arena->deallocate(t->p->data);
+  set_read_only(*t->p, false);
   t->p->data = nullptr;
   t->p->owns = true;
   t->p->ctx.reset();
@@ -557,6 +560,29 @@ int tb_tensor_block_table(tb_tensor t, int64_t* keys, int64_t* offsets) {
   REQUIRE_ARG(t != nullptr);
   if(keys) std::copy(t->p->keys.begin(), t->p->keys.end(), keys);
   if(offsets) std::copy(t->p->offsets.begin(), t->p->offsets.end(), offsets);
+  TB_API_END
+}
+
+int tb_tensor_set_read_only(tb_tensor t, int on) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr);
+  set_read_only(*t->p, on != 0);
+  TB_API_END
+}
+
+int tb_tensor_read_only_info(tb_tensor t, int* on, int64_t* zero_blocks, int64_t* zero_elems) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr);
+  const Tensor& T = *t->p;
+  int64_t       nz = 0, ne = 0;
+  for(size_t b = 0; b < T.zero_block.size(); b++)
+    if(T.zero_block[b]) {
+      nz++;
+      ne += (b + 1 < T.keys.size() ? T.offsets[b + 1] : T.nelems) - T.offsets[b];
+    }
+  if(on) *on = T.read_only ? 1 : 0;
+  if(zero_blocks) *zero_blocks = nz;
+  if(zero_elems) *zero_elems = ne;
   TB_API_END
 }
 
@@ -605,6 +631,7 @@ static void block_io(tb_tensor t, const int64_t* blockid, double* host, int64_t 
   T.check_blockid(blockid);
   const int64_t sz = T.block_size(blockid);
   TB_EXPECTS(n >= sz, "host buffer smaller than the block");
+  if(dir != 0) T.require_writable();
   if(!T.is_non_zero(blockid)) { // tensor_impl.hpp:324-329 / :395 / :432
     if(dir == 0) std::fill(host, host + sz, 0.0);
     return;
@@ -652,6 +679,7 @@ int tb_tensor_write(tb_tensor t, const double* host, int64_t n) {
   REQUIRE_ARG(t != nullptr && host != nullptr);
   TB_EXPECTS(n == t->p->nelems, "host buffer length must equal the stored element count");
   t->p->require_allocated();
+  t->p->require_writable();
   TB_CUDA(cudaSetDevice(t->p->ctx->device));
   TB_CUDA(cudaMemcpyAsync(t->p->data, host, sizeof(double) * n, cudaMemcpyHostToDevice, t->p->ctx->stream));
   TB_CUDA(cudaStreamSynchronize(t->p->ctx->stream));
@@ -726,6 +754,7 @@ int tb_tensor_load(tb_tensor t, const char* path) {
   REQUIRE_ARG(t != nullptr && path != nullptr);
   Tensor& T = *t->p;
   T.require_allocated();
+  T.require_writable();
   CkptFile cf;
   cf.f = fopen(path, "rb");
   TB_EXPECTS(cf.f != nullptr, std::string("cannot open for reading: ") + path);
@@ -757,6 +786,7 @@ int tb_tensor_write_async(tb_tensor t, const double* host, int64_t n) {
   Tensor& T = *t->p;
   TB_EXPECTS(n == T.nelems, "host buffer length must equal the stored element count");
   T.require_allocated();
+  T.require_writable();
   Ctx& c = *T.ctx;
   TB_CUDA(cudaSetDevice(c.device));
   if(!c.h2d) TB_CUDA(cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking));
@@ -875,7 +905,7 @@ int tb_mult_info(tb_labeled lhs, tb_labeled a, tb_labeled b, int64_t* ngroups, i
                         (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
   auto wl    = mult_worklist(op, lc, false);
   if(ngroups) *ngroups = (int64_t) wl->groups.size();
-  if(ntasks) *ntasks = (int64_t) wl->tasks.size();
+  if(ntasks) *ntasks = (int64_t) wl->tasks.size() + wl->ntasks_skipped;
   if(flops) *flops = wl->flops;
   TB_API_END
 }

@@ -34,6 +34,7 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <mutex>
 
 namespace tb {
 
@@ -1167,7 +1168,12 @@ constexpr int64_t kNoAllocBytes = int64_t(64) << 20; // 64 MiB of scratch per GP
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kNoAllocDevices = 64;
-void*         g_noalloc_base[kNoAllocDevices] = {nullptr}; // device address, per device
+// Device address of the array, looked up once per device (std::call_once: two host
+// threads making their first call on one device do not race on the entry).  A
+// cudaDeviceReset on the device would invalidate it, as it does every other device
+// object of the library.
+void*          g_noalloc_base[kNoAllocDevices] = {nullptr};
+std::once_flag g_noalloc_once[kNoAllocDevices];
 
 // Control words and descriptors at fixed offsets of the scratch.
 constexpr int64_t kCtlErr = 0, kCtlCtr = 4, kCtlBlockMax = 8, kCtlSlices = 16, kCtlDesc = 256, kCtlItems = 1280;
@@ -1241,6 +1247,8 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   p.err     = reinterpret_cast<int*>(base + kCtlErr);
   p.tslices = tsl;
   p.ctr     = reinterpret_cast<int*>(base + kCtlCtr);
+  // transposed reductions when C's last mode is a column label, as the allocating path
+  p.xpose = xpose_fits<S, NT>() && lc.nn > 0 && lc.n_c[lc.nn - 1] == lc.nc - 1 ? 1 : 0;
   const size_t smem = smem_bytes<S, NT>();
   TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
   k_contract_i8<S, NT, false><<<std::min(p.nitems, sm_count()), NTHREADS, smem, st>>>(p);
@@ -1372,11 +1380,11 @@ extern "C" int tb_block_multiply_int8_noalloc(double alpha, const double* a, con
     int dev = 0;
     TB_CUDA(cudaGetDevice(&dev));
     TB_EXPECTS(dev >= 0 && dev < kNoAllocDevices, "device index out of range");
-    if(g_noalloc_base[dev] == nullptr) {
+    std::call_once(g_noalloc_once[dev], [dev] {
       void* ptr = nullptr;
-      TB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+      TB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch)); // throws: the flag stays unset
       g_noalloc_base[dev] = ptr;
-    }
+    });
     auto*      base = static_cast<unsigned char*>(g_noalloc_base[dev]);
     const auto st   = static_cast<cudaStream_t>(stream);
     switch(S) {

@@ -81,7 +81,10 @@ struct DevItem {
 struct WorkList {
   std::vector<DevGroup> groups;
   std::vector<DevTask>  tasks;
-  double                flops = 0;
+  double                flops = 0;         // admitted FP64 FLOPs (tasks that run + skipped tasks)
+  double                flops_run = 0;     // FP64 FLOPs of the tasks in the list
+  double                flops_skipped = 0; // admitted tasks left out: an exactly-zero block of a read-only operand
+  int64_t               ntasks_skipped = 0;
   DevGroup*             d_groups = nullptr;
   DevTask*              d_tasks  = nullptr;
   int                   device   = -1;
@@ -188,6 +191,10 @@ void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks
                          int nunits, int nmodes, const double* eps, DenomSigns signs, double* part, double* out,
                          cudaStream_t stream);
 void launch_set_scalar(double* out, double v, cudaStream_t stream);
+// nonzero[b] = 1 if x[off_b, off_b + n_b) holds an element other than +0.0 / -0.0, else
+// 0, for the (off, n) pairs of a device array (the launcher clears nonzero first).
+void launch_block_nonzero(const double* x, const int64_t* pairs, int nblocks, uint32_t* nonzero,
+                          cudaStream_t stream);
 // Reads and clears the device error word of the split-INT8 launches of a work list;
 // throws TB_ERR_TIMEOUT if a device-side wait gave up.
 void check_int8_errors(const WorkList& wl, cudaStream_t stream);

@@ -155,16 +155,17 @@ double task_flops(const LabelClasses& lc, const DevGroup& g, const DevTask& t) {
 }
 
 void finalize_worklist(const LabelClasses& lc, WorkList& wl, bool upload) {
-  wl.flops = 0;
+  wl.flops_run = 0;
   for(const auto& g: wl.groups) {
     TB_EXPECTS(g.task_begin >= 0 && g.task_end >= g.task_begin &&
                  g.task_end <= (int64_t) wl.tasks.size(),
                "group task range out of bounds");
     for(int t = g.task_begin; t < g.task_end; t++) {
       validate_task(lc, g, wl.tasks[t]);
-      wl.flops += task_flops(lc, g, wl.tasks[t]);
+      wl.flops_run += task_flops(lc, g, wl.tasks[t]);
     }
   }
+  wl.flops = wl.flops_run + wl.flops_skipped;
   if(!upload) return;
   TB_CUDA(cudaGetDevice(&wl.device));
   auto up = [](auto*& dptr, const auto& vec) {

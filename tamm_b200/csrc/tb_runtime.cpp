@@ -329,6 +329,53 @@ void Tensor::require_allocated() const {
   if(data == nullptr && nelems > 0) fail(TB_ERR_STATE, "tensor is not allocated");
 }
 
+void Tensor::require_writable() const {
+  if(read_only) fail(TB_ERR_STATE, "tensor is marked read-only (tb_tensor_set_read_only)");
+}
+
+bool Tensor::block_is_zero(const int64_t* blockid) const {
+  if(!read_only) return false;
+  const int64_t k  = key(blockid);
+  auto          it = std::lower_bound(keys.begin(), keys.end(), k);
+  return it != keys.end() && *it == k && zero_block[it - keys.begin()] != 0;
+}
+
+// Sets or clears the read-only mark.  Setting it scans the stored blocks once on the
+// context's stream (after the work already enqueued there, which includes the waits
+// for asynchronous host writes) for blocks whose elements are all zero.
+void set_read_only(Tensor& T, bool on) {
+  if(!on) {
+    T.read_only = false;
+    T.zero_block.clear();
+    return;
+  }
+  T.require_allocated();
+  const int64_t nb = (int64_t) T.keys.size();
+  TB_EXPECTS(nb < (1ll << 31), "too many blocks");
+  std::vector<int64_t>  pairs(2 * std::max<int64_t>(nb, 1));
+  std::vector<uint32_t> nz(std::max<int64_t>(nb, 1), 1u);
+  for(int64_t b = 0; b < nb; b++) {
+    pairs[2 * b]     = T.offsets[b];
+    pairs[2 * b + 1] = (b + 1 < nb ? T.offsets[b + 1] : T.nelems) - T.offsets[b];
+  }
+  if(nb > 0) {
+    Ctx& c = *T.ctx;
+    TB_CUDA(cudaSetDevice(c.device));
+    auto* dp = static_cast<int64_t*>(c.arena->allocate((int64_t) sizeof(int64_t) * 2 * nb));
+    auto* dn = static_cast<uint32_t*>(c.arena->allocate((int64_t) sizeof(uint32_t) * nb));
+    TB_CUDA(cudaMemcpyAsync(dp, pairs.data(), sizeof(int64_t) * 2 * nb, cudaMemcpyHostToDevice, c.stream));
+    launch_block_nonzero(T.data, dp, (int) nb, dn, c.stream);
+    TB_CUDA(cudaMemcpyAsync(nz.data(), dn, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost, c.stream));
+    TB_CUDA(cudaStreamSynchronize(c.stream));
+    c.arena->deallocate(dn);
+    c.arena->deallocate(dp);
+  }
+  T.zero_block.assign(nb, 0);
+  for(int64_t b = 0; b < nb; b++) T.zero_block[b] = nz[b] ? 0 : 1;
+  T.read_only = true;
+  T.ro_serial = next_serial();
+}
+
 // -------------------------------------------------------------------- scheduler
 
 namespace {
@@ -375,7 +422,7 @@ bool same_target(const Labeled& x, const Labeled& y) {
 std::string signature(const Op& op) {
   std::ostringstream os;
   auto               put = [&](const Labeled& x) {
-    os << x.t << "#" << x.t->serial.v << ":";
+    os << x.t << "#" << x.t->serial.v << "r" << (x.t->read_only ? x.t->ro_serial : 0) << ":";
     for(size_t i = 0; i < x.labels.size(); i++)
       os << x.labels[i] << "@" << x.ltis[i].get() << "#" << x.ltis[i]->serial.v << ",";
     os << "|";
@@ -459,6 +506,8 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
     if(n == 0) return wl;
   std::vector<int64_t> itval(c.labels.size(), 0), inner(red.size(), 0);
   std::vector<int64_t> cid(c.labels.size()), aid(a.labels.size()), bid(b.labels.size());
+  std::vector<double>  skip_flops; // per group
+  std::vector<int64_t> skip_count;
   do {
     for(size_t i = 0; i < cid.size(); i++) cid[i] = cm[i][itval[i]];
     if(!c.t->is_non_zero(cid.data())) continue;
@@ -467,6 +516,8 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
     c.t->block_dims(cid.data(), g.cdims);
     g.task_begin = (int32_t) wl->tasks.size();
     std::fill(inner.begin(), inner.end(), 0);
+    double  gskip  = 0; // FLOPs and count of this group's skipped tasks
+    int64_t gskipn = 0;
     do {
       for(size_t i = 0; i < aid.size(); i++) {
         int64_t l = a_out[i] >= 0 ? itval[a_out[i]] : inner[a_red[i]];
@@ -483,17 +534,28 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
       t.b_off = b.t->locate(bid.data());
       a.t->block_dims(aid.data(), t.adims);
       b.t->block_dims(bid.data(), t.bdims);
+      // an admitted task over an exactly-zero block of a read-only operand adds exactly
+      // zero to C: it is counted, not run
+      if(a.t->block_is_zero(aid.data()) || b.t->block_is_zero(bid.data())) {
+        gskip += task_flops(lc, g, t);
+        gskipn++;
+        continue;
+      }
       wl->tasks.push_back(t);
     } while(!red.empty() && next_tuple(inner, red_nt));
     TB_EXPECTS(wl->tasks.size() < (1ull << 31), "too many tasks in one contraction");
     g.task_end = (int32_t) wl->tasks.size();
     wl->groups.push_back(g);
+    skip_flops.push_back(gskip);
+    skip_count.push_back(gskipn);
   } while(!cid.empty() && next_tuple(itval, c_nt));
   if(nranks > 1) { // keep the output blocks this rank owns
     const std::vector<int> owner = group_owners(lc, *wl, nranks);
     auto                   mine  = std::make_shared<WorkList>();
     for(size_t gi = 0; gi < wl->groups.size(); gi++) {
       if(owner[gi] != rank) continue;
+      mine->flops_skipped += skip_flops[gi];
+      mine->ntasks_skipped += skip_count[gi];
       DevGroup g   = wl->groups[gi];
       g.task_begin = (int32_t) mine->tasks.size();
       for(int t = wl->groups[gi].task_begin; t < wl->groups[gi].task_end; t++) mine->tasks.push_back(wl->tasks[t]);
@@ -502,6 +564,11 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
     }
     wl = mine;
   }
+  else
+    for(size_t gi = 0; gi < wl->groups.size(); gi++) {
+      wl->flops_skipped += skip_flops[gi];
+      wl->ntasks_skipped += skip_count[gi];
+    }
   finalize_worklist(lc, *wl, upload);
   return wl;
 }
@@ -517,6 +584,8 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
 
 void Sched::run(Op& op) {
   cudaStream_t st = ctx->stream;
+  if(op.kind == Op::Set || op.kind == Op::Add || op.kind == Op::Mult || op.kind == Op::Denom)
+    op.lhs.t->require_writable();
   if(op.kind == Op::Set) {
     op.lhs.t->require_allocated();
     if(op.fill_none) return;

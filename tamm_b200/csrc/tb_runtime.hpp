@@ -107,6 +107,13 @@ struct Tensor {
   bool                              owns   = true; // false: storage attached by the caller
   cudaEvent_t                       used   = nullptr; // end of the last compute op that touched it
   cudaEvent_t                       filled = nullptr; // end of the last asynchronous host write
+  // Read-only mark (tb_tensor_set_read_only): the contents stay constant while it is
+  // set, so contractions may rely on zero_block, one byte per stored block (key order),
+  // 1 where every element of the block is zero; ro_serial identifies the marking in
+  // the scheduler's cache keys.
+  bool                              read_only = false;
+  uint64_t                          ro_serial = 0;
+  std::vector<uint8_t>              zero_block;
   ~Tensor();
 
   void    build_table(); // Distribution_NW (distribution.hpp:201-243)
@@ -117,6 +124,9 @@ struct Tensor {
   void    block_dims(const int64_t* blockid, int32_t* dims) const;
   void    check_blockid(const int64_t* blockid) const;
   void    require_allocated() const;
+  void    require_writable() const; // TB_ERR_STATE while the read-only mark is set
+  // true if the tensor is marked read-only and the stored block is all zeros
+  bool    block_is_zero(const int64_t* blockid) const;
 };
 
 struct Labeled {

@@ -385,6 +385,8 @@ public:
     return v;
   }
   void write(const std::vector<double>& v) { check(tb_tensor_write(h_.get(), v.data(), (int64_t) v.size())); }
+  // contents constant until cleared; contractions skip tasks over its all-zero blocks
+  void set_read_only(bool on = true) { check(tb_tensor_set_read_only(h_.get(), on ? 1 : 0)); }
   tb_tensor handle() const { return h_.get(); }
 
 private:

@@ -280,6 +280,18 @@ class Tensor:
         self.ec = ec
         return self
 
+    def set_read_only(self, on: bool = True):
+        """Declare the contents constant (writes through the library then fail) and let
+        contractions skip tasks over its exactly-zero blocks (tb_tensor_set_read_only)."""
+        call("tb_tensor_set_read_only", self.h, int(bool(on)))
+        return self
+
+    def read_only_info(self):
+        """(marked, zero blocks, zero elements) found by the read-only scan."""
+        on, nb, ne = C.c_int(), C.c_int64(), C.c_int64()
+        call("tb_tensor_read_only_info", self.h, C.byref(on), C.byref(nb), C.byref(ne))
+        return bool(on.value), nb.value, ne.value
+
     def data_ptr(self):
         p = A.vp()
         call("tb_tensor_data", self.h, C.byref(p))
@@ -545,6 +557,11 @@ class Scheduler:
         self._keep += [e, sg]
         call("tb_sched_denom", self.h, self._labeled(t, ids), float(alpha), self._labeled(r, ids),
              e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
+        return self
+
+    def clear(self):
+        """Drop the queued ops without running them (e.g. after an execute failed)."""
+        call("tb_sched_clear", self.h)
         return self
 
     def release(self):

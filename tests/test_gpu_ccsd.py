@@ -42,7 +42,9 @@ def _add(dst, dlabels, alpha, src, slabels):
         dst.block(bid)[...] += alpha * blk.transpose([slabels.index(x) for x in dlabels])
 
 
-def _oracle_iteration(P, t2_0):
+def _oracle_iteration(P, t2_0, impl="port"):
+    """One iteration on the oracle's block tensors; impl "ref" runs every block triple
+    through the reference's compiled block_multiply."""
     T = P.T
     ot = {n: _ob(t, MASKS.get(n, [0, 0, 1, 1]), t.read()) for n, t in T.items()
           if n in ("L_vo", "L_oo", "L_vv", "f_oo", "f_vv", "v_vvoo", "v_oooo", "v_ovvo")}
@@ -51,26 +53,26 @@ def _oracle_iteration(P, t2_0):
     v = ot["v_vvoo"]
     mk = lambda like, mask=(0, 0, 1, 1): _ob(like, list(mask))
     F_vv = mk(T["F_vv"], (0, 1)); F_vv.data[:] = ot["f_vv"].data
-    O.mult_bufacc(F_vv, [b, c], -0.5, v, [c, d, k, l], t2, [b, d, k, l])
+    O.mult_bufacc(F_vv, [b, c], -0.5, v, [c, d, k, l], t2, [b, d, k, l], impl=impl)
     F_oo = mk(T["F_oo"], (0, 1)); F_oo.data[:] = ot["f_oo"].data
-    O.mult_bufacc(F_oo, [k, j], 0.5, v, [c, d, k, l], t2, [c, d, j, l])
+    O.mult_bufacc(F_oo, [k, j], 0.5, v, [c, d, k, l], t2, [c, d, j, l], impl=impl)
     W_oo = mk(T["W_oo"]); W_oo.data[:] = 0.5 * ot["v_oooo"].data
-    O.mult_bufacc(W_oo, [k, l, i, j], 0.25, v, [c, d, k, l], t2, [c, d, i, j])
+    O.mult_bufacc(W_oo, [k, l, i, j], 0.25, v, [c, d, k, l], t2, [c, d, i, j], impl=impl)
     W_ov = mk(T["W_ov"]); W_ov.data[:] = ot["v_ovvo"].data
-    O.mult_bufacc(W_ov, [k, b, c, j], 0.5, v, [c, d, k, l], t2, [d, b, l, j])
+    O.mult_bufacc(W_ov, [k, b, c, j], 0.5, v, [c, d, k, l], t2, [d, b, l, j], impl=impl)
     r2 = mk(T["r2"]); r2.data[:] = v.data
-    O.mult_bufacc(r2, [a, b, i, j], 1.0, F_vv, [b, c], t2, [a, c, i, j])
-    O.mult_bufacc(r2, [a, b, i, j], -1.0, F_vv, [a, c], t2, [b, c, i, j])
-    O.mult_bufacc(r2, [a, b, i, j], -1.0, F_oo, [k, j], t2, [a, b, i, k])
-    O.mult_bufacc(r2, [a, b, i, j], 1.0, F_oo, [k, i], t2, [a, b, j, k])
-    O.mult_bufacc(r2, [a, b, i, j], 1.0, W_oo, [k, l, i, j], t2, [a, b, k, l])
+    O.mult_bufacc(r2, [a, b, i, j], 1.0, F_vv, [b, c], t2, [a, c, i, j], impl=impl)
+    O.mult_bufacc(r2, [a, b, i, j], -1.0, F_vv, [a, c], t2, [b, c, i, j], impl=impl)
+    O.mult_bufacc(r2, [a, b, i, j], -1.0, F_oo, [k, j], t2, [a, b, i, k], impl=impl)
+    O.mult_bufacc(r2, [a, b, i, j], 1.0, F_oo, [k, i], t2, [a, b, j, k], impl=impl)
+    O.mult_bufacc(r2, [a, b, i, j], 1.0, W_oo, [k, l, i, j], t2, [a, b, k, l], impl=impl)
     X = mk(T["X"])
-    O.mult_bufacc(X, [a, b, i, j], 1.0, t2, [a, c, i, k], W_ov, [k, b, c, j])
+    O.mult_bufacc(X, [a, b, i, j], 1.0, t2, [a, c, i, k], W_ov, [k, b, c, j], impl=impl)
     for alpha, sl in ((1.0, [a, b, i, j]), (-1.0, [b, a, i, j]), (-1.0, [a, b, j, i]), (1.0, [b, a, j, i])):
         _add(r2, [a, b, i, j], alpha, X, sl)
     v4 = O.BlockTensor([V.tile_sizes] * 4, [V.tile_spins] * 4, [0, 0, 1, 1])
-    O.mult_bufacc(v4, [a, b, c, d], 1.0, ot["L_vv"], [q, a, c], ot["L_vv"], [q, b, d])
-    O.mult_bufacc(r2, [a, b, i, j], 0.5, v4, [a, b, c, d], t2, [c, d, i, j])
+    O.mult_bufacc(v4, [a, b, c, d], 1.0, ot["L_vv"], [q, a, c], ot["L_vv"], [q, b, d], impl=impl)
+    O.mult_bufacc(r2, [a, b, i, j], 0.5, v4, [a, b, c, d], t2, [c, d, i, j], impl=impl)
     energy = 0.25 * float(np.dot(v.data[:v.total], t2.data[:t2.total]))
     norm = float(np.sqrt(np.dot(r2.data[:r2.total], r2.data[:r2.total])))
     t2n = _ob(T["t2"], [0, 0, 1, 1], t2_0)

@@ -3,10 +3,11 @@ that cannot allocate device memory (their memory already belongs to other alloca
 or they must avoid the synchronisation a cudaMalloc / cudaFree can cause): it keeps its
 scratch in a fixed 64 MiB device array instead of allocating.
 
-Two calls in a row, on different block shapes, must each match the allocating
-tb_block_multiply in TB_MODE_INT8 within the split-INT8 tolerance of the other tests
-(max |diff| <= 1e-11 * max |product|), so nothing the first call leaves in the shared
-array leaks into the second.  Kept in its own file that pytest collects last."""
+Calls in a row, on different block shapes and digit counts, must each match both the
+oracle's block_multiply (the reference's compiled kernel where it was built) and the
+allocating tb_block_multiply in TB_MODE_INT8, within the split-INT8 tolerance of the
+other tests (max |diff| <= 1e-11 * max |product|), so nothing one call leaves in the
+shared array leaks into the next.  Kept in its own file that pytest collects last."""
 import ctypes as C
 
 import numpy as np
@@ -59,27 +60,39 @@ def _allocating(alpha, a, al, b, bl, c0, cl):
     return dc.cpu().numpy().reshape(c0.shape)
 
 
-def _no_alloc(alpha, a, al, b, bl, c0, cl):
+def _no_alloc(alpha, a, al, b, bl, c0, cl, nslices=0):
     (da, db, dc), k = _args(a, al, b, bl, c0, cl)
     A.call("tb_block_multiply_int8_noalloc", alpha, da.data_ptr(), k[0].ctypes.data_as(A.i64p),
            k[1].ctypes.data_as(A.ip), a.ndim, db.data_ptr(), k[2].ctypes.data_as(A.i64p),
            k[3].ctypes.data_as(A.ip), b.ndim, dc.data_ptr(), k[4].ctypes.data_as(A.i64p),
-           k[5].ctypes.data_as(A.ip), c0.ndim, 0, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+           k[5].ctypes.data_as(A.ip), c0.ndim, nslices, C.c_void_p(torch.cuda.current_stream().cuda_stream))
     torch.cuda.synchronize()
     return dc.cpu().numpy().reshape(c0.shape)
 
 
-def test_no_alloc_matches_allocating_entry_point_two_calls():
+def _oracle(alpha, a, al, b, bl, c0, cl):
+    c = c0.copy()
+    assert O.block_multiply(alpha, a, al, b, bl, 1.0, c, cl, 0, impl="ref" if O.ref() is not None else "port") == 0
+    return c
+
+
+def test_no_alloc_matches_oracle_and_allocating_entry_point():
     cases = [
-        (dict(a=24, b=31, c=29, d=37, i=20, j=20), ("abij", "abcd", "cdij"), 41),  # ladder-shaped tile pair
-        (dict(a=13, b=9, c=7, d=5, i=3, j=11), ("ijab", "cadb", "jdci"), 42),      # permuted labels
+        # ladder-shaped tile pair; C's last mode a column label (transposed epilogue)
+        (dict(a=24, b=31, c=29, d=37, i=20, j=20), ("abij", "abcd", "cdij"), 41, 0),
+        # permuted labels, C's last mode a row label
+        (dict(a=13, b=9, c=7, d=5, i=3, j=11), ("ijab", "cadb", "jdci"), 42, 0),
+        # eight digits: the 64-wide output tiles
+        (dict(a=40, b=7, c=33, d=3, i=6, j=17), ("abij", "acbd", "cdji"), 43, 8),
     ]
-    for shape, labels, seed in cases:  # two calls in a row on the shared scratch
+    for shape, labels, seed, ns in cases:  # calls in a row on the shared scratch
         a, b, c0, al, bl, cl = _case(shape, labels, seed)
+        ref = _oracle(0.75, a, al, b, bl, c0, cl)
         want = _allocating(0.75, a, al, b, bl, c0, cl)
-        got = _no_alloc(0.75, a, al, b, bl, c0, cl)
-        prod = want - c0
-        assert np.max(np.abs(got - want)) <= INT8_TOL * np.max(np.abs(prod))
+        got = _no_alloc(0.75, a, al, b, bl, c0, cl, ns)
+        scale = np.max(np.abs(ref - c0))
+        assert np.max(np.abs(got - ref)) <= INT8_TOL * scale, f"case {seed}: vs oracle"
+        assert np.max(np.abs(got - want)) <= INT8_TOL * scale, f"case {seed}: vs allocating entry point"
 
 
 def test_no_alloc_rejects_triples_beyond_the_static_scratch():
