@@ -14,8 +14,12 @@ The integral tensor v is marked read-only (it is constant through a coupled-clus
 run), so both the FP64 and the split-INT8 path skip the admitted tasks over its
 exactly-zero spin blocks; the metric still counts every admitted FLOP, and the line
 also reports the FLOPs that ran and the throughput on that basis.
-Under torchrun (N > 1) each rank runs an independent copy of the workload on its
-own GPU (replicas: the path needs no exchange), timing is the max over ranks.
+Under torchrun (N > 1) the ladder is sharded by output block (TAMM's owner-computes
+rule with a FLOP-balanced assignment every rank derives alone): each rank zeroes r2,
+computes the blocks it owns, and one NCCL all-reduce on the context's stream
+assembles r2 on every rank inside the step; inputs are replicated, the total work is
+fixed ("scaling": "strong"), timing is the max over ranks.  --shard runs the same
+path on one GPU (a one-rank NCCL group).
 
 After the ladder, the full doubles-residual iteration (O=60, V=480, tiles U{20..64},
 seed 2; about 50 ops captured in one CUDA graph) is timed in FP64 and autotuned
@@ -55,6 +59,7 @@ def parse():
     p.add_argument("--ccsd-steps", type=int, default=3, help="graph replays timed per mode")
     p.add_argument("--ccsd-oa", type=int, default=30)
     p.add_argument("--ccsd-va", type=int, default=240)
+    p.add_argument("--shard", action="store_true", help="owner-computes path with an all-reduce even at N=1")
     return p.parse_args()
 
 
@@ -244,10 +249,15 @@ def main():
 
     import torch
     import torch.distributed as dist
+    shard = world > 1 or args.shard
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    torch.cuda.set_device(local)
+    elif shard:  # one-rank group: the sharded path's collective on a single GPU
+        import datetime
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:29533", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=600))
     import tamm_b200 as tb
     from tamm_b200 import _capi as A
     from tamm_b200 import workloads as W
@@ -260,10 +270,22 @@ def main():
     _, v_zero_blocks, v_zero_elems = lad.v.read_only_info()
     a, b, c, d, i, j = lad.labels
     stream = torch.cuda.ExternalStream(ec.stream)
+    if shard:
+        lad.sch.set_owner(rank, world)  # Mult ops compute this rank's output blocks only
+
+    def allreduce(t):
+        """Sum of the ranks' shares of t, in place, on the context's stream."""
+        with torch.cuda.stream(stream):
+            dist.all_reduce(t.device_view())
+        t.record_use()
 
     def step(profile=False):
+        if shard:  # blocks of other ranks stay zero here; the all-reduce adds the shares
+            lad.sch(lad.r2().assign(0.0))
         lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(
             tb.ExecutionHW.GPU, profile)
+        if shard:
+            allreduce(lad.r2)
 
     def reset():
         lad.sch(lad.r2().assign(0.0)).execute()
@@ -272,6 +294,13 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        return float(t.item())
 
     def max_over_ranks(x):
         if world == 1:
@@ -313,7 +342,8 @@ def main():
     clocks = clk.stop()
     if fp64_ms is None:
         fp64_ms = ms
-    value = world * lad.flops / (ms * 1e-3) / 1e12
+    jobs = 1 if shard else world  # copies of the workload the job computes
+    value = jobs * lad.flops / (ms * 1e-3) / 1e12
 
     # e2e through the public API: every step copies its t2 in from pinned host memory
     # and reads its r2 back, with two device buffer sets used in turn so that a step's
@@ -328,7 +358,11 @@ def main():
     def e2e_step(k):
         t2x, r2x = bufs[k % 2]
         t2x.write_async(t2_pin.data_ptr())
+        if shard:
+            lad.sch(r2x().assign(0.0))
         lad.sch(r2x(a, b, i, j).iadd(lad.v(a, b, c, d) * t2x(c, d, i, j))).execute_async()
+        if shard:
+            allreduce(r2x)
         r2x.read_async(r2_pin[k % 2].data_ptr())
 
     n_e2e = args.steps
@@ -346,13 +380,13 @@ def main():
     lad.sch.wait()
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / n_e2e)
-    e2e_val = world * lad.flops / (e2e_ms * 1e-3) / 1e12
+    e2e_val = jobs * lad.flops / (e2e_ms * 1e-3) / 1e12
     lad.t2.write(lad.t2_host)
 
     # roofline of the dominant kernel from a profiled step (CUDA events on the stream)
     step(profile=True)
     st = lad.sch.op_stats(-1)
-    flops_run = st["flops_run"]
+    flops_run = sum_over_ranks(st["flops_run"]) if shard else st["flops_run"]
     peaks = load_peaks()
     if headline in ("int8", "bf16x3"):
         S = st["slices_max"]
@@ -415,7 +449,8 @@ def main():
                                       os.cpu_count() or 1)
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": {"fp64": "f64", "int8": "s8 balanced digits, s32 accumulate, f64 recombination",
                                            "bf16x3": "bf16 hi+lo pieces, f32 accumulate, f64 recombination"}[headline],
             "data": "synthetic (seeded; no dataset)",
@@ -425,9 +460,10 @@ def main():
                        "v_read_only": {"zero_blocks": v_zero_blocks, "zero_elements": v_zero_elems},
                        "slices": st.get("slices_max"),
                        "l2": f"inputs larger than L2 (v = {8*lad.v.nelems/1e9:.1f} GB), no flush",
-                       "parallelism": f"replicas x{world}"},
-            "fp64_path": {"value": world * lad.flops / (fp64_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": fp64_ms},
-            "value_nonzero": {"value": world * flops_run / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                       "parallelism": (f"owner-computes x{world} (output blocks FLOP-balanced, NCCL all-reduce of "
+                                       f"r2 in every step)") if shard else f"replicas x{world}"},
+            "fp64_path": {"value": jobs * lad.flops / (fp64_ms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": fp64_ms},
+            "value_nonzero": {"value": jobs * flops_run / (ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                               "basis": "FLOPs of the tasks that ran (exactly-zero blocks of v skipped)"},
             "speedup_vs_fp64_path": fp64_ms / ms,
             "max_rel_err_vs_fp64": max_rel_err,

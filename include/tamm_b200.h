@@ -275,6 +275,12 @@ int tb_tensor_add(tb_tensor t, const int64_t* blockid, const double* host, int64
  * must stay untouched until tb_ctx_synchronize / tb_sched_wait returns. */
 int tb_tensor_write_async(tb_tensor t, const double* host, int64_t n);
 int tb_tensor_read_async(tb_tensor t, double* host, int64_t n);
+/* Marks the end of the work enqueued so far on the context's compute stream as the
+ * tensor's last use (no counterpart in TAMM): a caller that enqueues its own work on
+ * the tensor there, e.g. an NCCL all-reduce assembling the shares of an owner-computes
+ * contraction, calls it so that a later asynchronous read or write waits for that
+ * work too. */
+int tb_tensor_record_use(tb_tensor t);
 /* Whole packed store <-> host (n == nelems). */
 int tb_tensor_write(tb_tensor t, const double* host, int64_t n);
 int tb_tensor_read(tb_tensor t, double* host, int64_t n);

@@ -88,6 +88,7 @@ PROTOS = {
     "tb_tensor_block_table": [h, i64p, i64p],
     "tb_tensor_data": [h, C.POINTER(vp)],
     "tb_tensor_set_read_only": [h, C.c_int],
+    "tb_tensor_record_use": [h],
     "tb_tensor_read_only_info": [h, ip, i64p, i64p],
     "tb_tensor_is_non_zero": [h, i64p, ip],
     "tb_tensor_block_size": [h, i64p, i64p],

@@ -798,6 +798,17 @@ int tb_tensor_write_async(tb_tensor t, const double* host, int64_t n) {
   TB_API_END
 }
 
+int tb_tensor_record_use(tb_tensor t) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr);
+  Tensor& T = *t->p;
+  T.require_allocated();
+  TB_CUDA(cudaSetDevice(T.ctx->device));
+  if(!T.used) TB_CUDA(cudaEventCreateWithFlags(&T.used, cudaEventDisableTiming));
+  TB_CUDA(cudaEventRecord(T.used, T.ctx->stream));
+  TB_API_END
+}
+
 int tb_tensor_read_async(tb_tensor t, double* host, int64_t n) {
   TB_API_BEGIN
   REQUIRE_ARG(t != nullptr && host != nullptr);

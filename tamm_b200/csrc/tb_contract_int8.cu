@@ -308,6 +308,208 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
   }
 }
 
+// Staged split for operand blocks whose rows lie one after another in memory (K
+// contiguous and row r at element offset r * K: e.g. v(a,b,c,d) split as rows (a,b) by
+// K = (c,d)).  Each unit of R rows (8, or 4 when K is long) is one contiguous range of
+// R * K doubles, brought into shared memory by one bulk copy; a producer warp keeps
+// NST units in flight in a ring of shared-memory stages, so every element is read from
+// HBM exactly once and both the row maximum and the digit conversion read shared
+// memory.  Consumers (8 warps): row max -> exponent, then thread (row, quad) turns 4
+// consecutive k into S digit words stored as in k_split_fused (core matrices of 8 rows
+// x 16 bytes; a 4-row unit fills half of each).  The copy covers the 16-byte aligned
+// interior [floor16(start), floor16(end)) of the unit's bytes; a last element past
+// floor16(end) is loaded with a plain load.  Waits are bounded: a timeout records
+// `code` in *err and the consumers agree (bar.red) to leave together.
+struct StageMeta {
+  int32_t blk, row0, nlive, delta, tail, pad;
+};
+
+constexpr int64_t kStagedSmem = 227 * 1024; // dynamic shared memory of one staged-split CTA, at most
+constexpr int64_t kStagedHead = 1024;       // barriers, stage records, row maxima, before the ring
+// bytes of one stage of R rows of K doubles (+16 for the aligned start), 128-byte multiple
+__host__ __device__ constexpr int64_t staged_stage_bytes(int R, int64_t K) {
+  return (R * K * 8 + 16 + 127) / 128 * 128;
+}
+
+template<int S, int R>
+__global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __restrict__ blocks,
+                                                        const int32_t* __restrict__ chunk_begin, int nblocks,
+                                                        int nchunks, int nst, uint32_t stage_bytes,
+                                                        const double* __restrict__ src, uint8_t* __restrict__ dst,
+                                                        int32_t* __restrict__ exps, int32_t* __restrict__ blockmax,
+                                                        int* err) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  constexpr int UPC = 8 / R; // units per 8-row chunk
+  uint64_t*     full  = reinterpret_cast<uint64_t*>(sm);
+  uint64_t*     empty = full + 8;
+  StageMeta*    meta  = reinterpret_cast<StageMeta*>(empty + 8);
+  float*        pmax  = reinterpret_cast<float*>(meta + 8); // unused padding keeps 128-byte alignment below
+  double*       part  = reinterpret_cast<double*>(sm + 512);   // [2][8] partial row maxima
+  int32_t*      shift = reinterpret_cast<int32_t*>(part + 16); // [2][8] digit shifts
+  uint8_t*      ring  = sm + 1024;
+  (void) pmax;
+  const int     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int     nunits = nchunks * UPC;
+  const uint64_t bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
+  if(threadIdx.x == 0) {
+    for(int x = 0; x < nst; x++) {
+      mbar_init(&full[x], 1);
+      mbar_init(&empty[x], 8); // one arrival per consumer warp
+    }
+    fence_mbarrier_init();
+  }
+  __syncthreads();
+  if(warp == 0) {
+    // ---------------- producer: block lookup and one bulk copy per unit ----------------
+    // Block of chunk c: chunk_begin[lo] <= c < chunk_begin[lo + 1]; units come in
+    // increasing order, so the cursor only moves forward (32 blocks per ballot).
+    int      lo = 0, slot = 0;
+    uint32_t ph = 0;
+    for(int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      const int c = u / UPC;
+      while(true) {
+        const int      idx = lo + 1 + lane;
+        const unsigned le  = __ballot_sync(0xffffffffu, idx < nblocks && __ldg(chunk_begin + idx) <= c);
+        lo += __popc(le);
+        if(le != 0xffffffffu) break;
+      }
+      if(!mbar_wait(&empty[slot], ph ^ 1, err, 21)) break; // (every lane polls; all agree on success)
+      if(lane == 0) {
+        const SplitBlock& b    = blocks[lo];
+        const int         row0 = 8 * (c - __ldg(chunk_begin + lo)) + (u % UPC) * R;
+        const int         nl   = max(0, min(R, b.rows - row0));
+        StageMeta         m{lo, row0, nl, 0, 0, 0};
+        uint32_t          bytes = 0;
+        uintptr_t         a16   = 0;
+        if(nl > 0) {
+          const uintptr_t start = reinterpret_cast<uintptr_t>(src + b.src_off + (int64_t) row0 * b.K);
+          const uintptr_t end   = start + (uintptr_t) nl * b.K * 8;
+          a16                   = start & ~uintptr_t(15);
+          bytes                 = (uint32_t) ((end & ~uintptr_t(15)) - a16);
+          m.delta               = (int32_t) (start - a16);
+          m.tail                = (end & 15) ? 1 : 0;
+        }
+        meta[slot] = m;
+        mbar_arrive_expect_tx(&full[slot], bytes);
+        if(bytes > 0) bulk_g2s(ring + (size_t) slot * stage_bytes, reinterpret_cast<const void*>(a16), bytes,
+                               &full[slot]);
+      }
+      __syncwarp();
+      if(++slot == nst) {
+        slot = 0;
+        ph ^= 1;
+      }
+    }
+    return;
+  }
+  // ---------------- consumers: warps 1..8 ----------------
+  const int cw  = warp - 1; // 0..7
+  const int ctid = threadIdx.x - 32;
+  int       slot = 0;
+  uint32_t  ph   = 0;
+  for(int u = blockIdx.x, it = 0; u < nunits; u += gridDim.x, it++) {
+    {
+      const bool got = mbar_wait(&full[slot], ph, err, 22);
+      uint32_t   anyfail;
+      asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
+                   "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                   : "=r"(anyfail)
+                   : "r"((uint32_t) got), "n"(256)
+                   : "memory");
+      if(anyfail) return;
+    }
+    const StageMeta    m   = meta[slot];
+    const SplitBlock&  b   = blocks[m.blk];
+    uint8_t*           buf = ring + (size_t) slot * stage_bytes;
+    const double*      rowbase = reinterpret_cast<const double*>(buf + m.delta);
+    const int          K   = b.K;
+    const int          par = it & 1;
+    if(m.tail && ctid == 0) { // the last element, past the copy's 16-byte aligned end
+      const_cast<double*>(rowbase)[(int64_t) m.nlive * K - 1] =
+        __ldg(src + b.src_off + (int64_t) (m.row0 + m.nlive) * K - 1);
+      // ordered before the bulk copy that later refills this stage
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    if(m.tail) asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    // row maxima: 8 / R warps per row, each over its share of K
+    {
+      constexpr int WPR = 8 / R;
+      const int     r = cw % R, sh = cw / R;
+      double        mx = 0.0;
+      if(r < m.nlive) {
+        const double* x  = rowbase + (int64_t) r * K;
+        const int     k0 = sh * ((K + WPR - 1) / WPR), k1 = min(K, k0 + (K + WPR - 1) / WPR);
+        for(int k = k0 + lane; k < k1; k += 32) mx = fmax(mx, fabs(x[k]));
+      }
+#pragma unroll
+      for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if(lane == 0) part[par * 8 + cw] = mx;
+    }
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    if(ctid < R) {
+      const int r   = ctid;
+      double    mx  = 0.0;
+      for(int w = r; w < 8; w += R) mx = fmax(mx, part[par * 8 + w]);
+      const bool live = r < m.nlive;
+      const int  e    = row_exponent(mx);
+      shift[par * 8 + r] = live ? 8 * S - 1 - e : kPadRow;
+      exps[b.exp_off + m.row0 + r] = e;
+      if(mx > 0.0) atomicMax(blockmax + b.id, e);
+    }
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    // digits: lanes per 16-wide k chunk = 4 R (row, quad); 32 / (4 R) chunks per warp step
+    {
+      constexpr int LPC = 4 * R, CPW = 32 / LPC;
+      const int     rr = (lane % LPC) >> 2, q = lane & 3, sub = lane / LPC;
+      const int     sh = shift[par * 8 + rr];
+      const bool    live = sh != kPadRow;
+      const double  f1 = ldexp(1.0, live ? sh / 2 : 0), f2 = ldexp(1.0, live ? sh - sh / 2 : 0);
+      const int     row = m.row0 + rr; // row within the block
+      const int     nkc = b.K_pad / KC;
+      uint8_t*      out = dst + b.dst_off + (int64_t) (row / b.tile_rows) * nkc * S * b.tile_rows * KC +
+                     ((row % b.tile_rows) >> 3) * 128 + (row & 7) * 16 + q * 4;
+      const double* x   = rowbase + (int64_t) rr * K;
+      const int     n16 = b.K_pad / 16;
+      for(int k16 = cw * CPW + sub; k16 < n16; k16 += 8 * CPW) {
+        const int k0 = k16 * 16 + q * 4;
+        double    v[4];
+#pragma unroll
+        for(int t = 0; t < 4; t++) v[t] = (live && k0 + t < K) ? x[k0 + t] : 0.0;
+        uint32_t lo[4], hi[4];
+#pragma unroll
+        for(int t = 0; t < 4; t++) {
+          const uint64_t Y = (uint64_t) __double2ll_rn(v[t] * f1 * f2) + bias;
+          lo[t]            = (uint32_t) Y;
+          hi[t]            = (uint32_t) (Y >> 32);
+        }
+        uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
+#pragma unroll
+        for(int i = 0; i < S; i++) {
+          const int p = S - 1 - i; // byte of Y holding digit i
+          uint32_t  w;
+          if(p < 4) {
+            const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
+            const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          else {
+            const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
+            const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
+            w                 = __byte_perm(t0, t1, 0x5410);
+          }
+          __stcs(reinterpret_cast<unsigned int*>(o + (int64_t) i * b.tile_rows * 16), w ^ 0x80808080u);
+        }
+      }
+    }
+    __syncwarp();
+    if(lane == 0) mbar_arrive(&empty[slot]); // this warp is done with the stage
+    if(++slot == nst) {
+      slot = 0;
+      ph ^= 1;
+    }
+  }
+}
+
 // Slice count per task: a task whose largest possible product (2^(maxexp A + maxexp
 // B) * K) is 2^(8m) below the largest of its output group needs m fewer digits for
 // the same absolute truncation error; numerically zero blocks keep one digit.
@@ -631,45 +833,79 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
         tphase ^= 1;
         tc_fence_after();
-        // Diagonal d carries the row factor 2^k, k = e_row - 7 - 8d.  For k well inside
-        // the normal range it is applied inside the int32 -> double conversion:
-        // v * 2^k = (2^52 + 2^31 + v) * 2^k - (2^52 + 2^31) * 2^k, whose first term is
-        // assembled from its bits (high word: exponent 1075 + k, low word: v + 2^31) —
-        // exact, with no conversion instruction and no multiply.
+        // Diagonal d carries the row factor 2^k, k = e_row - 7 - 8d.  INT8: groups of up to
+        // three adjacent diagonals are combined exactly in int64,
+        //   G = D_g * 2^16 + D_(g+1) * 2^8 + D_(g+2)   (|D| < 2^31, so |G| < 2^48),
+        // and G * 2^k (k of the group's last diagonal) is formed without a conversion
+        // instruction when k is well inside the normal range: the double whose bits are
+        // ((1075 + k) << 52) + 2^51 + G equals (2^52 + 2^51 + G) * 2^k, and subtracting
+        // (2^52 + 2^51) * 2^k leaves G * 2^k exactly.  One FP64 add and one FMA per group
+        // instead of per diagonal; one rounding per group.  Otherwise (extreme row
+        // exponents) each diagonal is converted and scaled on its own.  BF16x3: FP32
+        // accumulators, exact in FP64.
         const bool   fast = !BF && er - 7 - 8 * (S - 1) >= -1000 && er - 7 <= 900;
         const double sr   = ldexp(1.0, er - off);
-        // drain diagonal by diagonal; each diagonal's TMEM is released as soon as it
-        // has been read, so the next task's MMAs into it can start
+        if constexpr(BF) {
+          // drain diagonal by diagonal; each diagonal's TMEM is released as soon as it
+          // has been read, so the next task's MMAs into it can start
 #pragma unroll
-        for(int d = 0; d < S; d++) {
-          if(d < st) {
-            uint32_t       v[NH];
-            const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + d * NT + col0;
-#pragma unroll
-            for(int l = 0; l + 16 <= NH; l += 16) tmem_ld16(ta + l, *reinterpret_cast<uint32_t(*)[16]>(v + l));
-            if(NH % 16) tmem_ld8(ta + NH - 8, *reinterpret_cast<uint32_t(*)[8]>(v + NH - 8));
-            tmem_wait_ld();
-            tc_fence_before();
-            mbar_arrive(&tempty[d]);
-            if(fast) {
-              const int    hi   = 0x43300000 + (er - 7 - 8 * d) * (1 << 20);
-              const double bias = __hiloint2double(hi, (int) 0x80000000u);
-#pragma unroll
-              for(int x = 0; x < NH; x++)
-                racc[x] = fma(__hiloint2double(hi, (int) (v[x] ^ 0x80000000u)) - bias, scb[col0 + x], racc[x]);
-            }
-            else if constexpr(BF) { // FP32 accumulators, exact in FP64
+          for(int d = 0; d < S; d++) {
+            if(d < st) {
+              uint32_t       v[NH];
+              const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + d * NT + col0;
+              tmem_ld_cols<NH>(ta, v);
+              tmem_wait_ld();
+              tc_fence_before();
+              mbar_arrive(&tempty[d]);
 #pragma unroll
               for(int x = 0; x < NH; x++) racc[x] = fma((double) __uint_as_float(v[x]), sr * scb[col0 + x], racc[x]);
             }
-            else {
-              const double w = pow2i(-8 * d) * sr;
-#pragma unroll
-              for(int x = 0; x < NH; x++) racc[x] = fma((double) (int32_t) v[x], w * scb[col0 + x], racc[x]);
-            }
+            else
+              mbar_arrive(&tempty[d]);
           }
-          else
-            mbar_arrive(&tempty[d]);
+        }
+        else {
+          constexpr int  CH = NH >= 24 ? NH / 2 : NH; // columns per TMEM load round
+          static_assert(NH % CH == 0 && CH % 4 == 0, "drain chunking");
+          const uint32_t tq = tmem + ((uint32_t) (q * 32) << 16) + col0;
+#pragma unroll
+          for(int g0 = 0; g0 < S; g0 += 3) {
+            const int gl = S - g0 < 3 ? S - g0 : 3; // diagonals in this group
+            if(g0 < st) {                           // (st is the same for every thread)
+              const int     last = g0 + gl - 1;
+              const int64_t hb   = ((int64_t) (1075 + er - 7 - 8 * last) << 52) + (1ll << 51);
+              const double  bias = __longlong_as_double(hb);
+#pragma unroll
+              for(int c0 = 0; c0 < NH; c0 += CH) {
+                uint32_t v0[CH], v1[CH], v2[CH];
+                tmem_ld_cols<CH>(tq + g0 * NT + c0, v0);
+                if(gl > 1 && g0 + 1 < st) tmem_ld_cols<CH>(tq + (g0 + 1) * NT + c0, v1);
+                if(gl > 2 && g0 + 2 < st) tmem_ld_cols<CH>(tq + (g0 + 2) * NT + c0, v2);
+                tmem_wait_ld();
+                const bool has1 = gl > 1 && g0 + 1 < st, has2 = gl > 2 && g0 + 2 < st;
+                if(fast) {
+#pragma unroll
+                  for(int x = 0; x < CH; x++) {
+                    int64_t G = (int64_t) (int32_t) v0[x];
+                    if(gl > 1) G = G * 256 + (has1 ? (int32_t) v1[x] : 0);
+                    if(gl > 2) G = G * 256 + (has2 ? (int32_t) v2[x] : 0);
+                    racc[c0 + x] = fma(__longlong_as_double(hb + G) - bias, scb[col0 + c0 + x], racc[c0 + x]);
+                  }
+                }
+                else {
+#pragma unroll
+                  for(int x = 0; x < CH; x++) {
+                    double t = (double) (int32_t) v0[x] * pow2i(-8 * g0);
+                    if(has1) t = fma((double) (int32_t) v1[x], pow2i(-8 * (g0 + 1)), t);
+                    if(has2) t = fma((double) (int32_t) v2[x], pow2i(-8 * (g0 + 2)), t);
+                    racc[c0 + x] = fma(t * sr, scb[col0 + c0 + x], racc[c0 + x]);
+                  }
+                }
+              }
+              tc_fence_before();
+            }
+            for(int d = g0; d < g0 + gl; d++) mbar_arrive(&tempty[d]);
+          }
         }
       }
       if(!ok) break;
@@ -725,6 +961,16 @@ struct I8Layout {
   int                     S = 0, NT = 0, esize = 1; // digits, output tile width, bytes per digit
   std::vector<SplitBlock> a_blocks, b_blocks;
   std::vector<int32_t>    a_cbegin, b_cbegin; // first 8-row chunk of each block, then the total
+  // the blocks of each operand split by the staged kernel (rows contiguous) and by the
+  // general one, each with its own chunk table
+  struct SplitSet {
+    std::vector<SplitBlock> blocks;
+    std::vector<int32_t>    cbegin;
+    SplitBlock*             d_blocks = nullptr;
+    int32_t*                d_cbegin = nullptr;
+    int                     kmax     = 0;
+  };
+  SplitSet                a_staged, a_general, b_staged, b_general;
   std::vector<I8Task>     tasks;
   std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
@@ -746,6 +992,10 @@ struct I8Layout {
   ~I8Layout() {
     if(device >= 0) {
       cudaSetDevice(device);
+      for(SplitSet* x: {&a_staged, &a_general, &b_staged, &b_general}) {
+        cudaFree(x->d_blocks);
+        cudaFree(x->d_cbegin);
+      }
       cudaFree(d_ablocks);
       cudaFree(d_bblocks);
       cudaFree(d_acbegin);
@@ -894,6 +1144,28 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   chunks(L->a_blocks, L->a_cbegin);
   chunks(L->b_blocks, L->b_cbegin);
+  // staged-kernel eligibility: K contiguous, row r at element offset r * K, and two
+  // 4-row stages of the longest row fit in shared memory
+  auto staged_ok = [&](const SplitBlock& b) {
+    if(esize != 1 || !b.kcontig) return false;
+    int64_t st = b.K;
+    for(int j = b.nr - 1; j >= 0; j--) {
+      if(b.rstr[j] != st) return false;
+      st *= b.rdim[j];
+    }
+    return staged_stage_bytes(4, b.K) * 2 + kStagedHead <= kStagedSmem;
+  };
+  auto partition = [&](const std::vector<SplitBlock>& all, I8Layout::SplitSet& st, I8Layout::SplitSet& ge) {
+    for(const auto& b: all) {
+      I8Layout::SplitSet& x = staged_ok(b) ? st : ge;
+      x.blocks.push_back(b);
+      x.kmax = std::max(x.kmax, b.K);
+    }
+    chunks(st.blocks, st.cbegin);
+    chunks(ge.blocks, ge.cbegin);
+  };
+  partition(L->a_blocks, L->a_staged, L->a_general);
+  partition(L->b_blocks, L->b_staged, L->b_general);
   // output tiles, longest group first (every tile of a group costs the same, so
   // ordering the groups orders the tiles)
   std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
@@ -924,6 +1196,10 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   up(L->d_ablocks, L->a_blocks);
   up(L->d_bblocks, L->b_blocks);
+  for(I8Layout::SplitSet* x: {&L->a_staged, &L->a_general, &L->b_staged, &L->b_general}) {
+    up(x->d_blocks, x->blocks);
+    up(x->d_cbegin, x->cbegin);
+  }
   up(L->d_acbegin, L->a_cbegin);
   up(L->d_bcbegin, L->b_cbegin);
   up(L->d_tasks, L->tasks);
@@ -945,21 +1221,48 @@ int sm_count() {
   return n;
 }
 
+template<int S, int R>
+void launch_staged(const I8Layout::SplitSet& x, const double* src, uint8_t* slices, int32_t* exps,
+                   int32_t* blockmax, int* err, cudaStream_t st) {
+  const int      nblocks = (int) x.cbegin.size() - 1, nchunks = x.cbegin.back();
+  const uint32_t sb      = (uint32_t) staged_stage_bytes(R, x.kmax);
+  const int      nst     = (int) std::min<int64_t>(8, (kStagedSmem - kStagedHead) / sb);
+  const size_t   smem    = kStagedHead + (size_t) nst * sb;
+  static bool    configured[64] = {false};
+  int            dev            = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  if(dev < 64 && !configured[dev]) {
+    TB_CUDA(cudaFuncSetAttribute(k_split_staged<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem));
+    configured[dev] = true;
+  }
+  const int grid = std::min(nchunks * (8 / R), sm_count());
+  k_split_staged<S, R><<<grid, 288, smem, st>>>(x.d_blocks, x.d_cbegin, nblocks, nchunks, nst, sb, src, slices, exps,
+                                                blockmax, err);
+}
+
 template<int S, bool BF>
 void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const double* B, uint8_t* slices,
                   int32_t* exps, cudaStream_t st) {
   const int grid_cap = sm_count() * 8;
   // 0x80808080: below every exponent sum, marks blocks without a nonzero row
   TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
-  auto one = [&](const SplitBlock* blocks, const int32_t* cbegin, const std::vector<int32_t>& hbegin,
-                 const double* src) {
-    const int nblocks = (int) hbegin.size() - 1, nchunks = hbegin.back();
-    if(nchunks == 0) return;
-    const int grid = std::min(nchunks, grid_cap);
-    k_split_fused<S, BF><<<grid, 256, 0, st>>>(blocks, cbegin, nblocks, nchunks, src, slices, exps, L.d_blockmax);
+  auto one = [&](const I8Layout::SplitSet& staged, const I8Layout::SplitSet& general, const double* src) {
+    if(!general.blocks.empty() && general.cbegin.back() > 0) {
+      const int nblocks = (int) general.cbegin.size() - 1, nchunks = general.cbegin.back();
+      k_split_fused<S, BF><<<std::min(nchunks, grid_cap), 256, 0, st>>>(general.d_blocks, general.d_cbegin, nblocks,
+                                                                          nchunks, src, slices, exps, L.d_blockmax);
+    }
+    if constexpr(!BF) {
+      if(!staged.blocks.empty() && staged.cbegin.back() > 0) {
+        // 8-row units while three stages of the longest row fit, else 4-row units
+        if(kStagedHead + 3 * staged_stage_bytes(8, staged.kmax) <= kStagedSmem)
+          launch_staged<S, 8>(staged, src, slices, exps, L.d_blockmax, L.d_err, st);
+        else launch_staged<S, 4>(staged, src, slices, exps, L.d_blockmax, L.d_err, st);
+      }
+    }
   };
-  one(L.d_ablocks, L.d_acbegin, L.a_cbegin, A);
-  one(L.d_bblocks, L.d_bcbegin, L.b_cbegin, B);
+  one(L.a_staged, L.a_general, A);
+  one(L.b_staged, L.b_general, B);
   const int ng = (int) wl.groups.size();
   if constexpr(BF) { // both bf16 pieces in every task
     if(!L.tasks.empty()) TB_CUDA(cudaMemsetAsync(L.d_tslices, S, L.tasks.size(), st));

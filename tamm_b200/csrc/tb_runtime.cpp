@@ -333,6 +333,12 @@ void Tensor::require_writable() const {
   if(read_only) fail(TB_ERR_STATE, "tensor is marked read-only (tb_tensor_set_read_only)");
 }
 
+int64_t Tensor::block_index(const int64_t* blockid) const {
+  const int64_t k  = key(blockid);
+  auto          it = std::lower_bound(keys.begin(), keys.end(), k);
+  return (it != keys.end() && *it == k) ? (int64_t) (it - keys.begin()) : -1;
+}
+
 bool Tensor::block_is_zero(const int64_t* blockid) const {
   if(!read_only) return false;
   const int64_t k  = key(blockid);
@@ -534,9 +540,11 @@ std::shared_ptr<WorkList> build_mult_worklist(const Op& op, const LabelClasses& 
       t.b_off = b.t->locate(bid.data());
       a.t->block_dims(aid.data(), t.adims);
       b.t->block_dims(bid.data(), t.bdims);
-      // an admitted task over an exactly-zero block of a read-only operand adds exactly
-      // zero to C: it is counted, not run
-      if(a.t->block_is_zero(aid.data()) || b.t->block_is_zero(bid.data())) {
+      // an admitted task over an exactly-zero block of a read-only operand, or over a
+      // block that an earlier assignment of the same op list left without any
+      // contribution, adds exactly zero to C: it is counted, not run
+      if(a.t->block_is_zero(aid.data()) || b.t->block_is_zero(bid.data()) ||
+         (op.za && (*op.za)[a.t->block_index(aid.data())]) || (op.zb && (*op.zb)[b.t->block_index(bid.data())])) {
         gskip += task_flops(lc, g, t);
         gskipn++;
         continue;
@@ -771,9 +779,21 @@ void Sched::run(Op& op) {
 
 // Plan and work list of a MultOp, from the caches (keyed by the op's signature and
 // this rank's share).
+// Key of a structural-zero pattern: count of zero blocks and an FNV-1a hash of the bytes.
+static std::string zero_key(const std::shared_ptr<const std::vector<uint8_t>>& z) {
+  if(!z) return "-";
+  uint64_t h = 1469598103934665603ull, n = 0;
+  for(uint8_t x: *z) {
+    h = (h ^ x) * 1099511628211ull;
+    n += x;
+  }
+  return std::to_string(n) + ":" + std::to_string(h);
+}
+
 void Sched::prepare_mult(Op& op) {
   if(op.wl) return;
-  const std::string sig = signature(op) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks);
+  const std::string sig = signature(op) + "|owner " + std::to_string(rank) + "/" + std::to_string(nranks) +
+                          "|z " + zero_key(op.za) + " " + zero_key(op.zb);
   auto              pit = plan_cache.find(sig);
   if(pit == plan_cache.end()) {
     auto plan        = std::make_shared<Plan>();
@@ -951,6 +971,32 @@ Graph::~Graph() {
   pool.release();
 }
 
+// Updates the blocks known to be zero after `op` ran (see Sched::execute).
+void Sched::note_zeros(const Op& op, std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>>& szero) {
+  Tensor* t = op.lhs.t;
+  if(t == nullptr || op.kind == Op::Dot || op.kind == Op::DenomEnergy || op.kind == Op::SetScalar) return;
+  if(op.kind == Op::Set) {
+    bool whole = op.is_assign && op.value == 0.0;
+    for(int m = 0; whole && m < t->nmodes; m++) whole = op.lhs.ltis[m]->tiles == t->tis[m]->tiles;
+    if(whole) szero[t] = std::make_shared<std::vector<uint8_t>>(t->keys.size(), 1);
+    else szero.erase(t);
+    return;
+  }
+  auto it = szero.find(t);
+  if(it == szero.end()) return;
+  if(op.kind != Op::Mult || !op.wl) {
+    szero.erase(it);
+    return;
+  }
+  auto next = std::make_shared<std::vector<uint8_t>>(*it->second);
+  for(const auto& g: op.wl->groups) {
+    if(g.task_begin == g.task_end) continue;
+    auto o = std::lower_bound(t->offsets.begin(), t->offsets.end(), g.c_off);
+    if(o != t->offsets.end() && *o == g.c_off) (*next)[o - t->offsets.begin()] = 0;
+  }
+  it->second = next;
+}
+
 void Sched::execute(bool profile) {
   TB_CUDA(cudaSetDevice(ctx->device));
   // keep only the ops about to run (the history of earlier executes is not needed:
@@ -967,14 +1013,34 @@ void Sched::execute(bool profile) {
     ev.resize(2 * (ops.size() - start));
     for(auto& e: ev) TB_CUDA(cudaEventCreate(&e));
   }
+  // Blocks known to be zero by construction, per tensor, from the ops of this execute
+  // so far (nothing is assumed about a tensor's contents at the start): an assignment
+  // of zero makes every block zero, a contraction into the tensor clears the blocks of
+  // its output groups that have tasks, any other write forgets what was known.  This
+  // follows the op list's structure only, never the data, so a graph capture of the
+  // same list makes the same decisions for every replay.
+  std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>> szero;
+  auto known = [&](const Tensor* t) -> std::shared_ptr<const std::vector<uint8_t>> {
+    auto it = szero.find(t);
+    return it == szero.end() ? nullptr : it->second;
+  };
   for(size_t i = start; i < ops.size(); i++) {
     if(profile) TB_CUDA(cudaEventRecord(ev[2 * (i - start)], ctx->stream));
+    if(ops[i].kind == Op::Mult) {
+      ops[i].za = known(ops[i].a.t);
+      ops[i].zb = known(ops[i].b.t);
+    }
+    if(i + 1 < ops.size() && ops[i + 1].kind == Op::Mult) {
+      ops[i + 1].za = known(ops[i + 1].a.t);
+      ops[i + 1].zb = known(ops[i + 1].b.t);
+    }
     if(nranks == 1 && ctx->mode == TB_MODE_FP64 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
        ops[i].is_assign && ops[i].value == 0.0 &&
        ops[i + 1].kind == Op::Mult && same_target(ops[i].lhs, ops[i + 1].lhs) &&
        ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t) // C read as an operand needs the fill
       fuse_assign(ops[i], ops[i + 1]);
     run(ops[i]);
+    note_zeros(ops[i], szero);
     if(ops[i].kind == Op::Mult && deferred_checks && ops[i].wl) pending.push_back(ops[i].wl);
     if(!pinned) // (a captured graph orders its own ops)
       for(Tensor* t: {ops[i].lhs.t, ops[i].a.t, ops[i].b.t}) mark_used(t, ctx->stream);

@@ -127,6 +127,7 @@ struct Tensor {
   void    require_writable() const; // TB_ERR_STATE while the read-only mark is set
   // true if the tensor is marked read-only and the stored block is all zeros
   bool    block_is_zero(const int64_t* blockid) const;
+  int64_t block_index(const int64_t* blockid) const; // position in keys, -1 if not stored
 };
 
 struct Labeled {
@@ -168,6 +169,10 @@ struct Op {
   // Mult's work list leaves without tasks (fill_none: there are none)
   bool                                   store = false, fill_none = false;
   double                                 flops = 0;
+  // blocks of the operands known to be zero by construction at this op's place in its
+  // execute (one byte per stored block; null: nothing known): an earlier assignment of
+  // the same op list left them without any contribution
+  std::shared_ptr<const std::vector<uint8_t>> za, zb;
 };
 
 // Orbital energies over a root index space (device copy) and per-mode signs of a
@@ -217,6 +222,7 @@ struct Sched {
   void                                              execute(bool profile);
   void                                              run(Op& op);
   void                                              prepare_mult(Op& op);
+  void note_zeros(const Op& op, std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>>& szero);
   void                                              fuse_assign(Op& set, Op& mult);
   void                                              tune(Op& op, const std::string& key);
   double*                                           scalars();

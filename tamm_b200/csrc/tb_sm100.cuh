@@ -149,6 +149,22 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+// N consecutive columns (N a multiple of 4) into r[0..N), as x16 / x8 / x4 loads.
+template<int N>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, uint32_t* r) {
+  static_assert(N % 4 == 0, "columns in multiples of 4");
+#pragma unroll
+  for(int l = 0; l + 16 <= N; l += 16) tmem_ld16(taddr + l, *reinterpret_cast<uint32_t(*)[16]>(r + l));
+  constexpr int R16 = N / 16 * 16;
+  if constexpr((N - R16) >= 8) tmem_ld8(taddr + R16, *reinterpret_cast<uint32_t(*)[8]>(r + R16));
+  constexpr int R8 = R16 + ((N - R16) >= 8 ? 8 : 0);
+  if constexpr((N - R8) == 4) tmem_ld4(taddr + R8, *reinterpret_cast<uint32_t(*)[4]>(r + R8));
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 __device__ __forceinline__ bool elect_one() {

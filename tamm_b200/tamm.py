@@ -280,6 +280,24 @@ class Tensor:
         self.ec = ec
         return self
 
+    def record_use(self):
+        """Order later asynchronous transfers after work the caller enqueued on the
+        context's stream (e.g. a collective over this tensor's storage)."""
+        call("tb_tensor_record_use", self.h)
+        return self
+
+    def device_view(self):
+        """A torch tensor sharing this tensor's packed device storage (no copy), for
+        collectives and checks; valid while the tensor stays allocated."""
+        import torch
+
+        class _Dev:
+            pass
+        d = _Dev()
+        d.__cuda_array_interface__ = {"shape": (self.nelems,), "typestr": "<f8", "data": (self.data_ptr(), False),
+                                      "version": 3, "strides": None}
+        return torch.as_tensor(d, device=f"cuda:{self.ec.device}")
+
     def set_read_only(self, on: bool = True):
         """Declare the contents constant (writes through the library then fail) and let
         contractions skip tasks over its exactly-zero blocks (tb_tensor_set_read_only)."""

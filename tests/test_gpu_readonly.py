@@ -137,3 +137,38 @@ def test_read_only_tensor_rejects_writes(ec):
     assert np.array_equal(lad.v.read(), vh)
     lad.v.set_read_only(False)
     lad.v.write(vh)
+
+
+def test_structural_zeros_within_one_execute(ec):
+    """v = L*L assigned in the same execute as r2 += v*t2: the (alpha beta|beta alpha)
+    blocks of v get no task in the assignment (L vanishes between spins), so the
+    contraction skips them; the FP64 result is bit-identical to running the two ops in
+    separate executes (where nothing is known about v), split-INT8 within 1e-11."""
+    lad = W.ladder(4, 13, seed=11, tile_lo=3, tile_hi=6, ec=ec, build_v=False)
+    a, b, c, d, i, j = lad.labels
+    V = lad.V
+    CI = tb.TiledIndexSpace(tb.IndexSpace(40), 16)
+    q = CI.label()
+    L = tb.Tensor([CI, V, V], spin_mask=[2, 0, 1]).allocate(ec)
+    L.write(np.random.default_rng(3).normal(size=L.nelems))
+
+    def run(together, profile=True):
+        lad.sch(lad.r2().assign(0.0)).execute()
+        lad.sch(lad.v(a, b, c, d).assign(L(q, a, c) * L(q, b, d)))
+        if not together:
+            lad.sch.execute()
+        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute(tb.ExecutionHW.GPU, profile)
+        return lad.r2.read(), lad.sch.op_stats(-1)
+
+    apart, st0 = run(False)
+    joint, st1 = run(True)
+    assert st0["flops_run"] == st0["flops"]
+    assert st1["flops"] == st0["flops"] and st1["flops_run"] < st1["flops"]
+    assert np.array_equal(apart, joint)
+    ec.set_precision(tb.Precision.INT8, 1e-11)
+    try:
+        joint8, st8 = run(True)
+    finally:
+        ec.set_precision(tb.Precision.FP64)
+    assert st8["flops_run"] == st1["flops_run"]
+    assert rel_err(joint8, apart) <= 1e-11
