@@ -359,6 +359,40 @@ int tb_sched_release(tb_sched s);
 int tb_sched_dot(tb_sched s, int slot, double alpha, tb_labeled a, tb_labeled b);
 int tb_sched_norm(tb_sched s, int slot, double alpha, tb_labeled a);
 int tb_sched_scalars(tb_sched s, double* host, int n);
+/* Multi-factor product lhs (=|+=) alpha * F_0 * ... * F_(n-1) (TAMM's OpMin /
+ * OpExecutor, src/tamm/opmin.hpp:395-660, src/tamm/op_executor.hpp): the binary
+ * contraction tree of least cost under opmin::Optimizer's model (dynamic programming
+ * over factor subsets; a pair costs the product of the dense extents of the labels the
+ * two parts still need) is queued as Set(0) + Mult ops into intermediates over the
+ * needed labels (no spin symmetry; owned by the scheduler and reused when the same
+ * product is queued again), the root updating lhs.  n = 1 is an AddOp, n = 2 a MultOp. */
+int tb_sched_mult_n(tb_sched s, tb_labeled lhs, double alpha, const tb_labeled* factors, int n, int is_assign);
+/* The tree tb_sched_mult_n would run, host only: pairs[2k], pairs[2k+1] are the factor
+ * bit masks joined by the k-th binary contraction (execution order, n - 1 steps), and
+ * *cost the model's total. */
+int tb_opmin_order(tb_labeled lhs, const tb_labeled* factors, int n, int64_t* pairs, double* cost);
+
+/* MapOp family (src/tamm/mapop.hpp:28-120; Scheduler::exact_copy, scheduler.hpp:461-474;
+ * apply_ewise_ip / apply_ewise and their wrappers, tamm_utils.hpp:866-1100) on the
+ * device: lhs(labels) = f(rhs(labels)) element by element, over the blocks of lhs
+ * admitted in its label spaces; rhs carries the same labels in the same order (the
+ * same block ids, translated to its own tiled spaces as TAMM's translate_blockid) and
+ * may be lhs itself (in place).  A block of rhs that is not stored reads as zeros, as
+ * TAMM's get of a non-admitted block.  Device code cannot run a host lambda, so f is
+ * one of the element functions below (those of TAMM's apply_ewise wrappers), with
+ * parameter p where noted. */
+#define TB_MAP_COPY 0    /* x            (exact_copy) */
+#define TB_MAP_SCALE 1   /* p * x        (scale, scale_ip) */
+#define TB_MAP_SET 2     /* p            (set_val_ip) */
+#define TB_MAP_SQUARE 3  /* x * x        (square) */
+#define TB_MAP_SQRT 4    /* sqrt(x)      (sqrt) */
+#define TB_MAP_LOG 5     /* log(x)       (log) */
+#define TB_MAP_LOG10 6   /* log10(x)     (log10) */
+#define TB_MAP_INVERSE 7 /* 1 / x        (einverse) */
+#define TB_MAP_POW 8     /* pow(x, p)    (pow) */
+#define TB_MAP_ABS 9     /* |x| */
+int tb_sched_map(tb_sched s, tb_labeled lhs, tb_labeled rhs, int fn, double p);
+
 /* Orbital-energy denominator update of CC amplitudes (TAMM's jacobi_cc via
  * apply_ewise, tamm_utils.hpp:866-936): t += alpha * r / D element by element, with
  * D = sum over modes of signs[m] * eps[orbital index of mode m] (eps over the root

@@ -318,3 +318,63 @@ def fill_uniform(x, seed, first=0, lo=-1.0, hi=1.0):
 
 def fill_normal(x, seed, first=0, mean=0.0, sd=1.0):
     port().or_fill_normal(_dptr(x), x.size, seed, first, mean, sd)
+
+
+# ----------------------------------------------------------------------------- OpMin
+
+def _snoob(sub, full):
+    """Next larger subset of `full` with the same number of bits (the enumeration of
+    src/tamm/opmin.hpp:60-81); smaller than `sub` when the subsets of that size are
+    exhausted."""
+    low = sub & -sub
+    ripple = sub + low
+    if ripple > full:
+        return 0
+    ones = ((sub ^ ripple) >> 2) // low
+    return ripple | ones
+
+
+def opmin_order(factor_labels, lhs_labels, extent):
+    """opmin::Optimizer::optimize (src/tamm/opmin.hpp:438-477 with the callbacks at
+    :506-533): subsets of the n factors visited by size, then by value; available
+    labels of unions, required labels (available & (available of the rest | lhs)),
+    and the cheapest split of each subset, cost = product of the extents of
+    required(x) | required(y) plus the parts' costs, first strict improvement kept.
+    Returns ([(child1, child2) of each binary step, post order], total cost)."""
+    n = len(factor_labels)
+    full = (1 << n) - 1
+    visit = []
+    for k in range(1, n + 1):
+        x = (1 << k) - 1
+        while x and x <= full:
+            visit.append(x)
+            x = _snoob(x, full)
+    avail = {1 << i: frozenset(f) for i, f in enumerate(factor_labels)}
+    seen = []
+    for x in visit:
+        for y in seen:
+            avail[x | y] = avail[x] | avail[y]
+        seen.append(x)
+    lhs = frozenset(lhs_labels)
+    req = {x: avail[x] & (avail.get(full & ~x, frozenset()) | lhs) for x in visit}
+    cost = {x: (0.0 if bin(x).count("1") == 1 else float("inf")) for x in visit}
+    kids = {}
+    seen = []
+    for x in visit:
+        for y in seen:
+            if x & y:
+                continue
+            c = float(np.prod([extent[l] for l in req[x] | req[y]])) + cost[x] + cost[y]
+            if c < cost[x | y]:
+                cost[x | y] = c
+                kids[x | y] = (x, y)
+        seen.append(x)
+    steps = []
+
+    def walk(x):
+        if x in kids:
+            walk(kids[x][0])
+            walk(kids[x][1])
+            steps.append(kids[x])
+    walk(full)
+    return steps, (cost[full] if n > 1 else 0.0)

@@ -23,6 +23,9 @@ TB_ERR_STATE = 7
 TB_MODE_FP64 = 0
 TB_MODE_INT8 = 1
 TB_MODE_BF16X3 = 2
+# element functions of tb_sched_map
+TB_MAP_COPY, TB_MAP_SCALE, TB_MAP_SET, TB_MAP_SQUARE, TB_MAP_SQRT = 0, 1, 2, 3, 4
+TB_MAP_LOG, TB_MAP_LOG10, TB_MAP_INVERSE, TB_MAP_POW, TB_MAP_ABS = 5, 6, 7, 8, 9
 
 i64p = C.POINTER(C.c_int64)
 i32p = C.POINTER(C.c_int32)
@@ -109,6 +112,9 @@ PROTOS = {
     "tb_sched_execute": [h, C.c_int, C.c_int],
     "tb_sched_profile": [h, i64p, dp, dp, C.c_int64],
     "tb_sched_clear": [h],
+    "tb_sched_map": [h, tb_labeled, tb_labeled, C.c_int, C.c_double],
+    "tb_sched_mult_n": [h, tb_labeled, C.c_double, C.POINTER(tb_labeled), C.c_int, C.c_int],
+    "tb_opmin_order": [tb_labeled, C.POINTER(tb_labeled), C.c_int, i64p, dp],
     "tb_sched_release": [h],
     "tb_sched_op_stats": [h, C.c_int64, C.POINTER(tb_stats)],
     "tb_tensor_attach": [h, h, vp, C.c_int64],

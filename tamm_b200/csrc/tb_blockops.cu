@@ -347,6 +347,53 @@ void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double val
   TB_CUDA(cudaGetLastError());
 }
 
+__device__ __forceinline__ double map_fn(int fn, double x, double p) {
+  switch(fn) {
+    case TB_MAP_COPY: return x;
+    case TB_MAP_SCALE: return p * x;
+    case TB_MAP_SET: return p;
+    case TB_MAP_SQUARE: return x * x;
+    case TB_MAP_SQRT: return sqrt(x);
+    case TB_MAP_LOG: return log(x);
+    case TB_MAP_LOG10: return log10(x);
+    case TB_MAP_INVERSE: return 1.0 / x;
+    case TB_MAP_POW: return pow(x, p);
+    default: return fabs(x);
+  }
+}
+
+// Element function over a list of blocks: a CTA row (blockIdx.y) per block, 16-byte
+// accesses where both sides are aligned.
+__global__ void __launch_bounds__(kThreads) k_map_blocks(double* __restrict__ dst, const double* __restrict__ src,
+                                                         const int64_t* __restrict__ tri, int nblocks, int fn,
+                                                         double p) {
+  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
+    double* const       d      = dst + tri[3 * blk];
+    const int64_t       so     = tri[3 * blk + 1];
+    const double* const sp     = so >= 0 ? src + so : nullptr;
+    const int64_t       n      = tri[3 * blk + 2];
+    const int64_t       stride = (int64_t) gridDim.x * blockDim.x * 2;
+    for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
+      const bool vec = i + 1 < n && ((reinterpret_cast<uintptr_t>(d + i) & 15) == 0) &&
+                       (sp == nullptr || (reinterpret_cast<uintptr_t>(sp + i) & 15) == 0);
+      if(vec) {
+        const double2 x = sp ? *reinterpret_cast<const double2*>(sp + i) : make_double2(0.0, 0.0);
+        *reinterpret_cast<double2*>(d + i) = make_double2(map_fn(fn, x.x, p), map_fn(fn, x.y, p));
+      }
+      else
+        for(int64_t j = i; j < i + 2 && j < n; j++) d[j] = map_fn(fn, sp ? sp[j] : 0.0, p);
+    }
+  }
+}
+
+void launch_map_blocks(double* dst, const double* src, const int64_t* triples, int nblocks, int fn, double p,
+                       cudaStream_t stream) {
+  if(nblocks <= 0) return;
+  const dim3 grid(8, (unsigned) std::min(nblocks, 4096));
+  k_map_blocks<<<grid, kThreads, 0, stream>>>(dst, src, triples, nblocks, fn, p);
+  TB_CUDA(cudaGetLastError());
+}
+
 // One pass over the blocks of a read-only tensor: a CTA row (blockIdx.y) per block,
 // 16-byte loads where aligned, one OR per CTA that saw a nonzero element.
 __global__ void __launch_bounds__(kThreads) k_block_nonzero(const double* __restrict__ x,

@@ -879,6 +879,46 @@ int tb_sched_add(tb_sched s, tb_labeled lhs, double alpha, tb_labeled rhs, int i
   TB_API_END
 }
 
+int tb_sched_mult_n(tb_sched s, tb_labeled lhs, double alpha, const tb_labeled* factors, int n, int is_assign) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && factors != nullptr && n >= 1);
+  std::vector<Labeled> f;
+  for(int i = 0; i < n; i++) f.push_back(to_labeled(factors[i]));
+  std::vector<Op> queued;
+  queue_mult_n(*s->p, to_labeled(lhs), alpha, f, is_assign, [&](Op&& op) { queued.push_back(std::move(op)); });
+  for(auto& op: queued) s->p->ops.push_back(std::move(op)); // all or nothing
+  TB_API_END
+}
+
+int tb_opmin_order(tb_labeled lhs, const tb_labeled* factors, int n, int64_t* pairs, double* cost) {
+  TB_API_BEGIN
+  REQUIRE_ARG(factors != nullptr && n >= 1);
+  std::vector<Labeled> f;
+  for(int i = 0; i < n; i++) f.push_back(to_labeled(factors[i]));
+  std::vector<int64_t> p;
+  double               c = 0;
+  mult_n_order(to_labeled(lhs), f, p, c);
+  if(pairs) std::copy(p.begin(), p.end(), pairs);
+  if(cost) *cost = c;
+  TB_API_END
+}
+
+int tb_sched_map(tb_sched s, tb_labeled lhs, tb_labeled rhs, int fn, double p) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr);
+  TB_EXPECTS(fn >= TB_MAP_COPY && fn <= TB_MAP_ABS, "unknown element function (TB_MAP_*)");
+  Op op;
+  op.kind  = Op::Map;
+  op.lhs   = to_labeled(lhs);
+  op.a     = to_labeled(rhs);
+  op.fn    = fn;
+  op.value = p;
+  if(op.lhs.labels != op.a.labels)
+    fail(TB_ERR_NOT_IMPLEMENTED, "map: rhs must carry the lhs labels in the same order (no permutation)");
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
 int tb_sched_mult(tb_sched s, tb_labeled lhs, double alpha, tb_labeled a, tb_labeled b,
                   int is_assign) {
   TB_API_BEGIN

@@ -161,6 +161,10 @@ void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double val
                         cudaStream_t stream);
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream);
+// For each (dst offset, src offset or -1, n) triple of a device array:
+// dst[0:n) = f(src[0:n)) with f = TB_MAP_* and parameter p (src -1: zeros).
+void launch_map_blocks(double* dst, const double* src, const int64_t* triples, int nblocks, int fn, double p,
+                       cudaStream_t stream);
 double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream);
 // *out = scale * x.y (root: scale * sqrt(x.x)), staying on the device; part holds
 // 1024 doubles of scratch.  y == nullptr means x.x.

@@ -434,6 +434,7 @@ std::string signature(const Op& op) {
     os << "|";
   };
   os << (int) op.kind << "|";
+  if(op.kind == Op::Map) os << "f" << op.fn << "|";
   put(op.lhs);
   if(op.kind != Op::Set) put(op.a);
   if(op.kind == Op::Mult) put(op.b);
@@ -592,8 +593,56 @@ void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A,
 
 void Sched::run(Op& op) {
   cudaStream_t st = ctx->stream;
-  if(op.kind == Op::Set || op.kind == Op::Add || op.kind == Op::Mult || op.kind == Op::Denom)
+  if(op.kind == Op::Set || op.kind == Op::Add || op.kind == Op::Mult || op.kind == Op::Denom || op.kind == Op::Map)
     op.lhs.t->require_writable();
+  if(op.kind == Op::Map) {
+    op.lhs.t->require_allocated();
+    op.a.t->require_allocated();
+    if(!op.map_dev) {
+      const std::string key = "M|" + signature(op);
+      auto&             cached = fill_cache[key];
+      auto&             count  = map_count[key];
+      if(!cached) {
+        // MapOp's loop over the lhs label tuples (mapop.hpp:52-90): every admitted lhs
+        // block, the rhs block with the same label tiles (or zeros where not stored)
+        auto                 lm = tile_maps(op.lhs), rm = tile_maps(op.a);
+        std::vector<int64_t> nt, it(op.lhs.t->nmodes, 0), lid(op.lhs.t->nmodes), rid(op.a.t->nmodes), tri;
+        for(int i = 0; i < op.lhs.t->nmodes; i++) nt.push_back(op.lhs.ltis[i]->ntiles());
+        bool empty = false;
+        for(auto n: nt) empty |= (n == 0);
+        if(!empty) do {
+            for(int i = 0; i < op.lhs.t->nmodes; i++) {
+              lid[i] = lm[i][it[i]];
+              rid[i] = rm[i][it[i]];
+            }
+            if(!op.lhs.t->is_non_zero(lid.data())) continue;
+            const int64_t n = op.lhs.t->block_size(lid.data());
+            TB_EXPECTS(op.a.t->block_size(rid.data()) == n, "map: lhs and rhs blocks differ in size");
+            tri.push_back(op.lhs.t->locate(lid.data()));
+            tri.push_back(op.a.t->is_non_zero(rid.data()) ? op.a.t->locate(rid.data()) : -1);
+            tri.push_back(n);
+          } while(!it.empty() && next_tuple(it, nt));
+        TB_EXPECTS(tri.size() / 3 < (1u << 31), "too many blocks in one map");
+        int64_t*  d   = nullptr;
+        const int dev = ctx->device;
+        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * std::max<size_t>(tri.size(), 1)));
+        cached = std::shared_ptr<int64_t>(d, [dev](int64_t* q) {
+          int cur = -1;
+          cudaGetDevice(&cur);
+          cudaSetDevice(dev);
+          cudaFree(q);
+          if(cur >= 0) cudaSetDevice(cur);
+        });
+        if(!tri.empty())
+          TB_CUDA(cudaMemcpy(d, tri.data(), sizeof(int64_t) * tri.size(), cudaMemcpyHostToDevice));
+        count = (int) (tri.size() / 3);
+      }
+      op.map_dev = cached;
+      op.map_n   = count;
+    }
+    launch_map_blocks(op.lhs.t->data, op.a.t->data, op.map_dev.get(), op.map_n, op.fn, op.value, st);
+    return;
+  }
   if(op.kind == Op::Set) {
     op.lhs.t->require_allocated();
     if(op.fill_none) return;
@@ -900,11 +949,13 @@ double* Sched::scalars() {
 }
 
 Sched::~Sched() {
-  if(d_scalars) {
+  if(d_scalars || !temps.empty()) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(d_scalars);
   }
+  if(d_scalars) cudaFree(d_scalars);
+  for(auto& kv: temps)
+    if(kv.second && kv.second->data) ctx->arena->deallocate(kv.second->data);
 }
 
 // Block table of a denominator op over t's admitted blocks: packed offset, dims and

@@ -5,6 +5,7 @@
 
 #include "tb_internal.hpp"
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -145,7 +146,8 @@ struct Op {
   // Dot: scalar slot `slot` = alpha * sum a * b (root: alpha * sqrt(sum a * a)), kept on
   // the device; Denom: lhs += alpha * a / D with the orbital-energy denominator D.
   // DenomEnergy: slot += alpha * sum lhs^2 / D; SetScalar: slot = value.
-  enum Kind { Set, Add, Mult, Dot, Denom, DenomEnergy, SetScalar } kind;
+  // Map: lhs = f(a) element by element (f = TB_MAP_* in `fn`, parameter `value`).
+  enum Kind { Set, Add, Mult, Dot, Denom, DenomEnergy, SetScalar, Map } kind;
   Labeled lhs, a, b;
   double  alpha = 1.0, value = 0.0;
   int     is_assign = 0;
@@ -160,6 +162,9 @@ struct Op {
     int64_t ddims[kMaxModes], sdims[kMaxModes];
   };
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
+  int                                    fn = 0;     // Map: element function
+  std::shared_ptr<int64_t>               map_dev;    // Map: device (dst, src, n) triples
+  int                                    map_n = 0;  // number of triples
   bool                                   flat = false;
   std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
   std::shared_ptr<int64_t>               set_dev;    // device copy of set_blocks (from the scheduler's cache)
@@ -211,6 +216,10 @@ struct Sched {
   // device block lists of SetOps over some of a tensor's blocks, by the op's signature
   // (or, for the fill of a fused assignment, its contraction's), uploaded once
   std::map<std::string, std::shared_ptr<int64_t>>  fill_cache;
+  std::map<std::string, int>                        map_count; // triples of each cached map list
+  // intermediates of multi-factor products (tb_sched_mult_n), by signature; freed with
+  // the scheduler
+  std::map<std::string, std::unique_ptr<Tensor>>    temps;
   static constexpr int                              kSlots = 64;
   double*                                           d_scalars = nullptr; // kSlots + 1024 partials
   bool                                              autotune  = false;
@@ -228,6 +237,11 @@ struct Sched {
   double*                                           scalars();
   ~Sched();
 };
+
+// Multi-factor products (tb_opmin.cpp): queue as binary contractions; the chosen tree.
+void queue_mult_n(Sched& s, const Labeled& lhs, double alpha, const std::vector<Labeled>& f, int is_assign,
+                  const std::function<void(Op&&)>& push);
+void mult_n_order(const Labeled& lhs, const std::vector<Labeled>& f, std::vector<int64_t>& pairs, double& cost);
 
 // A captured sequence of scheduler ops: replayed with one graph launch.  Holds the
 // scratch the capture used and the work lists whose error words are checked.

@@ -472,6 +472,20 @@ public:
     return *this;
   }
 
+  // MapOp family: lhs = fn(rhs) element by element (TB_MAP_*; rhs has lhs's labels,
+  // may be lhs itself); exact_copy (Scheduler::exact_copy, scheduler.hpp:461).
+  Scheduler& map(const LabeledTensorBase& lhs, const LabeledTensorBase& rhs, int fn, double p = 0.0) {
+    std::map<std::string, int> ids;
+    std::vector<Lowered>       keep;
+    tb_labeled                 l = lower(lhs, ids, keep);
+    tb_labeled                 r = lower(rhs, ids, keep);
+    check(tb_sched_map(h_.get(), l, r, fn, p));
+    return *this;
+  }
+  Scheduler& exact_copy(const LabeledTensorBase& lhs, const LabeledTensorBase& rhs) {
+    return map(lhs, rhs, TB_MAP_COPY);
+  }
+
   void execute(ExecutionHW hw = ExecutionHW::DEFAULT, bool profile = false) {
     check(tb_sched_execute(h_.get(), static_cast<int>(hw), profile ? 1 : 0));
   }

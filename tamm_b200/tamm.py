@@ -39,6 +39,12 @@ class Precision:
     BF16X3 = A.TB_MODE_BF16X3
 
 
+class Map:
+    """Element functions of Scheduler.map (TAMM's apply_ewise wrappers)."""
+    COPY, SCALE, SET, SQUARE, SQRT = A.TB_MAP_COPY, A.TB_MAP_SCALE, A.TB_MAP_SET, A.TB_MAP_SQUARE, A.TB_MAP_SQRT
+    LOG, LOG10, INVERSE, POW, ABS = A.TB_MAP_LOG, A.TB_MAP_LOG10, A.TB_MAP_INVERSE, A.TB_MAP_POW, A.TB_MAP_ABS
+
+
 def _i64arr(v):
     a = np.ascontiguousarray(np.asarray(list(v) if not isinstance(v, np.ndarray) else v, dtype=np.int64))
     return a if a.size else np.zeros(1, dtype=np.int64)
@@ -459,6 +465,11 @@ def _to_c_labeled(lt: LabeledTensor, ids: dict, keep: list):
     return A.tb_labeled(lt.tensor.h, C.cast(lab, A.ip), C.cast(sp, C.POINTER(A.h)))
 
 
+def apply_ewise_ip(lt: LabeledTensor, fn: int, p: float = 0.0):
+    """apply_ewise_ip (tamm_utils.hpp:866): lt = fn(lt) in place, run now on lt's context."""
+    Scheduler(lt.tensor.ec).map(lt, lt, fn, p).execute()
+
+
 def mult_info(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor):
     """(admitted output blocks, admitted block triples, FP64 FLOPs) of lhs += a * b,
     computed on the host without running anything."""
@@ -468,6 +479,19 @@ def mult_info(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor):
     ng, nt, fl = C.c_int64(), C.c_int64(), C.c_double()
     call("tb_mult_info", l, x, y, C.byref(ng), C.byref(nt), C.byref(fl))
     return ng.value, nt.value, fl.value
+
+
+def opmin_order(lhs: LabeledTensor, *factors: LabeledTensor):
+    """The binary steps lhs = prod(factors) runs as: [(mask, mask), ...] of factor bits in
+    execution order, and the OpMin model's total cost (host only)."""
+    ids: dict = {}
+    keep: list = []
+    l = _to_c_labeled(lhs, ids, keep)
+    fs = (A.tb_labeled * len(factors))(*[_to_c_labeled(f, ids, keep) for f in factors])
+    pairs = np.zeros(max(2 * (len(factors) - 1), 1), dtype=np.int64)
+    cost = C.c_double()
+    call("tb_opmin_order", l, fs, len(factors), pairs.ctypes.data_as(A.i64p), C.byref(cost))
+    return [(int(pairs[2 * k]), int(pairs[2 * k + 1])) for k in range(len(factors) - 1)], cost.value
 
 
 def mult_owned(lhs: LabeledTensor, a: LabeledTensor, b: LabeledTensor, rank: int, nranks: int):
@@ -525,8 +549,10 @@ class Scheduler:
             a = self._labeled(rhs.factors[0], ids)
             b = self._labeled(rhs.factors[1], ids)
             call("tb_sched_mult", self.h, lhs, alpha, a, b, int(spec.is_assign))
-        else:
-            raise ValueError("a TAMM op has at most two tensor factors")
+        else:  # OpMin: the cheapest binary contraction tree, run through intermediates
+            fs = (A.tb_labeled * len(rhs.factors))(*[self._labeled(f, ids) for f in rhs.factors])
+            self._keep.append(fs)
+            call("tb_sched_mult_n", self.h, lhs, alpha, fs, len(rhs.factors), int(spec.is_assign))
         return self
 
     def execute(self, hw=ExecutionHW.DEFAULT, profile=False):
@@ -576,6 +602,17 @@ class Scheduler:
         call("tb_sched_denom", self.h, self._labeled(t, ids), float(alpha), self._labeled(r, ids),
              e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
         return self
+
+    def map(self, lhs: LabeledTensor, rhs: LabeledTensor, fn: int, p: float = 0.0):
+        """Queue lhs = fn(rhs) element by element over lhs's admitted blocks (MapOp; rhs has
+        lhs's labels in the same order and may be lhs itself)."""
+        ids: dict = {}
+        call("tb_sched_map", self.h, self._labeled(lhs, ids), self._labeled(rhs, ids), int(fn), float(p))
+        return self
+
+    def exact_copy(self, lhs: LabeledTensor, rhs: LabeledTensor):
+        """Scheduler::exact_copy: lhs's blocks = rhs's blocks with the same tile ids."""
+        return self.map(lhs, rhs, Map.COPY)
 
     def clear(self):
         """Drop the queued ops without running them (e.g. after an execute failed)."""
