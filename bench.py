@@ -438,7 +438,7 @@ def main():
         ccsd_line = {"workload": f"ccsd_doubles_iteration_O{2 * args.ccsd_oa}_V{2 * args.ccsd_va}",
                      "unit": "TFLOP/s (admitted FP64 FLOPs of the iteration's contractions / graph replay time)",
                      "flops": P.flops, "ops_per_iteration": len(CC._ops(P)) + 3,
-                     "ladder_batches": len(P.batches), **res}
+                     "ladder_batches": P.ladder_batches, **res}
         del P
     if world > 1:
         dist.barrier()

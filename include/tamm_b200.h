@@ -262,6 +262,40 @@ int tb_tensor_locate(tb_tensor t, const int64_t* blockid, int64_t* offset);
  * in stream order can share one buffer, e.g. the batches of an integral tensor
  * built on demand.  tb_tensor_deallocate detaches it without freeing. */
 int tb_tensor_attach(tb_tensor t, tb_ctx ctx, void* device_ptr, int64_t bytes);
+/* Lambda tensors (Tensor<T>(tis, Func), src/tamm/tensor.hpp:166-190, whose
+ * LambdaTensorImpl computes a block on request, src/tamm/tensor_impl.hpp:566-693): a
+ * tensor without storage whose blocks are produced on demand.  A contraction that
+ * reads it (either operand) is run in batches along the lambda tensor's first mode:
+ * the tiles of that mode's label space are cut into consecutive ranges whose admitted
+ * blocks fit the batch budget (tb_tensor_set_batch_bytes; default a quarter of the
+ * context arena's free bytes), each range is materialised into scratch on the context's
+ * stream and contracted with the label restricted to those tiles, then released.
+ *  - tb_tensor_create_lambda: fn fills ONE block (TAMM's lambda): blockid in the
+ *    tensor's own tile numbering, its dims, and a device buffer of n doubles that fn
+ *    must fill with work enqueued on `stream` (or before returning); nonzero return
+ *    aborts the op with TB_ERR_INVALID.
+ *  - tb_tensor_create_built: fn fills a whole batch at once (no counterpart in TAMM):
+ *    `batch` is an allocated tensor over tiles [first_tile, last_tile) of the first
+ *    mode's label space and the full other modes, and fn queues ops writing it on
+ *    `sch` (a scheduler on the same context, executed right after fn returns), e.g.
+ *    batch(a',b,c,d) = L(Q,a',c) * L(Q,b,d) for integrals built from Cholesky vectors.
+ * Only contractions read lambda tensors (other ops fail with TB_ERR_NOT_IMPLEMENTED);
+ * a graph capture records the callbacks' device work, so they must only enqueue work
+ * on the stream they are given. */
+typedef struct tb_sched_s* tb_sched; /* Scheduler handle (declared with its calls below) */
+typedef int (*tb_block_fn)(const int64_t* blockid, int nmodes, const int64_t* dims, double* block, int64_t n,
+                           void* stream, void* user);
+typedef int (*tb_batch_fn)(tb_tensor batch, int64_t first_tile, int64_t last_tile, tb_sched sch, void* user);
+int tb_tensor_create_lambda(int nmodes, const tb_tis* tis, const int* spin_mask, tb_block_fn fn, void* user,
+                            tb_tensor* out);
+int tb_tensor_create_built(int nmodes, const tb_tis* tis, const int* spin_mask, tb_batch_fn fn, void* user,
+                           tb_tensor* out);
+/* Device bytes one batch of a lambda tensor may take (0: a quarter of the free arena). */
+int tb_tensor_set_batch_bytes(tb_tensor t, int64_t bytes);
+/* A new handle to the tiled space of mode `mode` of t (destroy with tb_tis_destroy),
+ * e.g. the first-mode tile range of a lambda tensor's batch. */
+int tb_tensor_space(tb_tensor t, int mode, tb_tis* out);
+
 /* Tensor::get / put / add of one block with a HOST buffer of n >= block size
  * (tensor_impl.hpp:321-455; get of a non-admitted block returns zeros). */
 int tb_tensor_get(tb_tensor t, const int64_t* blockid, double* host, int64_t n);
@@ -303,7 +337,6 @@ typedef struct tb_labeled {
 
 /* Scheduler (src/tamm/scheduler.hpp:40-51,160-438): ops are queued with
  * operator() and run by execute() in dependence levels on the context's stream. */
-typedef struct tb_sched_s* tb_sched;
 int tb_sched_create(tb_ctx ctx, tb_sched* out);
 int tb_sched_destroy(tb_sched s);
 /* SetOp: lhs = value (is_assign) or lhs += value. */

@@ -41,6 +41,11 @@ class tb_stats(C.Structure):
                 ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int), ("flops_run", C.c_double)]
 
 
+# callbacks of lambda tensors (tb_block_fn, tb_batch_fn)
+BLOCK_FN = C.CFUNCTYPE(C.c_int, i64p, C.c_int, i64p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+BATCH_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p)
+
+
 class tb_labeled(C.Structure):
     _fields_ = [("tensor", h), ("labels", ip), ("label_tis", C.POINTER(h))]
 
@@ -92,6 +97,10 @@ PROTOS = {
     "tb_tensor_data": [h, C.POINTER(vp)],
     "tb_tensor_set_read_only": [h, C.c_int],
     "tb_tensor_record_use": [h],
+    "tb_tensor_create_lambda": [C.c_int, C.POINTER(h), ip, C.c_void_p, C.c_void_p, C.POINTER(h)],
+    "tb_tensor_create_built": [C.c_int, C.POINTER(h), ip, C.c_void_p, C.c_void_p, C.POINTER(h)],
+    "tb_tensor_set_batch_bytes": [h, C.c_int64],
+    "tb_tensor_space": [h, C.c_int, C.POINTER(h)],
     "tb_tensor_read_only_info": [h, ip, i64p, i64p],
     "tb_tensor_is_non_zero": [h, i64p, ip],
     "tb_tensor_block_size": [h, i64p, i64p],

@@ -20,9 +20,11 @@ as TAMM builds it with a lambda tensor (Test_CCSD.cpp:300-488):
 
 with v(a,b,i,j) = sum_Q L(Q,a,i) L(Q,b,j) (and v(c,d,k,l) the same tensor read as
 (oo|vv)), v_oooo and v_ovvo likewise from the Cholesky vectors.  Every tensor is
-spin-blocked with TAMM's sum rule.  The particle ladder runs in batches of virtual
-tiles: a batch builds v(a',b,c,d) for its tiles a' into one shared buffer and
-contracts it with t2, so v(a,b,c,d) is never stored whole.
+spin-blocked with TAMM's sum rule.  v(a,b,c,d) is a lambda tensor built on demand
+(tb_tensor_create_built): the ladder is one op, r2 += 1/2 v(a,b,c,d) t2(c,d,i,j), and
+the scheduler runs it in batches of the virtual tiles of a, each batch
+v(a',b,c,d) = L(Q,a',c) L(Q,b,d) materialised into scratch, contracted and released,
+so v is never stored whole.
 
     python -m tamm_b200.ccsd [--oa 30 --va 240 --seed 2 --tile-lo 20 --tile-hi 64]
 """
@@ -51,9 +53,8 @@ class CCSDProblem:
     V: TiledIndexSpace
     CI: TiledIndexSpace
     eps: np.ndarray                     # orbital energies over the MO space
-    T: dict                             # name -> Tensor
-    batches: list                       # (virtual sub-space of a', tensor v(a',b,c,d))
-    batch_buffer: object                # torch tensor holding the shared batch storage
+    T: dict                             # name -> Tensor (v_vvvv: the lambda tensor)
+    ladder_batches: int                 # batches the particle ladder runs in
     flops: dict = field(default_factory=dict)
 
 
@@ -119,24 +120,36 @@ def build(oa: int, va: int, seed: int = 2, tile_lo: int = 20, tile_hi: int = 64,
     sch(T["t2"]().assign(0.0))
     sch.denom(T["t2"](a, b, i, j), -1.0, T["v_vvoo"](a, b, i, j), eps, [1, 1, -1, -1])
     sch.execute(ExecutionHW.GPU)
-    # particle-ladder batches over the virtual tiles, sharing one buffer
-    nv = V.num_tiles
-    batches, most = [], 0
-    for first in range(0, nv, batch_tiles):
-        Vs = V.sub(first, min(first + batch_tiles, nv))
-        vb = Tensor([Vs, V, V, V], spin=(2, 2))
-        batches.append((Vs, vb))
-        most = max(most, vb.nelems)
-    buf = torch.empty(max(most, 1) * 8 + 256, dtype=torch.uint8, device=f"cuda:{ec.device}")
-    base = (buf.data_ptr() + 255) // 256 * 256
-    for _, vb in batches:
-        vb.attach(ec, base, max(most, 1) * 8)
+    # v(a,b,c,d) built on demand in batches of the virtual tiles of a, `batch_tiles`
+    # tiles' worth of blocks per batch
+    q2 = CI.label()
+
+    def build_batch(batch, first, last, bsch):
+        ap = batch.spaces[0].label()
+        b2, c2, d2 = V.labels(3)
+        bsch(batch(ap, b2, c2, d2).assign(T["L_vv"](q2, ap, c2) * T["L_vv"](q2, b2, d2)))
+
+    shape = Tensor([V, V, V, V], spin=(2, 2))  # host-only: the block table of v
+    keys, offs = shape.block_table()
+    stride = V.num_tiles ** 3
+    per_tile = np.zeros(V.num_tiles, dtype=np.int64)
+    ends = np.append(offs[1:], shape.nelems)
+    for k, o, e in zip(keys.tolist(), offs.tolist(), ends.tolist()):
+        per_tile[k // stride] += e - o
+    batch_bytes = 8 * int(max(per_tile[x:x + batch_tiles].sum() for x in range(V.num_tiles)))
+    T["v_vvvv"] = Tensor.built([V, V, V, V], build_batch, spin=(2, 2), batch_bytes=batch_bytes)
+    nb, acc = 0, None
+    for x in range(V.num_tiles):  # the scheduler's greedy cut of the first mode's tiles
+        if acc is None or acc + 8 * per_tile[x] > batch_bytes:
+            nb, acc = nb + 1, 8 * int(per_tile[x])
+        else:
+            acc += 8 * int(per_tile[x])
     # the integrals and Fock matrices stay constant through the iterations: marked
     # read-only, their exactly-zero spin blocks (e.g. v(a,b,i,j) with spin(a) != spin(i))
     # are skipped by the contractions that read them
     for name in ("L_vo", "L_oo", "L_vv", "f_oo", "f_vv", "v_vvoo", "v_oooo", "v_ovvo"):
         T[name].set_read_only(True)
-    P = CCSDProblem(ec, MO, O, V, CI, eps, T, batches, buf)
+    P = CCSDProblem(ec, MO, O, V, CI, eps, T, nb)
     P.flops = iteration_flops(P)
     return P
 
@@ -167,27 +180,26 @@ def _ops(P: CCSDProblem):
         (r2(a, b, i, j), -1.0, [X(a, b, j, i)], False),
         (r2(a, b, i, j), 1.0, [X(b, a, j, i)], False),
     ]
-    for Vs, vb in P.batches:
-        ap = Vs.label()
-        ops.append((vb(ap, b, c, d), 1.0, [T["L_vv"](q, ap, c), T["L_vv"](q, b, d)], True))
-        ops.append((r2(ap, b, i, j), 0.5, [vb(ap, b, c, d), t2(c, d, i, j)], False))
+    ops.append((r2(a, b, i, j), 0.5, [T["v_vvvv"](a, b, c, d), t2(c, d, i, j)], False))
     return ops
 
 
 def iteration_flops(P: CCSDProblem) -> dict:
-    """Admitted FP64 FLOPs of the iteration's contractions (the ladder batches' v
-    builds listed apart)."""
-    total, build, ladder = 0.0, 0.0, 0.0
-    for n, (lhs, _, f, _) in enumerate(_ops(P)):
+    """Admitted FP64 FLOPs of the iteration's contractions, with the particle ladder and
+    the on-demand build of its integrals v(a,b,c,d) = L(Q,a,c) L(Q,b,d) listed apart."""
+    total, ladder = 0.0, 0.0
+    ops = _ops(P)
+    for n, (lhs, _, f, _) in enumerate(ops):
         if len(f) == 2:
             fl = mult_info(lhs, f[0], f[1])[2]
             total += fl
-            if n >= 19:
-                if n % 2 == 1:
-                    build += fl
-                else:
-                    ladder += fl
-    return {"contractions": total, "ladder": ladder, "v_build": build}
+            if n == len(ops) - 1:
+                ladder = fl
+    a, b, c, d = P.V.labels(4)
+    q = P.CI.label()
+    shape = Tensor([P.V, P.V, P.V, P.V], spin=(2, 2))
+    build = mult_info(shape(a, b, c, d), P.T["L_vv"](q, a, c), P.T["L_vv"](q, b, d))[2]
+    return {"contractions": total + build, "ladder": ladder, "v_build": build}
 
 
 def queue_iteration(P: CCSDProblem, sch: Scheduler):
@@ -301,7 +313,7 @@ def main(argv=None):
     ec = ExecutionContext(0, args.pool_gib << 30)
     P = build(args.oa, args.va, seed=args.seed, tile_lo=args.tile_lo, tile_hi=args.tile_hi, ec=ec)
     out = {"workload": f"ccsd_doubles_iteration_O{2 * args.oa}_V{2 * args.va}", "flops": P.flops,
-           "ops_per_iteration": len(_ops(P)) + 3, "ladder_batches": len(P.batches)}
+           "ops_per_iteration": len(_ops(P)) + 3, "ladder_batches": P.ladder_batches}
     out.update(measure(P, args.iters, tuple(args.modes.split(","))))
     print(json.dumps(out))
 

@@ -493,6 +493,46 @@ int tb_tensor_create(int nmodes, const tb_tis* tis, const int* spin_mask, tb_ten
   TB_API_END
 }
 
+int tb_tensor_create_lambda(int nmodes, const tb_tis* tis, const int* spin_mask, tb_block_fn fn, void* user,
+                            tb_tensor* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(out != nullptr && fn != nullptr);
+  tb_tensor t          = new_tensor(nmodes, tis, spin_mask);
+  t->p->lambda_block   = fn;
+  t->p->lambda_user    = user;
+  *out                 = t;
+  TB_API_END
+}
+
+int tb_tensor_create_built(int nmodes, const tb_tis* tis, const int* spin_mask, tb_batch_fn fn, void* user,
+                           tb_tensor* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(out != nullptr && fn != nullptr);
+  tb_tensor t          = new_tensor(nmodes, tis, spin_mask);
+  t->p->lambda_batch   = fn;
+  t->p->lambda_user    = user;
+  *out                 = t;
+  TB_API_END
+}
+
+int tb_tensor_space(tb_tensor t, int mode, tb_tis* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr && out != nullptr);
+  TB_EXPECTS(mode >= 0 && mode < t->p->nmodes, "mode out of range");
+  auto* h = new tb_tis_s();
+  h->p    = t->p->tis[mode];
+  *out    = h;
+  TB_API_END
+}
+
+int tb_tensor_set_batch_bytes(tb_tensor t, int64_t bytes) {
+  TB_API_BEGIN
+  REQUIRE_ARG(t != nullptr);
+  TB_EXPECTS(bytes >= 0, "negative batch size");
+  t->p->batch_bytes = bytes;
+  TB_API_END
+}
+
 int tb_tensor_create_spin_sizes(int nmodes, const tb_tis* tis, int nupper, int nlower,
                                 tb_tensor* out) {
   TB_API_BEGIN
@@ -510,6 +550,7 @@ int tb_tensor_allocate(tb_tensor t, tb_ctx ctx) {
   TB_API_BEGIN
   REQUIRE_ARG(t != nullptr && ctx != nullptr);
   if(t->p->data != nullptr) fail(TB_ERR_STATE, "tensor already allocated");
+  if(t->p->is_lambda()) fail(TB_ERR_STATE, "a lambda tensor has no storage of its own");
   TB_CUDA(cudaSetDevice(ctx->p->device));
   t->p->data = static_cast<double*>(ctx->p->arena->allocate(sizeof(double) * std::max<int64_t>(t->p->nelems, 1)));
   t->p->ctx  = ctx->p;
@@ -1204,9 +1245,11 @@ int tb_sched_graph_create(tb_sched s, tb_graph* out) {
   TB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
   for(size_t i = first; i < S.ops.size(); i++)
     if(S.ops[i].kind == Op::Mult) {
-      g->int8_lists.push_back(S.ops[i].wl);
+      if(S.ops[i].wl) g->int8_lists.push_back(S.ops[i].wl);
       g->plans.push_back(S.ops[i].plan);
     }
+  for(auto& wl: S.batch_lists) g->int8_lists.push_back(wl); // lambda batches
+  S.batch_lists.clear();
   auto* h = new tb_graph_s();
   h->p    = std::move(g);
   *out    = h;

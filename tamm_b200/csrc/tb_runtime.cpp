@@ -326,6 +326,8 @@ void Tensor::check_blockid(const int64_t* blockid) const {
 }
 
 void Tensor::require_allocated() const {
+  if(is_lambda() && data == nullptr)
+    fail(TB_ERR_NOT_IMPLEMENTED, "a lambda tensor can only be read by a contraction (its blocks exist on demand)");
   if(data == nullptr && nelems > 0) fail(TB_ERR_STATE, "tensor is not allocated");
 }
 
@@ -786,6 +788,10 @@ void Sched::run(Op& op) {
     return;
   }
   // MultOp
+  if(op.a.t->is_lambda() || op.b.t->is_lambda()) {
+    run_lambda_mult(op);
+    return;
+  }
   op.lhs.t->require_allocated();
   op.a.t->require_allocated();
   op.b.t->require_allocated();
@@ -1022,6 +1028,149 @@ Graph::~Graph() {
   pool.release();
 }
 
+// A contraction with a lambda operand, batch by batch along the lambda tensor's first
+// mode (see tb_tensor_create_lambda): consecutive tiles of that mode's label space
+// whose admitted blocks fit the batch budget are materialised into scratch (one batch
+// tensor per range, cached with the scheduler so that plans and work lists are too),
+// the contraction runs over them with the first-mode label restricted to those tiles
+// in every operand, and the scratch is released in stream order.
+void Sched::run_lambda_mult(Op& op) {
+  TB_EXPECTS(!(op.a.t->is_lambda() && op.b.t->is_lambda()), "a contraction of two lambda tensors is not supported");
+  const bool on_a = op.a.t->is_lambda();
+  Labeled&   X    = on_a ? op.a : op.b;
+  Tensor&    L    = *X.t;
+  TB_EXPECTS(L.nmodes >= 1, "a lambda tensor needs at least one mode");
+  op.lhs.t->require_allocated();
+  (on_a ? op.b : op.a).t->require_allocated();
+  const int                   lab0 = X.labels[0];
+  const std::shared_ptr<TIS>& sp0  = X.ltis[0];
+  // elements of L's stored blocks per tile of the first mode's label space
+  std::vector<int64_t> of_tile(L.tis[0]->ntiles(), -1); // L tile -> index in sp0
+  for(int64_t k = 0; k < sp0->ntiles(); k++) {
+    const int64_t t = L.tis[0]->find_root(sp0->tiles[k]);
+    TB_EXPECTS(t >= 0, "label tile is not a tile of the lambda tensor's index space");
+    of_tile[t] = k;
+  }
+  std::vector<int64_t> per(sp0->ntiles(), 0);
+  for(size_t b = 0; b < L.keys.size(); b++) {
+    const int64_t t0 = L.keys[b] / L.key_stride[0];
+    const int64_t n  = (b + 1 < L.keys.size() ? L.offsets[b + 1] : L.nelems) - L.offsets[b];
+    if(of_tile[t0] >= 0) per[of_tile[t0]] += n;
+  }
+  const int64_t budget = L.batch_bytes > 0 ? L.batch_bytes
+                                           : std::max<int64_t>(64 << 20, (ctx->arena->capacity() - ctx->arena->used()) / 4);
+  double              flops = 0, flops_run = 0, split_ms = 0, gemm_ms = 0, int8_ops = 0;
+  int                 smin = 99, smax = 0;
+  const cudaStream_t  st = ctx->stream;
+  for(int64_t k0 = 0; k0 < sp0->ntiles();) {
+    int64_t k1 = k0 + 1, bytes = 8 * per[k0];
+    while(k1 < sp0->ntiles() && bytes + 8 * per[k1] <= budget) bytes += 8 * per[k1++];
+    const std::string key = std::to_string(L.serial.v) + "|" + std::to_string(sp0->serial.v) + "|" +
+                            std::to_string(k0) + "-" + std::to_string(k1);
+    auto& hb = lambda_batches[key];
+    if(!hb) {
+      hb         = std::make_unique<tb_tensor_s>();
+      hb->p      = std::make_unique<Tensor>();
+      Tensor& B  = *hb->p;
+      B.nmodes   = L.nmodes;
+      B.tis      = L.tis;
+      B.tis[0]   = tis_subrange(*sp0, k0, k1);
+      B.has_spin = L.has_spin;
+      std::copy(L.mask, L.mask + kMaxModes, B.mask);
+      B.build_table();
+    }
+    Tensor& B = *hb->p;
+    void*   storage = pinned ? pinned->get(8 * std::max<int64_t>(B.nelems, 1))
+                             : ctx->arena->allocate(8 * std::max<int64_t>(B.nelems, 1));
+    B.data = static_cast<double*>(storage);
+    B.ctx  = ctx;
+    if(L.lambda_batch) {
+      if(!builder) {
+        builder      = std::make_unique<tb_sched_s>();
+        builder->p   = std::make_unique<Sched>();
+        builder->p->ctx = ctx;
+      }
+      builder->p->pinned = pinned;
+      const int rc = L.lambda_batch(hb.get(), k0, k1, builder.get(), L.lambda_user);
+      if(rc != 0) {
+        builder->p->ops.clear();
+        builder->p->start = 0;
+        fail(TB_ERR_INVALID, "lambda tensor batch builder returned status " + std::to_string(rc));
+      }
+      builder->p->execute(false);
+      builder->p->pinned = nullptr;
+      for(size_t i = builder->p->last_first; i < builder->p->ops.size(); i++) {
+        const auto& bo = builder->p->ops[i];
+        if(bo.kind == Op::Mult && bo.wl) {
+          if(pinned) batch_lists.push_back(bo.wl);
+          else if(deferred_checks) pending.push_back(bo.wl);
+        }
+      }
+    }
+    else {
+      std::vector<int64_t> bid(B.nmodes), lid(B.nmodes), dims(B.nmodes);
+      for(size_t b = 0; b < B.keys.size(); b++) {
+        int64_t key2 = B.keys[b];
+        for(int m = B.nmodes - 1; m >= 0; m--) {
+          bid[m] = key2 % B.tis[m]->ntiles();
+          key2 /= B.tis[m]->ntiles();
+        }
+        lid       = bid;
+        lid[0]    = L.tis[0]->find_root(B.tis[0]->tiles[bid[0]]);
+        int64_t n = 1;
+        for(int m = 0; m < B.nmodes; m++) n *= (dims[m] = B.tis[m]->size(bid[m]));
+        const int rc = L.lambda_block(lid.data(), L.nmodes, dims.data(), B.data + B.offsets[b], n, st, L.lambda_user);
+        if(rc != 0) fail(TB_ERR_INVALID, "lambda tensor block function returned status " + std::to_string(rc));
+      }
+    }
+    // the contraction over this batch: the first-mode label takes the batch's tiles
+    Op sub   = op;
+    sub.plan = nullptr;
+    sub.wl   = nullptr;
+    sub.za    = on_a ? nullptr : op.za; // what is known of the stored operand stays
+    sub.zb    = on_a ? op.zb : nullptr;
+    sub.store = false;
+    (on_a ? sub.a : sub.b).t = &B;
+    if(L.lambda_batch) { // blocks the builder's assignment left without contributions
+      auto z = builder->p->last_zeros.find(&B);
+      if(z != builder->p->last_zeros.end()) (on_a ? sub.za : sub.zb) = z->second;
+    }
+    for(Labeled* x: {&sub.lhs, &sub.a, &sub.b})
+      for(size_t m = 0; m < x->labels.size(); m++)
+        if(x->labels[m] == lab0) x->ltis[m] = B.tis[0];
+    run(sub);
+    if(sub.wl) {
+      if(pinned) batch_lists.push_back(sub.wl);
+      else if(deferred_checks) pending.push_back(sub.wl);
+    }
+    if(sub.plan) {
+      const tb_stats& s = sub.plan->last;
+      flops += s.flops;
+      flops_run += s.flops_run;
+      split_ms += s.split_ms;
+      gemm_ms += s.gemm_ms;
+      int8_ops += s.int8_ops;
+      smin = std::min(smin, s.slices_min);
+      smax = std::max(smax, s.slices_max);
+    }
+    if(pinned) pinned->put(storage);
+    else ctx->arena->deallocate(storage); // reusable by later work on the stream
+    B.data = nullptr;
+    k0     = k1;
+  }
+  op.plan                 = std::make_shared<Plan>();
+  op.plan->last           = tb_stats{};
+  op.plan->last.flops     = flops;
+  op.plan->last.flops_run = flops_run;
+  op.plan->last.split_ms  = split_ms;
+  op.plan->last.gemm_ms   = gemm_ms;
+  op.plan->last.int8_ops  = int8_ops;
+  op.plan->last.slices_min = smax > 0 ? smin : 0;
+  op.plan->last.slices_max = smax;
+  op.plan->last.mode      = ctx->mode;
+  op.flops                = flops;
+}
+
 // Updates the blocks known to be zero after `op` ran (see Sched::execute).
 void Sched::note_zeros(const Op& op, std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>>& szero) {
   Tensor* t = op.lhs.t;
@@ -1088,7 +1237,8 @@ void Sched::execute(bool profile) {
     if(nranks == 1 && ctx->mode == TB_MODE_FP64 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
        ops[i].is_assign && ops[i].value == 0.0 &&
        ops[i + 1].kind == Op::Mult && same_target(ops[i].lhs, ops[i + 1].lhs) &&
-       ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t) // C read as an operand needs the fill
+       ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t && // C read as an operand needs the fill
+       !ops[i + 1].a.t->is_lambda() && !ops[i + 1].b.t->is_lambda())      // (a batched op adds batch by batch)
       fuse_assign(ops[i], ops[i + 1]);
     run(ops[i]);
     note_zeros(ops[i], szero);
@@ -1100,7 +1250,8 @@ void Sched::execute(bool profile) {
       prof_stats.push_back(ops[i].kind == Op::Mult && ops[i].plan ? ops[i].plan->last : tb_stats{});
     }
   }
-  profiling = false;
+  profiling  = false;
+  last_zeros = std::move(szero);
   if(profile) {
     TB_CUDA(cudaStreamSynchronize(ctx->stream));
     for(size_t i = start; i < ops.size(); i++) {

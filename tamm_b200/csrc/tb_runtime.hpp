@@ -12,6 +12,9 @@
 #include <utility>
 #include <vector>
 
+struct tb_tensor_s;
+struct tb_sched_s;
+
 namespace tb {
 
 // Stream-ordered arena: one cudaMalloc carved by a coalescing best-fit free list
@@ -115,6 +118,12 @@ struct Tensor {
   bool                              read_only = false;
   uint64_t                          ro_serial = 0;
   std::vector<uint8_t>              zero_block;
+  // lambda tensor (tb_tensor_create_lambda / _built): no storage, blocks on demand
+  tb_block_fn                       lambda_block = nullptr;
+  tb_batch_fn                       lambda_batch = nullptr;
+  void*                             lambda_user  = nullptr;
+  int64_t                           batch_bytes  = 0; // per materialised batch (0: default)
+  bool                              is_lambda() const { return lambda_block || lambda_batch; }
   ~Tensor();
 
   void    build_table(); // Distribution_NW (distribution.hpp:201-243)
@@ -220,6 +229,16 @@ struct Sched {
   // intermediates of multi-factor products (tb_sched_mult_n), by signature; freed with
   // the scheduler
   std::map<std::string, std::unique_ptr<Tensor>>    temps;
+  // batch tensors of lambda operands (storage only while a batch runs) and the
+  // scheduler that batch builders queue their ops on
+  std::map<std::string, std::unique_ptr<tb_tensor_s>> lambda_batches;
+  std::unique_ptr<tb_sched_s>                         builder;
+  // work lists of lambda batches run while capturing a graph (their error words are
+  // checked by the graph's sync)
+  std::vector<std::shared_ptr<WorkList>>              batch_lists;
+  // blocks known to be zero by construction at the end of the last execute
+  std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>> last_zeros;
+  void                                                run_lambda_mult(Op& op);
   static constexpr int                              kSlots = 64;
   double*                                           d_scalars = nullptr; // kSlots + 1024 partials
   bool                                              autotune  = false;

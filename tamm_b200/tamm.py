@@ -249,6 +249,84 @@ class Tensor:
         self.nmodes, self.nblocks, self.nelems = nm.value, nb.value, ne.value
         self.ec = None
 
+    # --- lambda tensors (blocks on demand) ---
+    @classmethod
+    def lambda_(cls, spaces: Sequence, fn, spin=None, spin_mask=None, batch_bytes: int = 0):
+        """Tensor<T>(tis, Func): fn(blockid, dims) -> array of the block's values, called
+        when a contraction reads the block (tb_tensor_create_lambda; the values are
+        copied to the device on the stream the library gives)."""
+        import torch
+
+        def cb(bid_p, nm, dims_p, dst, n, stream, user):
+            try:
+                bid = [bid_p[k] for k in range(nm)]
+                dims = [dims_p[k] for k in range(nm)]
+                arr = np.ascontiguousarray(fn(bid, dims), dtype=np.float64).reshape(-1)
+                if arr.size != n:
+                    return 2
+                view = _device_array(dst, n, torch.cuda.current_device())
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                    view.copy_(torch.from_numpy(arr))
+                return 0
+            except Exception:  # a failing callback fails the op, not the process
+                import traceback
+                traceback.print_exc()
+                return 1
+        return cls._on_demand(spaces, spin, spin_mask, "tb_tensor_create_lambda", A.BLOCK_FN(cb), batch_bytes)
+
+    @classmethod
+    def built(cls, spaces: Sequence, builder, spin=None, spin_mask=None, batch_bytes: int = 0):
+        """A tensor built batch by batch when a contraction reads it
+        (tb_tensor_create_built): builder(batch, first_tile, last_tile, sch) queues ops
+        on the scheduler `sch` that write the allocated tensor `batch` (the tiles
+        [first_tile, last_tile) of the first mode's label space, the other modes whole)."""
+        holder = {}
+
+        def cb(batch_h, first, last, sch_h, user):
+            try:
+                me = holder["t"]
+                spaces_b = []
+                for m in range(me.nmodes):
+                    th = A.h()
+                    call("tb_tensor_space", batch_h, m, C.byref(th))
+                    spaces_b.append(TiledIndexSpace(_handle=th, _parent=me.spaces[m]))
+                builder(_BorrowedTensor(batch_h, spaces_b), int(first), int(last), _BorrowedScheduler(sch_h))
+                return 0
+            except Exception:
+                import traceback
+                traceback.print_exc()
+                return 1
+        t = cls._on_demand(spaces, spin, spin_mask, "tb_tensor_create_built", A.BATCH_FN(cb), batch_bytes)
+        holder["t"] = t
+        return t
+
+    @classmethod
+    def _on_demand(cls, spaces, spin, spin_mask, ctor, cfn, batch_bytes):
+        self = cls.__new__(cls)
+        self.spaces = [s.tis if isinstance(s, TiledIndexLabel) else s for s in spaces]
+        self.default_labels = [s if isinstance(s, TiledIndexLabel) else None for s in spaces]
+        n = len(self.spaces)
+        hs = (A.h * max(n, 1))(*[s.h for s in self.spaces])
+        if spin is not None:
+            mask = [0] * int(spin[0]) + [1] * int(spin[1]) + [2] * (n - int(spin[0]) - int(spin[1]))
+        else:
+            mask = spin_mask
+        m = (C.c_int * n)(*mask) if mask is not None else None
+        self.h = A.h()
+        self._fn = cfn  # the C callback must outlive the tensor
+        call(ctor, n, hs, m, C.cast(cfn, C.c_void_p), None, C.byref(self.h))
+        if batch_bytes:
+            call("tb_tensor_set_batch_bytes", self.h, int(batch_bytes))
+        nm, nb, ne = C.c_int(), C.c_int64(), C.c_int64()
+        call("tb_tensor_info", self.h, C.byref(nm), C.byref(nb), C.byref(ne))
+        self.nmodes, self.nblocks, self.nelems = nm.value, nb.value, ne.value
+        self.ec = None
+        return self
+
+    def set_batch_bytes(self, nbytes: int):
+        call("tb_tensor_set_batch_bytes", self.h, int(nbytes))
+        return self
+
     # --- storage ---
     def allocate(self, ec: ExecutionContext):
         call("tb_tensor_allocate", self.h, ec.h)
@@ -295,14 +373,7 @@ class Tensor:
     def device_view(self):
         """A torch tensor sharing this tensor's packed device storage (no copy), for
         collectives and checks; valid while the tensor stays allocated."""
-        import torch
-
-        class _Dev:
-            pass
-        d = _Dev()
-        d.__cuda_array_interface__ = {"shape": (self.nelems,), "typestr": "<f8", "data": (self.data_ptr(), False),
-                                      "version": 3, "strides": None}
-        return torch.as_tensor(d, device=f"cuda:{self.ec.device}")
+        return _device_array(self.data_ptr(), self.nelems, self.ec.device)
 
     def set_read_only(self, on: bool = True):
         """Declare the contents constant (writes through the library then fail) and let
@@ -396,6 +467,34 @@ class Tensor:
             A.lib().tb_tensor_destroy(self.h)
         except Exception:
             pass
+
+
+class _BorrowedTensor(Tensor):
+    """A library-owned tensor handed to a callback (not destroyed from Python)."""
+
+    def __init__(self, h, spaces):
+        self.h = C.c_void_p(h) if not isinstance(h, C.c_void_p) else h
+        self.spaces = spaces
+        self.default_labels = [None] * len(spaces)
+        nm, nb, ne = C.c_int(), C.c_int64(), C.c_int64()
+        call("tb_tensor_info", self.h, C.byref(nm), C.byref(nb), C.byref(ne))
+        self.nmodes, self.nblocks, self.nelems = nm.value, nb.value, ne.value
+        self.ec = None
+
+    def __del__(self):
+        pass
+
+
+def _device_array(ptr: int, n: int, device: int):
+    """A torch view of n doubles of device memory at ptr (no copy)."""
+    import torch
+
+    class _Dev:
+        pass
+    d = _Dev()
+    d.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (int(ptr), False), "version": 3,
+                                  "strides": None}
+    return torch.as_tensor(d, device=f"cuda:{device}")
 
 
 class _Product:
@@ -681,6 +780,18 @@ class Scheduler:
             A.lib().tb_sched_destroy(self.h)
         except Exception:
             pass
+
+
+class _BorrowedScheduler(Scheduler):
+    """A library-owned scheduler handed to a batch builder (not destroyed from Python)."""
+
+    def __init__(self, h):
+        self.ec = None
+        self.h = C.c_void_p(h) if not isinstance(h, C.c_void_p) else h
+        self._keep = []
+
+    def __del__(self):
+        pass
 
 
 class Graph:
