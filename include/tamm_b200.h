@@ -217,6 +217,15 @@ int tb_tis_num_tiles(tb_tis tis, int64_t* ntiles);
  * and index in the root tiled space.  Arrays hold num_tiles entries. */
 int tb_tis_tiles(tb_tis tis, int64_t* sizes, int* spins, int64_t* root_tiles);
 int tb_tis_destroy(tb_tis tis);
+/* Dependent tiled index space (TiledIndexSpace{reference, {on...}, dep_map},
+ * src/tamm/tiled_index_space.hpp:60-72; DLPNO's PNO space over LMO pairs): for key n,
+ * the tile tuple keys[n * ndep .. n * ndep + ndep) of the spaces `on` (1..4 of them,
+ * ordinary spaces) maps to the sub-space values[n] of `reference`, whose tiles are the
+ * dependent space's tiles for that tuple; tuples not listed have no tiles.  The
+ * dependent space has the reference's tiles; a tensor mode over it exists only where
+ * its tile is listed for the tiles of the modes it depends on. */
+int tb_tis_create_dependent(tb_tis reference, int ndep, const tb_tis* on, int64_t nkeys, const int64_t* keys,
+                            const tb_tis* values, tb_tis* out);
 
 /* Tensor<T>{tis...} or Tensor<T>{{tis...}, SpinMask} (src/tamm/tensor.hpp:87-136,
  * spin rule tensor_base.hpp:243-263).  spin_mask NULL: no spin symmetry; else per
@@ -225,6 +234,12 @@ int tb_tis_destroy(tb_tis tis);
  * packed contiguously in one device arena allocation. */
 typedef struct tb_tensor_s* tb_tensor;
 int tb_tensor_create(int nmodes, const tb_tis* tis, const int* spin_mask, tb_tensor* out);
+/* Tensor with dependent modes (Tensor<T>{i, j, a(i, j), e(i, j)}): dep_modes holds 4
+ * ints per mode, the modes a mode over a dependent space depends on (in the order of
+ * that space's `on` list; -1 unused); admitted blocks also satisfy the dependency
+ * (translate_blockid_if_possible, src/tamm/utils.hpp:369). */
+int tb_tensor_create_dependent(int nmodes, const tb_tis* tis, const int* spin_mask, const int* dep_modes,
+                               tb_tensor* out);
 /* Tensor{{tis...}, {nupper, nlower}} form (tensor_impl.hpp:153-209). */
 int tb_tensor_create_spin_sizes(int nmodes, const tb_tis* tis, int nupper, int nlower,
                                 tb_tensor* out);

@@ -467,7 +467,53 @@ int tb_tis_destroy(tb_tis tis) {
   return TB_OK;
 }
 
-static tb_tensor new_tensor(int nmodes, const tb_tis* tis, const int* mask) {
+static tb_tensor new_tensor(int nmodes, const tb_tis* tis, const int* mask, const int* dep_modes = nullptr);
+
+int tb_tis_create_dependent(tb_tis reference, int ndep, const tb_tis* on, int64_t nkeys, const int64_t* keys,
+                            const tb_tis* values, tb_tis* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(reference != nullptr && out != nullptr && on != nullptr && ndep >= 1 && ndep <= 4);
+  REQUIRE_ARG(nkeys >= 0 && (nkeys == 0 || (keys != nullptr && values != nullptr)));
+  TB_EXPECTS(!reference->p->dep, "the reference of a dependent space must not be dependent itself");
+  auto dep = std::make_shared<Dependency>();
+  for(int k = 0; k < ndep; k++) {
+    REQUIRE_ARG(on[k] != nullptr);
+    dep->on.push_back(on[k]->p);
+  }
+  const TIS& ref = *reference->p;
+  for(int64_t n = 0; n < nkeys; n++) {
+    std::vector<int64_t> key(keys + n * ndep, keys + (n + 1) * ndep);
+    for(int k = 0; k < ndep; k++)
+      TB_EXPECTS(key[k] >= 0 && key[k] < dep->on[k]->ntiles(), "dependency key tile out of range");
+    REQUIRE_ARG(values[n] != nullptr);
+    const TIS& val = *values[n]->p;
+    TB_EXPECTS(val.root == ref.root, "a dependent space's tiles must be tiles of its reference space");
+    std::vector<uint8_t> ok(ref.ntiles(), 0);
+    for(int64_t t: val.tiles) {
+      const int64_t x = ref.find_root(t);
+      TB_EXPECTS(x >= 0, "a dependent space's tiles must be tiles of its reference space");
+      ok[x] = 1;
+    }
+    TB_EXPECTS(dep->valid.emplace(key, ok).second, "dependency key listed twice");
+  }
+  auto* h  = new tb_tis_s();
+  h->p     = std::make_shared<TIS>();
+  h->p->root  = ref.root;
+  h->p->tiles = ref.tiles;
+  h->p->dep   = dep;
+  *out        = h;
+  TB_API_END
+}
+
+int tb_tensor_create_dependent(int nmodes, const tb_tis* tis, const int* spin_mask, const int* dep_modes,
+                               tb_tensor* out) {
+  TB_API_BEGIN
+  REQUIRE_ARG(out != nullptr && dep_modes != nullptr);
+  *out = new_tensor(nmodes, tis, spin_mask, dep_modes);
+  TB_API_END
+}
+
+static tb_tensor new_tensor(int nmodes, const tb_tis* tis, const int* mask, const int* dep_modes) {
   TB_EXPECTS(nmodes >= 0 && nmodes <= kMaxModes, "tensor rank out of range (max 8)");
   auto t      = std::make_unique<Tensor>();
   t->nmodes   = nmodes;
@@ -478,6 +524,20 @@ static tb_tensor new_tensor(int nmodes, const tb_tis* tis, const int* mask) {
     if(mask) {
       TB_EXPECTS(mask[i] >= 0 && mask[i] <= 2, "spin mask entries are 0 upper, 1 lower, 2 ignore");
       t->mask[i] = mask[i];
+    }
+  }
+  t->dep_modes.assign(nmodes, {});
+  for(int i = 0; i < nmodes; i++) {
+    const auto& d = t->tis[i]->dep;
+    if(!d) continue;
+    TB_EXPECTS(dep_modes != nullptr, "a mode over a dependent space needs the modes it depends on "
+                                     "(tb_tensor_create_dependent)");
+    for(int k = 0; k < (int) d->on.size(); k++) {
+      const int o = dep_modes[4 * i + k];
+      TB_EXPECTS(o >= 0 && o < nmodes && o != i, "dependent mode refers to a mode out of range");
+      TB_EXPECTS(!t->tis[o]->dep, "a dependent mode must depend on ordinary modes");
+      TB_EXPECTS(t->tis[o]->root == d->on[k]->root, "a dependent mode's key mode is not over the space it depends on");
+      t->dep_modes[i].push_back(o);
     }
   }
   t->build_table();

@@ -252,6 +252,7 @@ std::shared_ptr<TIS> tis_named(const TIS& parent, const std::string& name) {
 
 std::shared_ptr<TIS> tis_subrange(const TIS& parent, int64_t first, int64_t last) {
   TB_EXPECTS(first >= 0 && last >= first && last <= parent.ntiles(), "tile range out of bounds");
+  TB_EXPECTS(!parent.dep, "tile sub-ranges of a dependent space are not supported");
   auto s  = std::make_shared<TIS>();
   s->root = parent.root;
   s->tiles.assign(parent.tiles.begin() + first, parent.tiles.begin() + last);
@@ -287,6 +288,21 @@ void Tensor::build_table() {
 }
 
 bool Tensor::is_non_zero(const int64_t* blockid) const {
+  // dependent modes: the block exists only where the tile of the dependent mode is one
+  // of the tiles its space lists for the tiles of the modes it depends on
+  // (translate_blockid_if_possible, utils.hpp:369)
+  for(int m = 0; m < (int) dep_modes.size(); m++) {
+    if(dep_modes[m].empty()) continue;
+    const Dependency&    d = *tis[m]->dep;
+    std::vector<int64_t> key(dep_modes[m].size());
+    for(size_t k = 0; k < key.size(); k++) {
+      const int o = dep_modes[m][k];
+      key[k]      = d.on[k]->find_root(tis[o]->tiles[blockid[o]]);
+      if(key[k] < 0) return false;
+    }
+    auto it = d.valid.find(key);
+    if(it == d.valid.end() || !it->second[blockid[m]]) return false;
+  }
   // TensorBase::is_non_zero (tensor_base.hpp:243-263)
   if(!has_spin) return true;
   int upper = 0, lower = 0;

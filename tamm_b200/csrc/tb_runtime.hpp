@@ -86,10 +86,20 @@ struct Serial {
   Serial& operator=(const Serial&) { return *this; }
 };
 
+// Dependency of a tiled index space on the tiles of other spaces (TAMM's dependent
+// TiledIndexSpace, tiled_index_space.hpp:60-72, as DLPNO's PNO space depends on an LMO
+// pair): for each tuple of tiles of the `on` spaces, which tiles of the dependent space
+// exist; tuples not listed have none.
+struct Dependency {
+  std::vector<std::shared_ptr<struct TIS>>             on;
+  std::map<std::vector<int64_t>, std::vector<uint8_t>> valid; // on-space tiles -> per tile, 1 if it exists
+};
+
 struct TIS {
   Serial                      serial;
   std::shared_ptr<RootTiling> root;
   std::vector<int64_t>        tiles;
+  std::shared_ptr<Dependency> dep; // set for a dependent space
   int64_t                     ntiles() const { return (int64_t) tiles.size(); }
   int64_t size(int64_t t) const { return root->offsets[tiles[t] + 1] - root->offsets[tiles[t]]; }
   int     spin(int64_t t) const { return root->spins[tiles[t]]; }
@@ -123,6 +133,8 @@ struct Tensor {
   tb_batch_fn                       lambda_batch = nullptr;
   void*                             lambda_user  = nullptr;
   int64_t                           batch_bytes  = 0; // per materialised batch (0: default)
+  // modes a dependent mode's tiles depend on (empty for an ordinary mode)
+  std::vector<std::vector<int>>     dep_modes;
   bool                              is_lambda() const { return lambda_block || lambda_batch; }
   ~Tensor();
 

@@ -154,6 +154,15 @@ class TiledIndexLabel:
     def __repr__(self):
         return f"TiledIndexLabel({self.name or self.id})"
 
+    def __call__(self, *deps: "TiledIndexLabel") -> "_DepLabel":
+        """a(i, j): a label over a dependent space, with the labels its tiles depend on."""
+        return _DepLabel(self, list(deps))
+
+
+class _DepLabel:
+    def __init__(self, label: TiledIndexLabel, deps: list):
+        self.label, self.deps = label, deps
+
 
 class TiledIndexSpace:
     """TiledIndexSpace{is, tile} or TiledIndexSpace{is, tile_list}."""
@@ -216,6 +225,20 @@ class TiledIndexSpace:
     def label(self, name=""):
         return TiledIndexLabel(self, name)
 
+    @classmethod
+    def dependent(cls, reference: "TiledIndexSpace", on: Sequence, dep: dict) -> "TiledIndexSpace":
+        """TiledIndexSpace{reference, {on...}, dep_map}: dep maps a tuple of tile indices
+        of the `on` spaces to the sub-space of `reference` whose tiles exist for it."""
+        keys = np.asarray([list(k) for k in dep.keys()] or [[0] * len(on)], dtype=np.int64).reshape(-1)
+        vals = (A.h * max(len(dep), 1))(*[v.h for v in dep.values()])
+        ons = (A.h * len(on))(*[o.h for o in on])
+        h = A.h()
+        call("tb_tis_create_dependent", reference.h, len(on), ons, len(dep), keys.ctypes.data_as(A.i64p), vals,
+             C.byref(h))
+        t = cls(_handle=h, _parent=reference)
+        t._deps = (list(on), dict(dep))  # keep the spaces alive
+        return t
+
     def labels(self, n, name="all"):
         sp = self if name == "all" else self(name)
         return tuple(TiledIndexLabel(sp) for _ in range(n))
@@ -232,12 +255,24 @@ class Tensor:
     spin-blocked sparsity."""
 
     def __init__(self, spaces: Sequence, spin=None, spin_mask=None):
-        self.spaces = [s.tis if isinstance(s, TiledIndexLabel) else s for s in spaces]
-        self.default_labels = [s if isinstance(s, TiledIndexLabel) else None for s in spaces]
+        dep = [s for s in spaces if isinstance(s, _DepLabel)]
+        plain = [s.label if isinstance(s, _DepLabel) else s for s in spaces]
+        self.spaces = [s.tis if isinstance(s, TiledIndexLabel) else s for s in plain]
+        self.default_labels = [s if isinstance(s, TiledIndexLabel) else None for s in plain]
         n = len(self.spaces)
         hs = (A.h * max(n, 1))(*[s.h for s in self.spaces])
         self.h = A.h()
-        if spin is not None:
+        if dep:  # Tensor{i, j, a(i, j), e(i, j)}: modes over dependent spaces
+            dm = (C.c_int * (4 * n))(*([-1] * (4 * n)))
+            for m, s in enumerate(spaces):
+                if isinstance(s, _DepLabel):
+                    for k, d in enumerate(s.deps):
+                        dm[4 * m + k] = [x is d for x in plain].index(True)
+            if spin is not None:
+                spin_mask = [0] * int(spin[0]) + [1] * int(spin[1]) + [2] * (n - int(spin[0]) - int(spin[1]))
+            mk = (C.c_int * n)(*spin_mask) if spin_mask is not None else None
+            call("tb_tensor_create_dependent", n, hs, mk, dm, C.byref(self.h))
+        elif spin is not None:
             call("tb_tensor_create_spin_sizes", n, hs, int(spin[0]), int(spin[1]), C.byref(self.h))
         elif spin_mask is not None:
             m = (C.c_int * n)(*spin_mask)
