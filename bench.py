@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--ccsd-oa", type=int, default=30)
     p.add_argument("--ccsd-va", type=int, default=240)
     p.add_argument("--shard", action="store_true", help="owner-computes path with an all-reduce even at N=1")
+    p.add_argument("--workload", default="ladder", choices=["ladder", "blockops"],
+                   help="blockops: the HBM-bound block kernels on the ladder's r2 (one JSON line, GB/s)")
     return p.parse_args()
 
 
@@ -239,6 +241,58 @@ def load_peaks():
         return {}
 
 
+def run_blockops(args, torch, tb, W, local):
+    """The HBM-bound block kernels at the ladder's sizes (r2, t2: O=40, V=360 spin-blocked,
+    7.8e7 elements, 0.62 GB each, beyond L2): permuted add r2(a,b,i,j) += X(b,a,j,i)
+    (k_assign_tiled, 24 B/element), flat add r2 += X (k_axpby, 24), dot r2.t2 and norm
+    (k_dot_partial, 16 and 8), denominator update t2 += r2 / D (k_denom, 24) and an
+    in-place map r2 = 2 r2 (k_map_blocks, 16).  Each timed over `steps` launches after
+    `warmup` with CUDA events on the context's stream; GB/s of algorithmic bytes."""
+    ec = tb.ExecutionContext(local, int(8 * 2 ** 30))
+    lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec, build_v=False)
+    a, b, c, d, i, j = lad.labels
+    X = tb.Tensor([lad.V, lad.V, lad.O, lad.O], spin=(2, 2)).allocate(ec)
+    X.write(np.random.default_rng(3).normal(size=X.nelems))
+    lad.r2.write(np.random.default_rng(4).normal(size=lad.r2.nelems))
+    n = lad.r2.nelems
+    eps = np.concatenate([np.full(2 * args.oa, -1.0), np.full(2 * args.va, 1.0)]) * \
+        np.random.default_rng(5).uniform(0.3, 2.0, size=2 * (args.oa + args.va))
+    stream = torch.cuda.ExternalStream(ec.stream)
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs")
+    cases = {
+        "permuted_add k_assign_tiled": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(b, a, j, i)))),
+        "flat_add k_axpby": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(a, b, i, j)))),
+        "dot k_dot_partial": (16, lambda s: s.dot(0, lad.r2(a, b, i, j), lad.t2(a, b, i, j))),
+        "norm k_dot_partial": (8, lambda s: s.norm(1, lad.r2(a, b, i, j))),
+        "denominator_update k_denom": (24, lambda s: s.denom(lad.t2(a, b, i, j), -1e-3, lad.r2(a, b, i, j), eps,
+                                                                [1, 1, -1, -1])),
+        "map_scale k_map_blocks": (16, lambda s: s.map(lad.r2(a, b, i, j), lad.r2(a, b, i, j), tb.Map.SCALE, 1.0)),
+    }
+    out = {}
+    for name, (bpe, q) in cases.items():
+        sch = tb.Scheduler(ec)
+        q(sch)
+        g = sch.graph()  # one captured launch per step: no host work in the timed region
+        for _ in range(args.warmup):
+            g.launch()
+        g.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.launch()
+        e1.record(stream)
+        g.sync()
+        ms = e0.elapsed_time(e1) / args.steps
+        del g
+        gbs = bpe * n / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "GB/s": gbs, "frac_of_measured_hbm": (gbs / hbm) if hbm else None,
+                     "bytes_per_element": bpe}
+    print(json.dumps({"workload": f"blockops_ladder_O{2 * args.oa}_V{2 * args.va}", "elements": n,
+                      "hbm_peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)",
+                      "kernels": out}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -262,6 +316,9 @@ def main():
     from tamm_b200 import _capi as A
     from tamm_b200 import workloads as W
 
+    if args.workload == "blockops":
+        run_blockops(args, torch, tb, W, local)
+        return
     headline = args.mode or "int8"
     modes = {"fp64": tb.Precision.FP64, "int8": tb.Precision.INT8, "bf16x3": tb.Precision.BF16X3}
     ec = tb.ExecutionContext(local, int(150 * 2 ** 30))

@@ -307,6 +307,107 @@ void launch_assign(const AssignLoop& lp, double* dst, double scale, const double
   TB_CUDA(cudaGetLastError());
 }
 
+BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off) {
+  BlockAssign b{};
+  b.dst_off = dst_off;
+  b.src_off = src_off;
+  b.nd      = lp.nd;
+  b.total   = 1;
+  for(int k = 0; k < lp.nd; k++) b.total *= lp.dims[k];
+  int p = -1;
+  for(int k = 0; k < lp.nd; k++)
+    if(lp.sld[k] == 1 && lp.dims[k] > 1) p = k;
+  const int q = lp.nd - 1;
+  const bool tiled = lp.nd >= 2 && p >= 0 && p != q && lp.dld[q] == 1 && lp.dims[q] >= 8 && lp.dims[p] >= 8;
+  b.p           = tiled ? p : -1;
+  b.outer_total = 1;
+  for(int k = 0; k < 4; k++) {
+    b.dims[k] = k < lp.nd ? lp.dims[k] : 1;
+    b.dld[k]  = k < lp.nd ? lp.dld[k] : 0;
+    b.sld[k]  = k < lp.nd ? lp.sld[k] : 0;
+    if(tiled && k < lp.nd && k != p && k != q) b.outer_total *= lp.dims[k];
+  }
+  return b;
+}
+
+// The block pairs of an AddOp in one launch: CTA row blockIdx.y takes pairs y, y +
+// gridDim.y, ...; within a pair the gridDim.x CTAs share its 32x32 tiles (a transposing
+// pair, as k_assign_tiled) or its elements (a streamed pair, as k_assign).
+__global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__ dst, double scale,
+                                                            const double* __restrict__ src,
+                                                            const BlockAssign* __restrict__ blocks, int nblocks,
+                                                            int is_assign) {
+  __shared__ double tile[32][33];
+  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
+    const BlockAssign a  = blocks[blk];
+    double* const     d0 = dst + a.dst_off;
+    const double*     s0 = src + a.src_off;
+    if(a.p >= 0) {
+      const int     q      = a.nd - 1;
+      const int64_t Dq     = a.dims[q], Dp = a.dims[a.p];
+      const int64_t tq     = (Dq + 31) / 32, tp = (Dp + 31) / 32;
+      const int64_t ntiles = a.outer_total * tq * tp;
+      for(int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int64_t x  = t;
+        int64_t bq = x % tq;
+        x /= tq;
+        int64_t bp = x % tp;
+        x /= tp;
+        int64_t so = 0, doff = 0;
+        for(int k = a.nd - 1; k >= 0; k--) {
+          if(k == q || k == a.p) continue;
+          const int64_t dk = a.dims[k];
+          const int64_t i  = x % dk;
+          x /= dk;
+          so += i * a.sld[k];
+          doff += i * a.dld[k];
+        }
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        for(int r = ty; r < 32; r += 8) {
+          const int64_t iq = bq * 32 + r, ip = bp * 32 + tx;
+          if(iq < Dq && ip < Dp) tile[r][tx] = __ldg(s0 + so + iq * a.sld[q] + ip * a.sld[a.p]);
+        }
+        __syncthreads();
+        for(int r = ty; r < 32; r += 8) {
+          const int64_t ip = bp * 32 + r, iq = bq * 32 + tx;
+          if(iq < Dq && ip < Dp) {
+            double*      dp = d0 + doff + iq * a.dld[q] + ip * a.dld[a.p];
+            const double v  = scale * tile[tx][r];
+            *dp             = is_assign ? v : *dp + v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    else {
+      const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+      for(int64_t lin = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; lin < a.total; lin += stride) {
+        int64_t x = lin, so = 0, doff = 0;
+#pragma unroll
+        for(int k = 3; k >= 0; k--) {
+          if(k >= a.nd) continue;
+          const int64_t dk = a.dims[k];
+          const int64_t qk = x / dk;
+          const int64_t i  = x - qk * dk;
+          so += i * a.sld[k];
+          doff += i * a.dld[k];
+          x = qk;
+        }
+        const double v = scale * __ldg(s0 + so);
+        d0[doff]       = is_assign ? v : d0[doff] + v;
+      }
+    }
+  }
+}
+
+void launch_assign_blocks(double* dst, double scale, const double* src, const BlockAssign* blocks, int nblocks,
+                          int is_assign, cudaStream_t stream) {
+  if(nblocks <= 0) return;
+  const dim3 grid(8, (unsigned) std::min(nblocks, 8192));
+  k_assign_blocks<<<grid, kThreads, 0, stream>>>(dst, scale, src, blocks, nblocks, is_assign);
+  TB_CUDA(cudaGetLastError());
+}
+
 void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream) {
   if(n <= 0) return;
   k_fill<<<grid_for(n, 8), kThreads, 0, stream>>>(x, n, value, is_assign);

@@ -155,6 +155,19 @@ AssignLoop plan_assign(const int64_t* ddims, const int* dlabels, int nd, const i
                        const int* slabels, int ns);
 void launch_assign(const AssignLoop& lp, double* dst, double scale, const double* src,
                    int is_assign, cudaStream_t stream);
+// One block pair of a permuted AddOp: offsets and the loop of plan_assign, with the
+// position of the source's stride-1 loop mode when the pair goes through the 32x32
+// shared-memory transpose (-1: streamed).
+struct BlockAssign {
+  int64_t dst_off, src_off;
+  int32_t nd, p;
+  int64_t dims[4], dld[4], sld[4];
+  int64_t outer_total, total;
+};
+BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off);
+// All block pairs of an AddOp in one launch (device array of nblocks BlockAssign).
+void launch_assign_blocks(double* dst, double scale, const double* src, const BlockAssign* blocks, int nblocks,
+                          int is_assign, cudaStream_t stream);
 void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream);
 // x[off .. off + n) (=|+=) value for each (off, n) pair of a device array
 void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double value, int is_assign,

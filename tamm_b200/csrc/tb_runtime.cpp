@@ -762,12 +762,37 @@ void Sched::run(Op& op) {
                    op.lhs.t->nelems, st);
       return;
     }
-    for(const auto& ab: *op.add_blocks) {
-      AssignLoop lp = plan_assign(ab.ddims, op.lhs.labels.data(), op.lhs.t->nmodes, ab.sdims,
-                                  op.a.labels.data(), op.a.t->nmodes);
-      launch_assign(lp, op.lhs.t->data + ab.dst_off, op.alpha, op.a.t->data + ab.src_off,
-                    op.is_assign, st);
+    if(!op.add_dev) { // every block pair in one launch; the list is uploaded once per signature
+      const std::string key    = "A|" + signature(op);
+      auto&             cached = fill_cache[key];
+      auto&             count  = map_count[key];
+      if(!cached) {
+        std::vector<BlockAssign> list;
+        for(const auto& ab: *op.add_blocks) {
+          AssignLoop lp = plan_assign(ab.ddims, op.lhs.labels.data(), op.lhs.t->nmodes, ab.sdims,
+                                      op.a.labels.data(), op.a.t->nmodes);
+          list.push_back(make_block_assign(lp, ab.dst_off, ab.src_off));
+        }
+        TB_EXPECTS(list.size() < (1u << 31), "too many block pairs in one add");
+        BlockAssign* d   = nullptr;
+        const int    dev = ctx->device;
+        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(BlockAssign) * std::max<size_t>(list.size(), 1)));
+        cached = std::shared_ptr<int64_t>(reinterpret_cast<int64_t*>(d), [dev](int64_t* q) {
+          int cur = -1;
+          cudaGetDevice(&cur);
+          cudaSetDevice(dev);
+          cudaFree(q);
+          if(cur >= 0) cudaSetDevice(cur);
+        });
+        if(!list.empty())
+          TB_CUDA(cudaMemcpy(d, list.data(), sizeof(BlockAssign) * list.size(), cudaMemcpyHostToDevice));
+        count = (int) list.size();
+      }
+      op.add_dev = cached;
+      op.add_n   = count;
     }
+    launch_assign_blocks(op.lhs.t->data, op.alpha, op.a.t->data, reinterpret_cast<const BlockAssign*>(op.add_dev.get()),
+                         op.add_n, op.is_assign, st);
     return;
   }
   if(op.kind == Op::Dot) {

@@ -183,6 +183,8 @@ struct Op {
     int64_t ddims[kMaxModes], sdims[kMaxModes];
   };
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
+  std::shared_ptr<int64_t>               add_dev;   // device BlockAssign list (scheduler's cache)
+  int                                    add_n = 0;
   int                                    fn = 0;     // Map: element function
   std::shared_ptr<int64_t>               map_dev;    // Map: device (dst, src, n) triples
   int                                    map_n = 0;  // number of triples
