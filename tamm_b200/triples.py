@@ -117,6 +117,10 @@ def build(oa: int, va: int, tile: int = 40, jtile: int = 2, dtile: int = 0, seed
     sch(T["vx"](b, c, k, d).assign(T["L_vv"](q, b, d) * T["L_vo"](q, c, k)))
     sch(T["vy"](l, c, j, k).assign(T["L_oo"](q, l, j) * T["L_vo"](q, c, k)))
     sch.execute(ExecutionHW.GPU)
+    # constant through the streamed steps: marked read-only, the exactly-zero spin
+    # blocks of the integrals (e.g. vx(b,c,k,d) with spin(b) != spin(d)) are skipped
+    for t in T.values():
+        t.set_read_only(True)
     most = 0  # the W layout depends on the spin of i and on the j block
     for i in (0, oa):
         for jt in range(Oj.num_tiles):
