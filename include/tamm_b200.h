@@ -186,6 +186,14 @@ int tb_ctx_synchronize(tb_ctx ctx); /* compute and copy streams */
 /* Makes later work on the compute stream wait for everything enqueued so far on the
  * context's copy streams (e.g. to time transfers with events on the compute stream). */
 int tb_ctx_join(tb_ctx ctx);
+/* Digit cache (no counterpart in TAMM): up to `bytes` of the context's arena keep the
+ * split-INT8 digits of read-only tensors (tb_tensor_set_read_only) per operand view,
+ * so that a constant operand, such as the integrals of a coupled-cluster run, is split
+ * once instead of in every contraction that reads it.  0 (the default) turns it off
+ * and frees nothing already kept (entries go when their tensor's mark changes).
+ * *used receives the bytes kept now. */
+int tb_ctx_set_digit_cache(tb_ctx ctx, int64_t bytes);
+int tb_ctx_digit_cache_info(tb_ctx ctx, int64_t* used, int64_t* limit);
 /* Sub-allocation from the context's stream-ordered arena (TAMM's RMM pool,
  * rmm_memory_pool.hpp:50-263): 256-byte aligned device memory, reusable by any
  * later work on the context's stream as soon as it is freed. */

@@ -97,6 +97,8 @@ PROTOS = {
     "tb_tensor_data": [h, C.POINTER(vp)],
     "tb_tensor_set_read_only": [h, C.c_int],
     "tb_tensor_record_use": [h],
+    "tb_ctx_set_digit_cache": [h, C.c_int64],
+    "tb_ctx_digit_cache_info": [h, i64p, i64p],
     "tb_tis_create_dependent": [h, C.c_int, C.POINTER(h), C.c_int64, i64p, C.POINTER(h), C.POINTER(h)],
     "tb_tensor_create_dependent": [C.c_int, C.POINTER(h), ip, ip, C.POINTER(h)],
     "tb_tensor_create_lambda": [C.c_int, C.POINTER(h), ip, C.c_void_p, C.c_void_p, C.POINTER(h)],

@@ -36,8 +36,11 @@ def main(argv=None):
     p.add_argument("--h", type=float, default=1e-5)
     p.add_argument("--budget-bytes", type=int, default=1 << 62)
     p.add_argument("--pool-gib", type=int, default=60)
+    p.add_argument("--digit-cache-gib", type=int, default=16,
+                   help="split-INT8 digits of the read-only integrals kept across contractions (0: off)")
     args = p.parse_args(argv)
     ec = ExecutionContext(0, args.pool_gib << 30)
+    ec.set_digit_cache(args.digit_cache_gib << 30)
     P = W.energy_problem(args.oa, args.va, seed=args.seed, ec=ec, budget_bytes=args.budget_bytes)
     amps = W.fd_amplitudes(P.lad.t2, args.fd, seed=args.seed + 101)
     offs = [o for _, _, o in amps]

@@ -319,6 +319,22 @@ int tb_ctx_set_precision(tb_ctx ctx, int mode, double err_target, int nslices) {
   TB_API_END
 }
 
+int tb_ctx_set_digit_cache(tb_ctx ctx, int64_t bytes) {
+  TB_API_BEGIN
+  REQUIRE_ARG(ctx != nullptr);
+  TB_EXPECTS(bytes >= 0, "negative cache size");
+  ctx->p->digit_cache_bytes = bytes;
+  TB_API_END
+}
+
+int tb_ctx_digit_cache_info(tb_ctx ctx, int64_t* used, int64_t* limit) {
+  TB_API_BEGIN
+  REQUIRE_ARG(ctx != nullptr);
+  if(used) *used = ctx->p->digit_cache_used;
+  if(limit) *limit = ctx->p->digit_cache_bytes;
+  TB_API_END
+}
+
 int tb_ctx_stream(tb_ctx ctx, void** stream) {
   TB_API_BEGIN
   REQUIRE_ARG(ctx != nullptr && stream != nullptr);

@@ -515,21 +515,21 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
 // the same absolute truncation error; numerically zero blocks keep one digit.
 // One warp per output group, lanes over its tasks.
 __global__ void k_task_slices(const I8TaskMeta* __restrict__ meta, const DevGroup* __restrict__ groups,
-                              int ngroups, const int32_t* __restrict__ blockmax, int smax,
-                              uint8_t* __restrict__ tslices) {
+                              int ngroups, const int32_t* __restrict__ amax, const int32_t* __restrict__ bmax,
+                              int smax, uint8_t* __restrict__ tslices) {
   constexpr int kNone = -1000000; // blockmax slots start at 0x80808080 (no nonzero row)
   const int     lane  = threadIdx.x & 31;
   for(int gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < ngroups; gi += (gridDim.x * blockDim.x) >> 5) {
     const DevGroup g  = groups[gi];
     int            eg = kNone;
     for(int t = g.task_begin + lane; t < g.task_end; t += 32) {
-      const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
+      const int ea = amax[meta[t].a_block], eb = bmax[meta[t].b_block];
       if(ea > kNone && eb > kNone) eg = max(eg, ea + eb + meta[t].log2k);
     }
 #pragma unroll
     for(int o = 16; o > 0; o >>= 1) eg = max(eg, __shfl_xor_sync(0xffffffffu, eg, o));
     for(int t = g.task_begin + lane; t < g.task_end; t += 32) {
-      const int ea = blockmax[meta[t].a_block], eb = blockmax[meta[t].b_block];
+      const int ea = amax[meta[t].a_block], eb = bmax[meta[t].b_block];
       int       s  = 1;
       if(ea > kNone && eb > kNone) s = max(1, smax - (eg - (ea + eb + meta[t].log2k)) / 8);
       tslices[t] = (uint8_t) s;
@@ -538,8 +538,10 @@ __global__ void k_task_slices(const I8TaskMeta* __restrict__ meta, const DevGrou
 }
 
 struct I8Params {
-  const uint8_t*  slices;
-  const int32_t*  exps;
+  const uint8_t*  a_slices; // digit slices of the A blocks (task a_off is relative to it)
+  const uint8_t*  b_slices;
+  const int32_t*  a_exps;   // row exponents (task a_exp / b_exp relative to these)
+  const int32_t*  b_exps;
   const I8Task*   tasks;
   const DevGroup* groups;
   const I8Item*   items;
@@ -648,8 +650,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         const DevGroup g    = p.groups[item.group];
         for(int t = g.task_begin; t < g.task_end; t++) {
           const I8Task   tk = p.tasks[t];
-          const uint8_t* ga = p.slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
-          const uint8_t* gb = p.slices + tk.b_off + (int64_t) item.nt * tk.nkc * B_BYTES;
+          const uint8_t* ga = p.a_slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
+          const uint8_t* gb = p.b_slices + tk.b_off + (int64_t) item.nt * tk.nkc * B_BYTES;
           const uint32_t st = p.tslices[t]; // only the task's leading digits travel
           const uint32_t ab = st * MT * 16, bb = st * NT * 16; // per K half
           for(int kc = 0; kc < tk.nkc; kc++) {
@@ -814,10 +816,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         // back) all passed the previous task's barrier below.
         const I8Task tk  = p.tasks[t];
         const int    st  = p.tslices[t];
-        const int    er  = __ldg(p.exps + tk.a_exp + item.mt * MT + row);
+        const int    er  = __ldg(p.a_exps + tk.a_exp + item.mt * MT + row);
         double*      scb = sc + (tcount & 1) * NT;
         constexpr int off = BF ? 0 : 7; // digit weights: 2^(e - 7 - 8d) (INT8), 2^e (BF16 pieces)
-        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.exps + tk.b_exp + item.nt * NT + et) - off);
+        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.b_exps + tk.b_exp + item.nt * NT + et) - off);
         // the epilogue threads agree on a timeout, so none is left in a barrier; the
         // barrier also publishes the scales
         const bool     waited = mbar_wait(tfull, tphase, p.err, 4);
@@ -957,20 +959,57 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 
 // ---------------------------------------------------------------- host side
 
+// Blocks split by one kernel: the staged kernel (rows contiguous) or the general one,
+// with their chunk table (first 8-row chunk of each block, then the total).
+struct SplitSet {
+  std::vector<SplitBlock> blocks;
+  std::vector<int32_t>    cbegin;
+  SplitBlock*             d_blocks = nullptr;
+  int32_t*                d_cbegin = nullptr;
+  int                     kmax     = 0;
+};
+
+// Digits of every stored, nonzero block of a read-only tensor under one operand view
+// (side, digit count, tile rows, element size, the label classes' rows / K of the
+// tensor's modes), kept in the context's arena while the tensor stays read-only, so
+// that constant operands (the integrals) are split once instead of in every
+// contraction that reads them.
+struct DigitEntry {
+  Arena*                        arena = nullptr;
+  int64_t*                      used  = nullptr; // the context's cache account
+  int64_t                       bytes = 0;
+  uint8_t*                      slices   = nullptr;
+  int32_t*                      exps     = nullptr;
+  int32_t*                      blockmax = nullptr;
+  int*                          err      = nullptr;
+  std::map<int64_t, SplitBlock> by_off; // element offset of a stored block -> its view here
+  SplitSet                      staged, general;
+  const double*                 src    = nullptr; // the tensor's packed store
+  bool                          filled = false;   // digits written (stream order)
+  ~DigitEntry() {
+    for(SplitSet* x: {&staged, &general}) {
+      cudaFree(x->d_blocks);
+      cudaFree(x->d_cbegin);
+    }
+    cudaFree(err);
+    if(arena) {
+      arena->deallocate(slices);
+      arena->deallocate(exps);
+      arena->deallocate(blockmax);
+    }
+    if(used) *used -= bytes;
+  }
+};
+
 struct I8Layout {
   int                     S = 0, NT = 0, esize = 1; // digits, output tile width, bytes per digit
   std::vector<SplitBlock> a_blocks, b_blocks;
   std::vector<int32_t>    a_cbegin, b_cbegin; // first 8-row chunk of each block, then the total
   // the blocks of each operand split by the staged kernel (rows contiguous) and by the
   // general one, each with its own chunk table
-  struct SplitSet {
-    std::vector<SplitBlock> blocks;
-    std::vector<int32_t>    cbegin;
-    SplitBlock*             d_blocks = nullptr;
-    int32_t*                d_cbegin = nullptr;
-    int                     kmax     = 0;
-  };
   SplitSet                a_staged, a_general, b_staged, b_general;
+  // cached digits of a read-only operand (the layout then holds none of its blocks)
+  std::shared_ptr<DigitEntry> a_cache, b_cache;
   std::vector<I8Task>     tasks;
   std::vector<I8TaskMeta> meta;
   std::vector<I8Item>     items;
@@ -1015,107 +1054,151 @@ int nt_for(int S) { return S <= 6 ? 80 : 64; }
 
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S, int NT, int esize) {
-  auto L   = std::make_shared<I8Layout>();
-  L->S     = S;
-  L->NT    = NT;
-  L->esize = esize;
+// The GEMM view of one operand block: rows = the outer labels (positions rpos, in C's
+// order), K = the inner labels (positions kpos, in A's order), element strides of the
+// block's row-major layout; tile_rows / kstep set the padding.
+SplitBlock view_block(const int32_t* dims, int nmodes, const int8_t* rpos, int nr, const int8_t* kpos, int nk,
+                      int tile_rows, int kstep) {
+  int64_t str[kMaxModes];
+  int64_t st = 1;
+  for(int i = nmodes - 1; i >= 0; i--) {
+    str[i] = st;
+    st *= dims[i];
+  }
+  SplitBlock b{};
+  b.nr   = nr;
+  b.nk   = nk;
+  b.rows = 1;
+  for(int j = 0; j < nr; j++) {
+    b.rdim[j] = dims[rpos[j]];
+    b.rstr[j] = (int32_t) str[rpos[j]];
+    b.rows *= b.rdim[j];
+  }
+  b.K = 1;
+  for(int j = 0; j < nk; j++) {
+    b.kdim[j] = dims[kpos[j]];
+    b.kstr[j] = (int32_t) str[kpos[j]];
+    b.K *= b.kdim[j];
+  }
+  b.kcontig = 1;
+  for(int j = 0; j < nk; j++) b.kcontig &= (kpos[j] == nmodes - nk + j) ? 1 : 0;
+  b.tile_rows = tile_rows;
+  b.rows_pad  = (int32_t) rup(b.rows, tile_rows);
+  b.K_pad     = (int32_t) rup(b.K, kstep);
+  return b;
+}
+
+// Staged-kernel eligibility: K contiguous, row r at element offset r * K, and two
+// 4-row stages of the longest row fit in shared memory.
+bool staged_ok(const SplitBlock& b, int esize) {
+  if(esize != 1 || !b.kcontig) return false;
+  int64_t st = b.K;
+  for(int j = b.nr - 1; j >= 0; j--) {
+    if(b.rstr[j] != st) return false;
+    st *= b.rdim[j];
+  }
+  return staged_stage_bytes(4, b.K) * 2 + kStagedHead <= kStagedSmem;
+}
+
+void chunk_table(const std::vector<SplitBlock>& bl, std::vector<int32_t>& out) {
+  out.resize(bl.size() + 1);
+  int64_t n = 0;
+  for(size_t i = 0; i < bl.size(); i++) {
+    out[i] = (int32_t) n;
+    n += bl[i].rows_pad / 8;
+  }
+  TB_EXPECTS(n < (1ll << 31), "too many split row groups");
+  out[bl.size()] = (int32_t) n;
+}
+
+void partition_sets(const std::vector<SplitBlock>& all, int esize, SplitSet& st, SplitSet& ge) {
+  for(const auto& b: all) {
+    SplitSet& x = staged_ok(b, esize) ? st : ge;
+    x.blocks.push_back(b);
+    x.kmax = std::max(x.kmax, b.K);
+  }
+  chunk_table(st.blocks, st.cbegin);
+  chunk_table(ge.blocks, ge.cbegin);
+}
+
+template<typename T>
+void upload_vec(T*& dptr, const std::vector<T>& vec) {
+  if(vec.empty()) return;
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&dptr), sizeof(T) * vec.size()));
+  TB_CUDA(cudaMemcpy(dptr, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice));
+}
+
+// ea / eb: cached digits of a read-only A / B (their blocks are not split per launch).
+std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& wl, int S, int NT, int esize,
+                                       const std::shared_ptr<DigitEntry>& ea = nullptr,
+                                       const std::shared_ptr<DigitEntry>& eb = nullptr) {
+  auto L     = std::make_shared<I8Layout>();
+  L->S       = S;
+  L->NT      = NT;
+  L->esize   = esize;
+  L->a_cache = ea;
+  L->b_cache = eb;
   const int kstep = KC / esize; // K elements per 32-byte MMA step
   std::map<int64_t, int> amap, bmap;
   int64_t                aexp = 0, bexp = 0, abytes = 0, bbytes = 0;
-  auto                   strides = [](const int32_t* dims, int n, int64_t* str) {
-    int64_t s = 1;
-    for(int i = n - 1; i >= 0; i--) {
-      str[i] = s;
-      s *= dims[i];
-    }
-  };
   L->tasks.resize(wl.tasks.size());
   L->meta.resize(wl.tasks.size());
+  auto cached = [](const std::shared_ptr<DigitEntry>& e, int64_t off) -> const SplitBlock& {
+    auto it = e->by_off.find(off);
+    TB_EXPECTS(it != e->by_off.end(), "read-only operand block missing from its digit cache");
+    return it->second;
+  };
   for(const auto& g: wl.groups) {
     for(int t = g.task_begin; t < g.task_end; t++) {
       const DevTask& tk = wl.tasks[t];
-      int64_t        astr[kMaxModes], bstr[kMaxModes];
-      strides(tk.adims, lc.na, astr);
-      strides(tk.bdims, lc.nb, bstr);
-      int32_t K = 1;
-      for(int j = 0; j < lc.nk; j++) K *= tk.adims[lc.k_a[j]];
-      auto ia = amap.find(tk.a_off);
-      if(ia == amap.end()) {
-        SplitBlock b{};
-        b.src_off = tk.a_off;
-        b.nr      = lc.nm;
-        b.nk      = lc.nk;
-        b.rows    = 1;
-        for(int j = 0; j < lc.nm; j++) {
-          b.rdim[j] = tk.adims[lc.m_a[j]];
-          b.rstr[j] = (int32_t) astr[lc.m_a[j]];
-          b.rows *= b.rdim[j];
+      const SplitBlock* A = nullptr;
+      const SplitBlock* B = nullptr;
+      if(ea) A = &cached(ea, tk.a_off);
+      else {
+        auto ia = amap.find(tk.a_off);
+        if(ia == amap.end()) {
+          SplitBlock b = view_block(tk.adims, lc.na, lc.m_a, lc.nm, lc.k_a, lc.nk, MT, kstep);
+          b.src_off    = tk.a_off;
+          b.id         = (int32_t) L->a_blocks.size();
+          b.dst_off    = abytes;
+          b.exp_off    = (int32_t) aexp;
+          abytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
+          aexp += b.rows_pad;
+          ia = amap.emplace(tk.a_off, (int) L->a_blocks.size()).first;
+          L->a_blocks.push_back(b);
         }
-        for(int j = 0; j < lc.nk; j++) {
-          b.kdim[j] = tk.adims[lc.k_a[j]];
-          b.kstr[j] = (int32_t) astr[lc.k_a[j]];
-        }
-        b.K         = K;
-        b.kcontig   = 1;
-        for(int j = 0; j < lc.nk; j++) b.kcontig &= (lc.k_a[j] == lc.na - lc.nk + j) ? 1 : 0;
-        b.id        = (int32_t) L->a_blocks.size();
-        b.tile_rows = MT;
-        b.rows_pad  = (int32_t) rup(b.rows, MT);
-        b.K_pad     = (int32_t) rup(K, kstep);
-        b.dst_off   = abytes;
-        b.exp_off   = (int32_t) aexp;
-        abytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
-        aexp += b.rows_pad;
-        ia = amap.emplace(tk.a_off, (int) L->a_blocks.size()).first;
-        L->a_blocks.push_back(b);
+        A = &L->a_blocks[ia->second];
       }
-      auto ib = bmap.find(tk.b_off);
-      if(ib == bmap.end()) {
-        SplitBlock b{};
-        b.src_off = tk.b_off;
-        b.nr      = lc.nn;
-        b.nk      = lc.nk;
-        b.rows    = 1;
-        for(int j = 0; j < lc.nn; j++) {
-          b.rdim[j] = tk.bdims[lc.n_b[j]];
-          b.rstr[j] = (int32_t) bstr[lc.n_b[j]];
-          b.rows *= b.rdim[j];
+      if(eb) B = &cached(eb, tk.b_off);
+      else {
+        auto ib = bmap.find(tk.b_off);
+        if(ib == bmap.end()) {
+          SplitBlock b = view_block(tk.bdims, lc.nb, lc.n_b, lc.nn, lc.k_b, lc.nk, L->NT, kstep);
+          b.src_off    = tk.b_off;
+          b.id         = (int32_t) L->b_blocks.size(); // rebased after the A blocks below
+          b.dst_off    = bbytes;
+          b.exp_off    = (int32_t) bexp;
+          bbytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
+          bexp += b.rows_pad;
+          ib = bmap.emplace(tk.b_off, (int) L->b_blocks.size()).first;
+          L->b_blocks.push_back(b);
         }
-        for(int j = 0; j < lc.nk; j++) {
-          b.kdim[j] = tk.bdims[lc.k_b[j]];
-          b.kstr[j] = (int32_t) bstr[lc.k_b[j]];
-        }
-        b.K         = K;
-        b.kcontig   = 1;
-        for(int j = 0; j < lc.nk; j++) b.kcontig &= (lc.k_b[j] == lc.nb - lc.nk + j) ? 1 : 0;
-        b.id        = (int32_t) L->b_blocks.size(); // rebased after the A blocks below
-        b.tile_rows = L->NT;
-        b.rows_pad  = (int32_t) rup(b.rows, L->NT);
-        b.K_pad     = (int32_t) rup(K, kstep);
-        b.dst_off   = bbytes;
-        b.exp_off   = (int32_t) bexp;
-        bbytes += (int64_t) b.rows_pad * b.K_pad * esize * S;
-        bexp += b.rows_pad;
-        ib = bmap.emplace(tk.b_off, (int) L->b_blocks.size()).first;
-        L->b_blocks.push_back(b);
+        B = &L->b_blocks[ib->second];
       }
-      const SplitBlock& A = L->a_blocks[ia->second];
-      const SplitBlock& B = L->b_blocks[ib->second];
-      I8Task            it{};
-      it.a_off     = A.dst_off;
-      it.b_off     = B.dst_off; // rebased below
-      it.a_exp     = A.exp_off;
-      it.b_exp     = B.exp_off;
-      it.nkc       = A.K_pad / kstep;
-      L->tasks[t]  = it;
+      I8Task it{};
+      it.a_off    = A->dst_off;
+      it.b_off    = B->dst_off; // rebased below (layout blocks)
+      it.a_exp    = A->exp_off;
+      it.b_exp    = B->exp_off;
+      it.nkc      = A->K_pad / kstep;
+      L->tasks[t] = it;
       I8TaskMeta mt{};
-      mt.a_block = A.id;
-      mt.b_block = B.id; // rebased below
+      mt.a_block = A->id;
+      mt.b_block = B->id; // rebased below (layout blocks)
       int lk = 0;
-      while((1ll << lk) < K) lk++;
-      mt.log2k    = lk;
-      L->meta[t]  = mt;
+      while((1ll << lk) < A->K) lk++;
+      mt.log2k   = lk;
+      L->meta[t] = mt;
     }
   }
   TB_EXPECTS(aexp + bexp < (1ll << 31), "too many split rows");
@@ -1124,10 +1207,12 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
     b.exp_off += (int32_t) aexp;
     b.id += (int32_t) L->a_blocks.size();
   }
-  for(auto& m: L->meta) m.b_block += (int32_t) L->a_blocks.size();
-  for(auto& t: L->tasks) {
-    t.b_off += abytes;
-    t.b_exp += (int32_t) aexp;
+  if(!eb) { // layout B blocks sit after the layout A blocks in the scratch arrays
+    for(auto& m: L->meta) m.b_block += (int32_t) L->a_blocks.size();
+    for(auto& t: L->tasks) {
+      t.b_off += abytes;
+      t.b_exp += (int32_t) aexp;
+    }
   }
   L->a_bytes     = abytes;
   L->slice_bytes = abytes + bbytes;
@@ -1144,28 +1229,8 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   chunks(L->a_blocks, L->a_cbegin);
   chunks(L->b_blocks, L->b_cbegin);
-  // staged-kernel eligibility: K contiguous, row r at element offset r * K, and two
-  // 4-row stages of the longest row fit in shared memory
-  auto staged_ok = [&](const SplitBlock& b) {
-    if(esize != 1 || !b.kcontig) return false;
-    int64_t st = b.K;
-    for(int j = b.nr - 1; j >= 0; j--) {
-      if(b.rstr[j] != st) return false;
-      st *= b.rdim[j];
-    }
-    return staged_stage_bytes(4, b.K) * 2 + kStagedHead <= kStagedSmem;
-  };
-  auto partition = [&](const std::vector<SplitBlock>& all, I8Layout::SplitSet& st, I8Layout::SplitSet& ge) {
-    for(const auto& b: all) {
-      I8Layout::SplitSet& x = staged_ok(b) ? st : ge;
-      x.blocks.push_back(b);
-      x.kmax = std::max(x.kmax, b.K);
-    }
-    chunks(st.blocks, st.cbegin);
-    chunks(ge.blocks, ge.cbegin);
-  };
-  partition(L->a_blocks, L->a_staged, L->a_general);
-  partition(L->b_blocks, L->b_staged, L->b_general);
+  partition_sets(L->a_blocks, esize, L->a_staged, L->a_general);
+  partition_sets(L->b_blocks, esize, L->b_staged, L->b_general);
   // output tiles, longest group first (every tile of a group costs the same, so
   // ordering the groups orders the tiles)
   std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
@@ -1196,7 +1261,7 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   };
   up(L->d_ablocks, L->a_blocks);
   up(L->d_bblocks, L->b_blocks);
-  for(I8Layout::SplitSet* x: {&L->a_staged, &L->a_general, &L->b_staged, &L->b_general}) {
+  for(SplitSet* x: {&L->a_staged, &L->a_general, &L->b_staged, &L->b_general}) {
     up(x->d_blocks, x->blocks);
     up(x->d_cbegin, x->cbegin);
   }
@@ -1222,7 +1287,7 @@ int sm_count() {
 }
 
 template<int S, int R>
-void launch_staged(const I8Layout::SplitSet& x, const double* src, uint8_t* slices, int32_t* exps,
+void launch_staged(const SplitSet& x, const double* src, uint8_t* slices, int32_t* exps,
                    int32_t* blockmax, int* err, cudaStream_t st) {
   const int      nblocks = (int) x.cbegin.size() - 1, nchunks = x.cbegin.back();
   const uint32_t sb      = (uint32_t) staged_stage_bytes(R, x.kmax);
@@ -1240,35 +1305,49 @@ void launch_staged(const I8Layout::SplitSet& x, const double* src, uint8_t* slic
                                                 blockmax, err);
 }
 
+// Splits the blocks of one operand: the staged kernel for the blocks with contiguous
+// rows, the general kernel for the rest.
+template<int S, bool BF>
+void split_sets(const SplitSet& staged, const SplitSet& general, const double* src, uint8_t* slices,
+                int32_t* exps, int32_t* blockmax, int* err, cudaStream_t st) {
+  if(!general.blocks.empty() && general.cbegin.back() > 0) {
+    const int nblocks = (int) general.cbegin.size() - 1, nchunks = general.cbegin.back();
+    k_split_fused<S, BF><<<std::min(nchunks, sm_count() * 8), 256, 0, st>>>(general.d_blocks, general.d_cbegin,
+                                                                            nblocks, nchunks, src, slices, exps,
+                                                                            blockmax);
+  }
+  if constexpr(!BF) {
+    if(!staged.blocks.empty() && staged.cbegin.back() > 0) {
+      // 8-row units while three stages of the longest row fit, else 4-row units
+      if(kStagedHead + 3 * staged_stage_bytes(8, staged.kmax) <= kStagedSmem)
+        launch_staged<S, 8>(staged, src, slices, exps, blockmax, err, st);
+      else launch_staged<S, 4>(staged, src, slices, exps, blockmax, err, st);
+    }
+  }
+}
+
 template<int S, bool BF>
 void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const double* B, uint8_t* slices,
                   int32_t* exps, cudaStream_t st) {
-  const int grid_cap = sm_count() * 8;
+  // a read-only operand's cached digits are split once, on first use
+  for(DigitEntry* e: {L.a_cache.get(), L.b_cache.get()})
+    if(e && !e->filled) {
+      TB_CUDA(cudaMemsetAsync(e->blockmax, 0x80, sizeof(int32_t) * std::max<size_t>(e->by_off.size(), 1), st));
+      split_sets<S, BF>(e->staged, e->general, e->src, e->slices, e->exps, e->blockmax, e->err, st);
+      e->filled = true;
+    }
   // 0x80808080: below every exponent sum, marks blocks without a nonzero row
   TB_CUDA(cudaMemsetAsync(L.d_blockmax, 0x80, sizeof(int32_t) * (L.a_blocks.size() + L.b_blocks.size()), st));
-  auto one = [&](const I8Layout::SplitSet& staged, const I8Layout::SplitSet& general, const double* src) {
-    if(!general.blocks.empty() && general.cbegin.back() > 0) {
-      const int nblocks = (int) general.cbegin.size() - 1, nchunks = general.cbegin.back();
-      k_split_fused<S, BF><<<std::min(nchunks, grid_cap), 256, 0, st>>>(general.d_blocks, general.d_cbegin, nblocks,
-                                                                          nchunks, src, slices, exps, L.d_blockmax);
-    }
-    if constexpr(!BF) {
-      if(!staged.blocks.empty() && staged.cbegin.back() > 0) {
-        // 8-row units while three stages of the longest row fit, else 4-row units
-        if(kStagedHead + 3 * staged_stage_bytes(8, staged.kmax) <= kStagedSmem)
-          launch_staged<S, 8>(staged, src, slices, exps, L.d_blockmax, L.d_err, st);
-        else launch_staged<S, 4>(staged, src, slices, exps, L.d_blockmax, L.d_err, st);
-      }
-    }
-  };
-  one(L.a_staged, L.a_general, A);
-  one(L.b_staged, L.b_general, B);
+  split_sets<S, BF>(L.a_staged, L.a_general, A, slices, exps, L.d_blockmax, L.d_err, st);
+  split_sets<S, BF>(L.b_staged, L.b_general, B, slices, exps, L.d_blockmax, L.d_err, st);
   const int ng = (int) wl.groups.size();
   if constexpr(BF) { // both bf16 pieces in every task
     if(!L.tasks.empty()) TB_CUDA(cudaMemsetAsync(L.d_tslices, S, L.tasks.size(), st));
   }
   else if(ng > 0)
-    k_task_slices<<<(ng + 7) / 8, 256, 0, st>>>(L.d_meta, wl.d_groups, ng, L.d_blockmax, S, L.d_tslices);
+    k_task_slices<<<(ng + 7) / 8, 256, 0, st>>>(L.d_meta, wl.d_groups, ng,
+                                                L.a_cache ? L.a_cache->blockmax : L.d_blockmax,
+                                                L.b_cache ? L.b_cache->blockmax : L.d_blockmax, S, L.d_tslices);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -1277,8 +1356,10 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
                  const uint8_t* slices, const int32_t* exps, double* C, cudaStream_t st) {
   if(L.items.empty()) return;
   I8Params p;
-  p.slices = slices;
-  p.exps   = exps;
+  p.a_slices = L.a_cache ? L.a_cache->slices : slices;
+  p.b_slices = L.b_cache ? L.b_cache->slices : slices;
+  p.a_exps   = L.a_cache ? L.a_cache->exps : exps;
+  p.b_exps   = L.b_cache ? L.b_cache->exps : exps;
   p.tasks  = L.d_tasks;
   p.groups = wl.d_groups;
   p.items  = L.d_items;
@@ -1334,6 +1415,71 @@ int slices_for(double err_target) {
 
 std::map<const WorkList*, std::shared_ptr<I8Layout>> g_layouts; // per work list, keyed by S below
 
+// The cached digits of read-only tensor T as operand `side` (0 = A, 1 = B) of a
+// contraction with the plan's label classes, for S digits, `tile_rows` rows per tile
+// and esize-byte elements: every stored block the scan did not find zero, split on
+// first use (launch_split) into arena memory counted against the context's cache
+// budget.  Null when the budget does not allow it.
+std::shared_ptr<DigitEntry> digit_entry(const Plan& plan, const Tensor* T, int side, int S, int tile_rows,
+                                        int esize) {
+  if(T == nullptr || plan.cache_used == nullptr || plan.arena == nullptr || !T->read_only) return nullptr;
+  const LabelClasses& lc = plan.lc;
+  const int8_t*       rp = side == 0 ? lc.m_a : lc.n_b;
+  const int           nr = side == 0 ? lc.nm : lc.nn;
+  const int8_t*       kp = side == 0 ? lc.k_a : lc.k_b;
+  std::string         key = std::to_string(side) + "|" + std::to_string(S) + "|" + std::to_string(tile_rows) + "|" +
+                    std::to_string(esize) + "|";
+  for(int j = 0; j < nr; j++) key += std::to_string(rp[j]) + ",";
+  key += "|";
+  for(int j = 0; j < lc.nk; j++) key += std::to_string(kp[j]) + ",";
+  auto hit = T->digit_cache.find(key);
+  if(hit != T->digit_cache.end()) return std::static_pointer_cast<DigitEntry>(hit->second);
+  auto                    e     = std::make_shared<DigitEntry>();
+  const int               kstep = KC / esize;
+  int64_t                 sbytes = 0, nexp = 0;
+  std::vector<SplitBlock> all;
+  std::vector<int64_t>    bid(T->nmodes);
+  int32_t                 dims[kMaxModes];
+  for(size_t b = 0; b < T->keys.size(); b++) {
+    if(!T->zero_block.empty() && T->zero_block[b]) continue; // its tasks never run
+    int64_t k = T->keys[b];
+    for(int m = T->nmodes - 1; m >= 0; m--) {
+      bid[m] = k % T->tis[m]->ntiles();
+      k /= T->tis[m]->ntiles();
+    }
+    for(int m = 0; m < T->nmodes; m++) dims[m] = (int32_t) T->tis[m]->size(bid[m]);
+    SplitBlock v = view_block(dims, T->nmodes, rp, nr, kp, lc.nk, tile_rows, kstep);
+    v.src_off    = T->offsets[b];
+    v.id         = (int32_t) all.size();
+    v.dst_off    = sbytes;
+    v.exp_off    = (int32_t) nexp;
+    sbytes += (int64_t) v.rows_pad * v.K_pad * esize * S;
+    nexp += v.rows_pad;
+    TB_EXPECTS(nexp < (1ll << 31), "too many split rows");
+    all.push_back(v);
+    e->by_off[v.src_off] = v;
+  }
+  const int64_t total = sbytes + 4 * nexp + 4 * (int64_t) std::max<size_t>(all.size(), 1);
+  if(*plan.cache_used + total > plan.cache_limit) return nullptr;
+  e->arena    = plan.arena;
+  e->slices   = static_cast<uint8_t*>(plan.arena->allocate(std::max<int64_t>(sbytes, 1)));
+  e->exps     = static_cast<int32_t*>(plan.arena->allocate(4 * std::max<int64_t>(nexp, 1)));
+  e->blockmax = static_cast<int32_t*>(plan.arena->allocate(4 * (int64_t) std::max<size_t>(all.size(), 1)));
+  e->used     = plan.cache_used;
+  e->bytes    = total;
+  *e->used += total;
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&e->err), sizeof(int)));
+  TB_CUDA(cudaMemset(e->err, 0, sizeof(int)));
+  partition_sets(all, esize, e->staged, e->general);
+  for(SplitSet* x: {&e->staged, &e->general}) {
+    upload_vec(x->d_blocks, x->blocks);
+    upload_vec(x->d_cbegin, x->cbegin);
+  }
+  e->src                  = T->data;
+  T->digit_cache[key]     = e;
+  return e;
+}
+
 } // namespace
 
 // Split contraction, shared by the split-INT8 mode (bf = false: S balanced INT8 digits)
@@ -1351,8 +1497,12 @@ void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* 
   const int esize = bf ? 2 : 1;
   TB_EXPECTS((NT == 48 || NT == 64 || NT == 80) && S * NT <= 512,
              "split output tile width must be 48, 64 or 80 with slices x width <= 512");
-  auto& L = g_layouts[&wl];
-  if(!L || L->S != S || L->NT != NT || L->esize != esize) L = build_layout(lc, wl, S, NT, esize);
+  // digits of read-only operands kept across contractions (when the context allows it)
+  const auto ea = digit_entry(plan, plan.cache_a, 0, S, MT, esize);
+  const auto eb = digit_entry(plan, plan.cache_b, 1, S, NT, esize);
+  auto&      L  = g_layouts[&wl];
+  if(!L || L->S != S || L->NT != NT || L->esize != esize || L->a_cache != ea || L->b_cache != eb)
+    L = build_layout(lc, wl, S, NT, esize, ea, eb);
   Scratch sc;
   sc.stream = stream;
   sc.arena  = plan.arena;
@@ -1536,10 +1686,12 @@ void noalloc_launch(const NoAllocDesc& d, unsigned char* base, int64_t exps_off,
   const int cap = sm_count() * 8;
   k_split_fused<S, false><<<std::min(d.nchunk_a, cap), 256, 0, st>>>(sb, cb, 1, d.nchunk_a, A, sl, exps, bmax);
   k_split_fused<S, false><<<std::min(d.nchunk_b, cap), 256, 0, st>>>(sb + 1, cb + 2, 1, d.nchunk_b, B, sl, exps, bmax);
-  k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, S, tsl);
+  k_task_slices<<<1, 32, 0, st>>>(meta, grp, 1, bmax, bmax, S, tsl);
   I8Params p{};
-  p.slices  = sl;
-  p.exps    = exps;
+  p.a_slices = sl;
+  p.b_slices = sl;
+  p.a_exps   = exps;
+  p.b_exps   = exps;
   p.tasks   = tsk;
   p.groups  = grp;
   p.items   = reinterpret_cast<const I8Item*>(base + kCtlItems);

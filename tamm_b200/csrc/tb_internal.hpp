@@ -98,6 +98,7 @@ struct WorkList {
 };
 
 class Arena;
+struct Tensor;
 
 // Scratch of a captured CUDA graph: buffers stay allocated for the graph's lifetime;
 // ops of the graph run in stream order, so a buffer returned by one op can serve the
@@ -128,6 +129,12 @@ struct Plan {
   // belongs to exactly one output tile); blocks of groups without tasks are left
   // untouched
   bool         store        = false;
+  // read-only operands whose split digits may be kept (tb_ctx_set_digit_cache), and the
+  // context's cache account
+  const Tensor* cache_a = nullptr;
+  const Tensor* cache_b = nullptr;
+  int64_t       cache_limit = 0;
+  int64_t*      cache_used  = nullptr;
 };
 
 void forget_int8_layout(const WorkList* wl);

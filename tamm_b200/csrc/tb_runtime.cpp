@@ -368,6 +368,7 @@ bool Tensor::block_is_zero(const int64_t* blockid) const {
 // context's stream (after the work already enqueued there, which includes the waits
 // for asynchronous host writes) for blocks whose elements are all zero.
 void set_read_only(Tensor& T, bool on) {
+  T.digit_cache.clear(); // (entries still used by cached layouts live until those go)
   if(!on) {
     T.read_only = false;
     T.zero_block.clear();
@@ -864,6 +865,10 @@ void Sched::run(Op& op) {
   op.plan->profile      = profiling;
   op.plan->pinned       = pinned;
   op.plan->check_errors = pinned == nullptr && !deferred_checks;
+  op.plan->cache_limit  = ctx->digit_cache_bytes;
+  op.plan->cache_used   = &ctx->digit_cache_used;
+  op.plan->cache_a      = ctx->digit_cache_bytes > 0 && op.a.t->read_only ? op.a.t : nullptr;
+  op.plan->cache_b      = ctx->digit_cache_bytes > 0 && op.b.t->read_only ? op.b.t : nullptr;
   op.flops              = op.wl->flops;
   run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
                ctx->arena.get());

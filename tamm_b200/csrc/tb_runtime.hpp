@@ -51,6 +51,8 @@ struct Ctx {
   int                    mode       = TB_MODE_FP64;
   double                 err_target = 1e-11;
   int                    nslices    = 0;
+  int64_t                digit_cache_bytes = 0; // split digits of read-only operands kept, at most
+  int64_t                digit_cache_used  = 0;
   ~Ctx();
 };
 
@@ -128,6 +130,9 @@ struct Tensor {
   bool                              read_only = false;
   uint64_t                          ro_serial = 0;
   std::vector<uint8_t>              zero_block;
+  // split digits of this (read-only) tensor per operand view, kept by the split-INT8
+  // contraction (opaque here; dropped whenever the read-only mark changes)
+  mutable std::map<std::string, std::shared_ptr<void>> digit_cache;
   // lambda tensor (tb_tensor_create_lambda / _built): no storage, blocks on demand
   tb_block_fn                       lambda_block = nullptr;
   tb_batch_fn                       lambda_batch = nullptr;

@@ -62,6 +62,17 @@ class ExecutionContext:
         call("tb_ctx_set_precision", self.h, int(mode), float(err_target), int(nslices))
 
     @property
+    def set_digit_cache(self, nbytes: int):
+        """Keep up to nbytes of split-INT8 digits of read-only tensors across contractions."""
+        call("tb_ctx_set_digit_cache", self.h, int(nbytes))
+        return self
+
+    def digit_cache_info(self):
+        """(bytes kept, limit) of the digit cache."""
+        u, l = C.c_int64(), C.c_int64()
+        call("tb_ctx_digit_cache_info", self.h, C.byref(u), C.byref(l))
+        return u.value, l.value
+
     def stream(self):
         s = A.vp()
         call("tb_ctx_stream", self.h, C.byref(s))

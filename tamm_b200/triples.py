@@ -192,8 +192,11 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=4)
     p.add_argument("--steps", type=int, default=8)
     p.add_argument("--pool-gib", type=int, default=80)
+    p.add_argument("--digit-cache-gib", type=int, default=16,
+                   help="split-INT8 digits of the read-only integrals kept across contractions (0: off)")
     args = p.parse_args(argv)
     ec = ExecutionContext(0, args.pool_gib << 30)
+    ec.set_digit_cache(args.digit_cache_gib << 30)
     P = build(args.oa, args.va, tile=args.tile, jtile=args.jtile, dtile=args.dtile, seed=args.seed, ec=ec)
     allsteps = steps(P)
     rng = np.random.default_rng(args.seed + 5)

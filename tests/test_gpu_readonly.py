@@ -172,3 +172,37 @@ def test_structural_zeros_within_one_execute(ec):
         ec.set_precision(tb.Precision.FP64)
     assert st8["flops_run"] == st1["flops_run"]
     assert rel_err(joint8, apart) <= 1e-11
+
+
+def test_digit_cache_bitwise_and_bounded(ec):
+    """With the digit cache on, the read-only v is split once and kept: two contractions
+    in a row give the bits of the per-call split, the cache holds bytes, a budget too
+    small keeps nothing, and clearing the mark releases them."""
+    lad, vh, zero = _ladder_with_zero_blocks(ec, seed=13)
+    a, b, c, d, i, j = lad.labels
+    want = _oracle(lad, vh)
+    lad.v.set_read_only(True)
+
+    def run():
+        lad.sch(lad.r2().assign(0.0)).execute()
+        lad.sch(lad.r2(a, b, i, j).iadd(lad.v(a, b, c, d) * lad.t2(c, d, i, j))).execute()
+        return lad.r2.read()
+
+    ec.set_precision(tb.Precision.INT8, 1e-11)
+    try:
+        plain = run()
+        ec.set_digit_cache(1 << 30)
+        first, second = run(), run()
+        used, limit = ec.digit_cache_info()
+        assert used > 0 and limit == 1 << 30
+        assert np.array_equal(first, plain) and np.array_equal(second, plain)
+        assert rel_err(second, want) <= 1e-11
+        lad.v.set_read_only(False)  # drops the entries (and the work lists keyed by the mark)
+        run()
+        lad.v.set_read_only(True)
+        ec.set_digit_cache(1)  # too small for any entry: split per call, same bits
+        assert np.array_equal(run(), plain)
+    finally:
+        ec.set_digit_cache(0)
+        ec.set_precision(tb.Precision.FP64)
+        lad.v.set_read_only(False)
