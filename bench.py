@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--ccsd-oa", type=int, default=30)
     p.add_argument("--ccsd-va", type=int, default=240)
     p.add_argument("--shard", action="store_true", help="owner-computes path with an all-reduce even at N=1")
+    p.add_argument("--adjoint", action="store_true", help="also time the energy gradient (O=30, V=240)")
+    p.add_argument("--triples", action="store_true", help="also time sampled triples-energy steps (O=50, V=500)")
+    p.add_argument("--triples-steps", type=int, default=4)
     p.add_argument("--workload", default="ladder", choices=["ladder", "blockops"],
                    help="blockops: the HBM-bound block kernels on the ladder's r2 (one JSON line, GB/s)")
     return p.parse_args()
@@ -239,6 +242,68 @@ def load_peaks():
             return json.load(f)
     except Exception:
         return {}
+
+
+def measure_adjoint(ec, torch):
+    """Energy + gradient of E(t2) = w.t2 + 1/4 t2.(v t2) at O=30, V=240 through the tape,
+    FP64 and split-INT8 (v read-only, its digits kept): device time of one evaluation
+    after a warm-up, FP64-equivalent TFLOP/s of its two contractions."""
+    import tamm_b200 as tb
+    from tamm_b200 import workloads as W
+    P = W.energy_problem(15, 120, seed=3, ec=ec)
+    stream = torch.cuda.ExternalStream(ec.stream)
+    flops = 2.0 * P.lad.flops
+    out, grads = {"workload": "ccsd_energy_gradient_O30_V240", "admitted_flops_per_gradient": flops}, {}
+    ec.set_digit_cache(int(8 * 2 ** 30))
+    for name, mode in (("fp64", tb.Precision.FP64), ("int8", tb.Precision.INT8)):
+        ec.set_precision(mode, 1e-11)
+        W.energy(P, gradient=True)
+        ec.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        W.energy(P, gradient=True)
+        e1.record(stream)
+        ec.synchronize()
+        ms = e0.elapsed_time(e1)
+        grads[name] = P.g.read()
+        out[name] = {"gradient_ms": ms, "tflops": flops / ms / 1e9}
+    ec.set_precision(tb.Precision.FP64)
+    ec.set_digit_cache(0)
+    out["speedup_int8_vs_fp64"] = out["fp64"]["gradient_ms"] / out["int8"]["gradient_ms"]
+    out["int8_vs_fp64_gradient_max_rel_err"] = float(np.max(np.abs(grads["int8"] - grads["fp64"])) /
+                                                     np.max(np.abs(grads["fp64"])))
+    P.lad.v.set_read_only(False)
+    P.lad.sch.deallocate(P.lad.v, P.lad.t2, P.lad.r2, P.w, P.X, P.g)
+    return out
+
+
+def measure_triples(ec, torch, nsteps):
+    """Sampled steps of the streamed triples energy at O=50, V=500, tile 40 (j blocks of
+    2, the summed d one tile per spin block), FP64 and split-INT8 (integrals read-only,
+    their digits kept): device time of the sample, FP64-equivalent TFLOP/s."""
+    import tamm_b200 as tb
+    from tamm_b200 import triples as T3
+    P = T3.build(25, 250, tile=40, jtile=2, dtile=0, seed=4, ec=ec)
+    allsteps = T3.steps(P)
+    rng = np.random.default_rng(9)
+    sample = [allsteps[int(x)] for x in rng.choice(len(allsteps), size=nsteps, replace=False)]
+    out, es = {"workload": "triples_energy_O50_V500_tile40", "sampled_steps": sample, "steps_total": len(allsteps)}, {}
+    ec.set_digit_cache(int(24 * 2 ** 30))
+    for name, mode in (("fp64", tb.Precision.FP64), ("int8", tb.Precision.INT8)):
+        ec.set_precision(mode, 1e-11)
+        sch = tb.Scheduler(ec)
+        T3.energy(P, sample[:1], sch)  # warm-up
+        e, fl, ms = T3.energy(P, sample, sch)
+        es[name] = e
+        out[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9}
+    ec.set_precision(tb.Precision.FP64)
+    ec.set_digit_cache(0)
+    out["speedup_int8_vs_fp64"] = out["fp64"]["ms"] / out["int8"]["ms"]
+    out["int8_vs_fp64_energy_rel_err"] = abs(es["int8"] - es["fp64"]) / abs(es["fp64"])
+    for t in P.T.values():
+        t.set_read_only(False)
+        t.deallocate()
+    return out
 
 
 def run_blockops(args, torch, tb, W, local):
@@ -511,6 +576,8 @@ def main():
                      "flops": P.flops, "ops_per_iteration": len(CC._ops(P)) + 3,
                      "ladder_batches": P.ladder_batches, **res}
         del P
+    adjoint_line = measure_adjoint(ec, torch) if args.adjoint else None
+    triples_line = measure_triples(ec, torch, args.triples_steps) if args.triples else None
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -546,9 +613,11 @@ def main():
             "gpu_launches": args.steps * {"int8": 4, "bf16x3": 3, "fp64": 1}[headline],
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "ccsd_iteration": ccsd_line,
+            "adjoint": adjoint_line,
+            "triples": triples_line,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if shard:
         dist.destroy_process_group()
 
 

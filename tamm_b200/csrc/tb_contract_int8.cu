@@ -107,6 +107,20 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return e;
 }
 
+constexpr int kStagedWarps = 16; // consumer warps of k_split_staged (plus one producer warp)
+
+// round(x * 2^sh) + bias as a 64-bit word whose bytes are the balanced digits + 128.
+// For S <= 6 (|X| < 2^47) one FMA against 1.5 * 2^52 leaves the integer, rounded to
+// nearest even, in the low mantissa bits (2^52 + 2^51 + X); larger S convert directly.
+template<int S>
+__device__ __forceinline__ uint64_t digit_word(double x, double f, uint64_t bias) {
+  if constexpr(S <= 6) {
+    const uint64_t t = (uint64_t) __double_as_longlong(fma(x, f, 6755399441055744.0));
+    return t + (bias - ((uint64_t) 1075 << 52) - ((uint64_t) 1 << 51));
+  }
+  else return (uint64_t) __double2ll_rn(x * f) + bias;
+}
+
 // Split in one pass over HBM: persistent CTAs, each taking 8-row groups ("chunks") in
 // turn.  Phase 1, warp w streams row w
 // (16-byte loads from the row's first 16-byte boundary, eight in flight per lane) for
@@ -272,7 +286,7 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
         uint32_t lo[4], hi[4];
 #pragma unroll
         for(int x = 0; x < 4; x++) {
-          const uint64_t Y = (uint64_t) __double2ll_rn(v[x] * f1 * f2) + bias;
+          const uint64_t Y = digit_word<S>(v[x] * f2, f1, bias);
           lo[x]            = (uint32_t) Y;
           hi[x]            = (uint32_t) (Y >> 32);
         }
@@ -332,7 +346,7 @@ __host__ __device__ constexpr int64_t staged_stage_bytes(int R, int64_t K) {
 }
 
 template<int S, int R>
-__global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __restrict__ blocks,
+__global__ void __launch_bounds__(32 * (kStagedWarps + 1), 1) k_split_staged(const SplitBlock* __restrict__ blocks,
                                                         const int32_t* __restrict__ chunk_begin, int nblocks,
                                                         int nchunks, int nst, uint32_t stage_bytes,
                                                         const double* __restrict__ src, uint8_t* __restrict__ dst,
@@ -344,8 +358,8 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
   uint64_t*     empty = full + 8;
   StageMeta*    meta  = reinterpret_cast<StageMeta*>(empty + 8);
   float*        pmax  = reinterpret_cast<float*>(meta + 8); // unused padding keeps 128-byte alignment below
-  double*       part  = reinterpret_cast<double*>(sm + 512);   // [2][8] partial row maxima
-  int32_t*      shift = reinterpret_cast<int32_t*>(part + 16); // [2][8] digit shifts
+  double*       part  = reinterpret_cast<double*>(sm + 384);   // [2][kStagedWarps] partial row maxima
+  int32_t*      shift = reinterpret_cast<int32_t*>(part + 2 * kStagedWarps); // [2][8] digit shifts
   uint8_t*      ring  = sm + 1024;
   (void) pmax;
   const int     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -354,7 +368,7 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
   if(threadIdx.x == 0) {
     for(int x = 0; x < nst; x++) {
       mbar_init(&full[x], 1);
-      mbar_init(&empty[x], 8); // one arrival per consumer warp
+      mbar_init(&empty[x], kStagedWarps); // one arrival per consumer warp
     }
     fence_mbarrier_init();
   }
@@ -402,8 +416,8 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
     }
     return;
   }
-  // ---------------- consumers: warps 1..8 ----------------
-  const int cw  = warp - 1; // 0..7
+  // ---------------- consumers: warps 1..kStagedWarps ----------------
+  const int cw  = warp - 1;
   const int ctid = threadIdx.x - 32;
   int       slot = 0;
   uint32_t  ph   = 0;
@@ -414,7 +428,7 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
       asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
                    "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
                    : "=r"(anyfail)
-                   : "r"((uint32_t) got), "n"(256)
+                   : "r"((uint32_t) got), "n"(32 * kStagedWarps)
                    : "memory");
       if(anyfail) return;
     }
@@ -430,10 +444,10 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
       // ordered before the bulk copy that later refills this stage
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     }
-    if(m.tail) asm volatile("bar.sync 1, 256;\n" ::: "memory");
-    // row maxima: 8 / R warps per row, each over its share of K
+    if(m.tail) asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
+    // row maxima: kStagedWarps / R warps per row, each over its share of K
     {
-      constexpr int WPR = 8 / R;
+      constexpr int WPR = kStagedWarps / R;
       const int     r = cw % R, sh = cw / R;
       double        mx = 0.0;
       if(r < m.nlive) {
@@ -443,34 +457,36 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
       }
 #pragma unroll
       for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if(lane == 0) part[par * 8 + cw] = mx;
+      if(lane == 0) part[par * kStagedWarps + cw] = mx;
     }
-    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
     if(ctid < R) {
       const int r   = ctid;
       double    mx  = 0.0;
-      for(int w = r; w < 8; w += R) mx = fmax(mx, part[par * 8 + w]);
+      for(int w = r; w < kStagedWarps; w += R) mx = fmax(mx, part[par * kStagedWarps + w]);
       const bool live = r < m.nlive;
       const int  e    = row_exponent(mx);
       shift[par * 8 + r] = live ? 8 * S - 1 - e : kPadRow;
       exps[b.exp_off + m.row0 + r] = e;
       if(mx > 0.0) atomicMax(blockmax + b.id, e);
     }
-    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
     // digits: lanes per 16-wide k chunk = 4 R (row, quad); 32 / (4 R) chunks per warp step
     {
       constexpr int LPC = 4 * R, CPW = 32 / LPC;
       const int     rr = (lane % LPC) >> 2, q = lane & 3, sub = lane / LPC;
       const int     sh = shift[par * 8 + rr];
       const bool    live = sh != kPadRow;
-      const double  f1 = ldexp(1.0, live ? sh / 2 : 0), f2 = ldexp(1.0, live ? sh - sh / 2 : 0);
+      // 2^sh in one factor where it is a normal double, else as two (tiny rows)
+      const bool    wide = live && (sh > 1000 || sh < -1000);
+      const double  f1 = ldexp(1.0, live ? (wide ? sh / 2 : sh) : 0), f2 = ldexp(1.0, wide ? sh - sh / 2 : 0);
       const int     row = m.row0 + rr; // row within the block
       const int     nkc = b.K_pad / KC;
       uint8_t*      out = dst + b.dst_off + (int64_t) (row / b.tile_rows) * nkc * S * b.tile_rows * KC +
                      ((row % b.tile_rows) >> 3) * 128 + (row & 7) * 16 + q * 4;
       const double* x   = rowbase + (int64_t) rr * K;
       const int     n16 = b.K_pad / 16;
-      for(int k16 = cw * CPW + sub; k16 < n16; k16 += 8 * CPW) {
+      for(int k16 = cw * CPW + sub; k16 < n16; k16 += kStagedWarps * CPW) {
         const int k0 = k16 * 16 + q * 4;
         double    v[4];
 #pragma unroll
@@ -478,7 +494,7 @@ __global__ void __launch_bounds__(288, 1) k_split_staged(const SplitBlock* __res
         uint32_t lo[4], hi[4];
 #pragma unroll
         for(int t = 0; t < 4; t++) {
-          const uint64_t Y = (uint64_t) __double2ll_rn(v[t] * f1 * f2) + bias;
+          const uint64_t Y = digit_word<S>(wide ? v[t] * f2 : v[t], f1, bias);
           lo[t]            = (uint32_t) Y;
           hi[t]            = (uint32_t) (Y >> 32);
         }
@@ -1301,7 +1317,7 @@ void launch_staged(const SplitSet& x, const double* src, uint8_t* slices, int32_
     configured[dev] = true;
   }
   const int grid = std::min(nchunks * (8 / R), sm_count());
-  k_split_staged<S, R><<<grid, 288, smem, st>>>(x.d_blocks, x.d_cbegin, nblocks, nchunks, nst, sb, src, slices, exps,
+  k_split_staged<S, R><<<grid, 32 * (kStagedWarps + 1), smem, st>>>(x.d_blocks, x.d_cbegin, nblocks, nchunks, nst, sb, src, slices, exps,
                                                 blockmax, err);
 }
 
