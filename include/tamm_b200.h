@@ -164,6 +164,7 @@ typedef struct tb_stats {
   int    tile_n;          /* split-INT8 output tile width (0: the default for the slice count) */
   double flops_run;       /* FP64 FLOPs of the tasks that ran: admitted minus the tasks skipped
                              over exactly-zero blocks of read-only operands */
+  double int8_ops_alg;    /* the INT8 ops of int8_ops without tile padding (profiled runs) */
 } tb_stats;
 
 /* C += alpha * sum over tasks of A * B, all groups, one stream-ordered pass.

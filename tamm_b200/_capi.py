@@ -38,7 +38,8 @@ h = C.c_void_p  # opaque handles
 class tb_stats(C.Structure):
     _fields_ = [("flops", C.c_double), ("int8_ops", C.c_double), ("slices_min", C.c_int),
                 ("slices_max", C.c_int), ("scratch_bytes", C.c_int64), ("split_ms", C.c_double),
-                ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int), ("flops_run", C.c_double)]
+                ("gemm_ms", C.c_double), ("mode", C.c_int), ("tile_n", C.c_int), ("flops_run", C.c_double),
+                ("int8_ops_alg", C.c_double)]
 
 
 # callbacks of lambda tensors (tb_block_fn, tb_batch_fn)

@@ -1565,17 +1565,26 @@ void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* 
     std::vector<uint8_t> ts(L->tasks.size());
     TB_CUDA(cudaMemcpyAsync(ts.data(), L->d_tslices, ts.size(), cudaMemcpyDeviceToHost, stream));
     TB_CUDA(cudaStreamSynchronize(stream));
-    double ops = 0;
+    double ops = 0, alg = 0;
     int    smin = S, smax = 1;
     for(const auto& it: L->items) {
       const DevGroup& g = wl.groups[it.group];
+      int64_t         M = 1, N = 1;
+      for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
+      for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
+      const double rows = (double) std::min<int64_t>(MT, M - (int64_t) it.mt * MT);
+      const double cols = (double) std::min<int64_t>(L->NT, N - (int64_t) it.nt * L->NT);
       for(int t = g.task_begin; t < g.task_end; t++) {
         const int st = ts[t];
         ops += 2.0 * MT * L->NT * (KC / L->esize) * L->tasks[t].nkc * (st * (st + 1) / 2);
+        double K = 1;
+        for(int j = 0; j < lc.nk; j++) K *= wl.tasks[t].adims[lc.k_a[j]];
+        alg += 2.0 * rows * cols * K * (st * (st + 1) / 2);
         smin = std::min(smin, st);
         smax = std::max(smax, st);
       }
     }
+    plan.last.int8_ops_alg = alg;
     plan.last.int8_ops   = ops;
     plan.last.slices_min = smin;
     plan.last.slices_max = smax;

@@ -1105,7 +1105,7 @@ void Sched::run_lambda_mult(Op& op) {
   }
   const int64_t budget = L.batch_bytes > 0 ? L.batch_bytes
                                            : std::max<int64_t>(64 << 20, (ctx->arena->capacity() - ctx->arena->used()) / 4);
-  double              flops = 0, flops_run = 0, split_ms = 0, gemm_ms = 0, int8_ops = 0;
+  double              flops = 0, flops_run = 0, split_ms = 0, gemm_ms = 0, int8_ops = 0, int8_alg = 0;
   int                 smin = 99, smax = 0;
   const cudaStream_t  st = ctx->stream;
   for(int64_t k0 = 0; k0 < sp0->ntiles();) {
@@ -1196,6 +1196,7 @@ void Sched::run_lambda_mult(Op& op) {
       split_ms += s.split_ms;
       gemm_ms += s.gemm_ms;
       int8_ops += s.int8_ops;
+      int8_alg += s.int8_ops_alg;
       smin = std::min(smin, s.slices_min);
       smax = std::max(smax, s.slices_max);
     }
@@ -1211,6 +1212,7 @@ void Sched::run_lambda_mult(Op& op) {
   op.plan->last.split_ms  = split_ms;
   op.plan->last.gemm_ms   = gemm_ms;
   op.plan->last.int8_ops  = int8_ops;
+  op.plan->last.int8_ops_alg = int8_alg;
   op.plan->last.slices_min = smax > 0 ? smin : 0;
   op.plan->last.slices_max = smax;
   op.plan->last.mode      = ctx->mode;
