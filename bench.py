@@ -22,8 +22,9 @@ fixed ("scaling": "strong"), timing is the max over ranks.  --shard runs the sam
 path on one GPU (a one-rank NCCL group).
 
 After the ladder, the full doubles-residual iteration (O=60, V=480, tiles U{20..64},
-seed 2; about 50 ops captured in one CUDA graph) is timed in FP64 and autotuned
-split-INT8 and reported under "ccsd_iteration" (--no-ccsd skips it).
+seed 2; one CUDA graph per mode) is timed in FP64, autotuned split-INT8 and BF16x3 and
+reported under "ccsd_iteration" with a sampled reference-CPU baseline (--no-ccsd skips
+it).
 """
 from __future__ import annotations
 
@@ -569,11 +570,12 @@ def main():
         del t2_pin, r2_pin
         from tamm_b200 import ccsd as CC
         P = CC.build(args.ccsd_oa, args.ccsd_va, seed=2, tile_lo=20, tile_hi=64, ec=ec)
-        res = CC.measure(P, max(1, args.ccsd_steps), ("fp64", "int8"))
+        res = CC.measure(P, max(1, args.ccsd_steps), ("fp64", "int8", "bf16x3"))
         for m in res.values():  # max over ranks of the replay time
             m["graph_ms"] = max_over_ranks(m["graph_ms"])
             m["tflops_graph"] = world * P.flops["contractions"] / m["graph_ms"] / 1e9
-        res["int8"]["speedup_vs_fp64"] = res["fp64"]["graph_ms"] / res["int8"]["graph_ms"]
+        for m in ("int8", "bf16x3"):
+            res[m]["speedup_vs_fp64"] = res["fp64"]["graph_ms"] / res[m]["graph_ms"]
         cpu3 = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             # the reference's block_multiply on a fixed-seed sample of the iteration's
