@@ -314,7 +314,7 @@ def run_blockops(args, torch, tb, W, local):
     (k_dot_partial, 16 and 8), denominator update t2 += r2 / D (k_denom, 24) and an
     in-place map r2 = 2 r2 (k_map_blocks, 16).  Each timed over `steps` launches after
     `warmup` with CUDA events on the context's stream; GB/s of algorithmic bytes."""
-    ec = tb.ExecutionContext(local, int(8 * 2 ** 30))
+    ec = tb.ExecutionContext(local, int(64 * 2 ** 30))  # (the ladder allocates v, 50 GB, unfilled here)
     lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec, build_v=False)
     a, b, c, d, i, j = lad.labels
     X = tb.Tensor([lad.V, lad.V, lad.O, lad.O], spin=(2, 2)).allocate(ec)

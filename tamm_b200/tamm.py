@@ -61,7 +61,6 @@ class ExecutionContext:
     def set_precision(self, mode=Precision.FP64, err_target=1e-11, nslices=0):
         call("tb_ctx_set_precision", self.h, int(mode), float(err_target), int(nslices))
 
-    @property
     def set_digit_cache(self, nbytes: int):
         """Keep up to nbytes of split-INT8 digits of read-only tensors across contractions."""
         call("tb_ctx_set_digit_cache", self.h, int(nbytes))
@@ -73,6 +72,7 @@ class ExecutionContext:
         call("tb_ctx_digit_cache_info", self.h, C.byref(u), C.byref(l))
         return u.value, l.value
 
+    @property
     def stream(self):
         s = A.vp()
         call("tb_ctx_stream", self.h, C.byref(s))

@@ -155,3 +155,11 @@ def test_invalid_ops_rejected_on_host():
         tb.tamm.mult_info(x(i, i), x(i, j), x(j, i))
     with pytest.raises(ValueError):
         x(i, j, k)
+
+
+def test_front_end_attribute_kinds():
+    """The context's stream is a property (bench and tests pass it to torch as an int);
+    the digit-cache controls are methods."""
+    import tamm_b200 as tb
+    assert isinstance(tb.ExecutionContext.stream, property)
+    assert callable(tb.ExecutionContext.set_digit_cache) and callable(tb.ExecutionContext.digit_cache_info)
