@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--adjoint", action="store_true", help="also time the energy gradient (O=30, V=240)")
     p.add_argument("--triples", action="store_true", help="also time sampled triples-energy steps (O=50, V=500)")
     p.add_argument("--triples-steps", type=int, default=4)
+    p.add_argument("--pool-gib", type=float, default=150.0,
+                   help="device arena of the ladder workloads (small cases: a few GiB)")
     p.add_argument("--workload", default="ladder", choices=["ladder", "blockops"],
                    help="blockops: the HBM-bound block kernels on the ladder's r2 (one JSON line, GB/s)")
     return p.parse_args()
@@ -304,18 +306,21 @@ def measure_triples(ec, torch, nsteps):
     for t in P.T.values():
         t.set_read_only(False)
         t.deallocate()
+    P.release()
     return out
 
 
 def run_blockops(args, torch, tb, W, local):
     """The HBM-bound block kernels at the ladder's sizes (r2, t2: O=40, V=360 spin-blocked,
     7.8e7 elements, 0.62 GB each, beyond L2): permuted add r2(a,b,i,j) += X(b,a,j,i)
-    (k_assign_tiled, 24 B/element), flat add r2 += X (k_axpby, 24), dot r2.t2 and norm
+    (k_assign_blocks, 24 B/element), flat add r2 += X (k_axpby, 24), dot r2.t2 and norm
     (k_dot_partial, 16 and 8), denominator update t2 += r2 / D (k_denom, 24) and an
     in-place map r2 = 2 r2 (k_map_blocks, 16).  Each timed over `steps` launches after
     `warmup` with CUDA events on the context's stream; GB/s of algorithmic bytes."""
-    ec = tb.ExecutionContext(local, int(64 * 2 ** 30))  # (the ladder allocates v, 50 GB, unfilled here)
-    lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec, build_v=False)
+    # r2, t2 and X only (v is not needed): 1.9 GB at O=40, V=360
+    lad = W.ladder(args.oa, args.va, seed=args.seed, ec=tb.ExecutionContext(local, int(4 * 2 ** 30)),
+                   build_v=False, alloc_v=False)
+    ec = lad.ec
     a, b, c, d, i, j = lad.labels
     X = tb.Tensor([lad.V, lad.V, lad.O, lad.O], spin=(2, 2)).allocate(ec)
     X.write(np.random.default_rng(3).normal(size=X.nelems))
@@ -327,7 +332,7 @@ def run_blockops(args, torch, tb, W, local):
     peaks = load_peaks()
     hbm = peaks.get("hbm_gbs")
     cases = {
-        "permuted_add k_assign_tiled": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(b, a, j, i)))),
+        "permuted_add k_assign_blocks": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(b, a, j, i)))),
         "flat_add k_axpby": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(a, b, i, j)))),
         "dot k_dot_partial": (16, lambda s: s.dot(0, lad.r2(a, b, i, j), lad.t2(a, b, i, j))),
         "norm k_dot_partial": (8, lambda s: s.norm(1, lad.r2(a, b, i, j))),
@@ -387,7 +392,7 @@ def main():
         return
     headline = args.mode or "int8"
     modes = {"fp64": tb.Precision.FP64, "int8": tb.Precision.INT8, "bf16x3": tb.Precision.BF16X3}
-    ec = tb.ExecutionContext(local, int(150 * 2 ** 30))
+    ec = tb.ExecutionContext(local, int(args.pool_gib * 2 ** 30))
     lad = W.ladder(args.oa, args.va, seed=args.seed, ec=ec)
     lad.v.set_read_only(True)  # constant integrals: tasks over exactly-zero blocks are skipped
     _, v_zero_blocks, v_zero_elems = lad.v.read_only_info()

@@ -307,12 +307,37 @@ void launch_assign(const AssignLoop& lp, double* dst, double scale, const double
   TB_CUDA(cudaGetLastError());
 }
 
-BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off) {
+// min(want, the CTAs of `kernel` (kThreads threads, static shared memory) resident on
+// the current device at once): one wave, each CTA taking an equal share.
+template <class K>
+int resident_grid(K kernel, int64_t want) {
+  static int per_sm[64] = {0};
+  int        dev        = 0;
+  TB_CUDA(cudaGetDevice(&dev));
+  int& k = per_sm[dev < 64 ? dev : 63];
+  if(k == 0) {
+    int r = 0;
+    TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kernel, kThreads, 0));
+    k = std::max(r, 1);
+  }
+  int nsm = 0;
+  TB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  return (int) std::max<int64_t>(1, std::min<int64_t>(want, (int64_t) nsm * k));
+}
+
+constexpr int kAsgEdge       = 64;                          // sub-tile edge along q and p
+constexpr int kAsgCap        = kAsgEdge * (kAsgEdge + 1);   // doubles of shared memory per CTA
+constexpr int kAsgMaxSub     = 32;                          // sub-tiles per work unit
+constexpr int kAsgStreamUnit = 8192;                        // elements per streamed work unit
+constexpr int kAsgElems      = 8;                           // elements in flight per thread
+
+BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off, int64_t first) {
   BlockAssign b{};
   b.dst_off = dst_off;
   b.src_off = src_off;
   b.nd      = lp.nd;
   b.total   = 1;
+  b.first   = first;
   for(int k = 0; k < lp.nd; k++) b.total *= lp.dims[k];
   int p = -1;
   for(int k = 0; k < lp.nd; k++)
@@ -327,61 +352,156 @@ BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src
     b.sld[k]  = k < lp.nd ? lp.sld[k] : 0;
     if(tiled && k < lp.nd && k != p && k != q) b.outer_total *= lp.dims[k];
   }
+  int64_t units = 0;
+  if(b.total == 0) b.per_unit = 1;
+  else if(tiled) {
+    // offsets within a transposed block pair are 32-bit
+    int64_t ssize = 1, dsize = 1;
+    for(int k = 0; k < lp.nd; k++) {
+      ssize += (lp.dims[k] - 1) * lp.sld[k];
+      dsize += (lp.dims[k] - 1) * lp.dld[k];
+    }
+    TB_EXPECTS(ssize < (int64_t(1) << 31) && dsize < (int64_t(1) << 31), "block too large");
+    const int64_t tq = std::min<int64_t>(b.dims[q], kAsgEdge), tp = std::min<int64_t>(b.dims[p], kAsgEdge);
+    const int64_t ntiles = b.outer_total * ((b.dims[q] + tq - 1) / tq) * ((b.dims[p] + tp - 1) / tp);
+    b.per_unit = (int) std::max<int64_t>(1, std::min<int64_t>(kAsgMaxSub, kAsgCap / (tq * (tp | 1))));
+    units      = (ntiles + b.per_unit - 1) / b.per_unit;
+  }
+  else {
+    b.per_unit = kAsgStreamUnit;
+    units      = (b.total + kAsgStreamUnit - 1) / kAsgStreamUnit;
+  }
+  TB_EXPECTS(units < (int64_t(1) << 31), "block pair too large");
+  b.units = (int) units;
   return b;
 }
 
-// The block pairs of an AddOp in one launch: CTA row blockIdx.y takes pairs y, y +
-// gridDim.y, ...; within a pair the gridDim.x CTAs share its 32x32 tiles (a transposing
-// pair, as k_assign_tiled) or its elements (a streamed pair, as k_assign).
+// The block pairs of an AddOp in one launch.  Work units (a batch of sub-tiles of one
+// pair's transposed (q, p) plane, or a run of a streamed pair's elements) are split
+// into equal contiguous ranges, one per CTA.  A transposing unit loads its sub-tiles
+// along the source's stride-1 mode p into shared memory (odd row pitch),
+// then writes them row by row along the destination's stride-1 mode q.  Threads walk
+// the unit's elements in flat order (kAsgElems loads in flight each), and sub-tiles
+// have the exact extents of the blocks (at most 64 x 64), so no lanes are spent on
+// padding for small tiles.
 __global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__ dst, double scale,
                                                             const double* __restrict__ src,
                                                             const BlockAssign* __restrict__ blocks, int nblocks,
-                                                            int is_assign) {
-  __shared__ double tile[32][33];
-  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
-    const BlockAssign a  = blocks[blk];
-    double* const     d0 = dst + a.dst_off;
-    const double*     s0 = src + a.src_off;
+                                                            int64_t nunits, int is_assign) {
+  __shared__ double  tile[kAsgCap];
+  __shared__ int     s_so[kAsgMaxSub], s_do[kAsgMaxSub]; // sub-tile origins within the blocks
+  __shared__ int     s_nq[kAsgMaxSub], s_np[kAsgMaxSub];
+  __shared__ int     s_pair;
+  const int64_t u0 = nunits * blockIdx.x / gridDim.x, u1 = nunits * (blockIdx.x + 1) / gridDim.x;
+  if(u0 >= u1) return;
+  if(threadIdx.x == 0) { // the pair holding unit u0: last pair with first <= u0
+    int lo = 0, hi = nblocks - 1;
+    while(lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if(blocks[mid].first <= u0) lo = mid;
+      else hi = mid - 1;
+    }
+    s_pair = lo;
+  }
+  __syncthreads();
+  int pi = s_pair;
+  for(int64_t u = u0; u < u1; u++) {
+    while(u >= blocks[pi].first + blocks[pi].units) pi++;
+    const BlockAssign& a  = blocks[pi];
+    double* const      d0 = dst + a.dst_off;
+    const double*      s0 = src + a.src_off;
+    const int64_t      lu = u - a.first;
     if(a.p >= 0) {
-      const int     q      = a.nd - 1;
-      const int64_t Dq     = a.dims[q], Dp = a.dims[a.p];
-      const int64_t tq     = (Dq + 31) / 32, tp = (Dp + 31) / 32;
-      const int64_t ntiles = a.outer_total * tq * tp;
-      for(int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        int64_t x  = t;
-        int64_t bq = x % tq;
-        x /= tq;
-        int64_t bp = x % tp;
-        x /= tp;
+      const int     q = a.nd - 1, p = a.p;
+      const int64_t Dq = a.dims[q], Dp = a.dims[p];
+      const int     TQ = (int) min(Dq, (int64_t) kAsgEdge), TP = (int) min(Dp, (int64_t) kAsgEdge);
+      const int     pitch = TP | 1;
+      const int64_t nbq = (Dq + TQ - 1) / TQ, nbp = (Dp + TP - 1) / TP;
+      const int64_t ntiles = a.outer_total * nbq * nbp;
+      const int64_t t0 = lu * a.per_unit;
+      const int     nt = (int) min((int64_t) a.per_unit, ntiles - t0);
+      const int     sq = (int) a.sld[q], dp = (int) a.dld[p];
+      if(threadIdx.x < nt) { // origin and extents of each sub-tile of the unit
+        int64_t       x  = t0 + threadIdx.x;
+        const int64_t bq = x % nbq;
+        x /= nbq;
+        const int64_t bp = x % nbp;
+        x /= nbp;
         int64_t so = 0, doff = 0;
         for(int k = a.nd - 1; k >= 0; k--) {
-          if(k == q || k == a.p) continue;
+          if(k == q || k == p) continue;
           const int64_t dk = a.dims[k];
           const int64_t i  = x % dk;
           x /= dk;
           so += i * a.sld[k];
           doff += i * a.dld[k];
         }
-        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-        for(int r = ty; r < 32; r += 8) {
-          const int64_t iq = bq * 32 + r, ip = bp * 32 + tx;
-          if(iq < Dq && ip < Dp) tile[r][tx] = __ldg(s0 + so + iq * a.sld[q] + ip * a.sld[a.p]);
-        }
-        __syncthreads();
-        for(int r = ty; r < 32; r += 8) {
-          const int64_t ip = bp * 32 + r, iq = bq * 32 + tx;
-          if(iq < Dq && ip < Dp) {
-            double*      dp = d0 + doff + iq * a.dld[q] + ip * a.dld[a.p];
-            const double v  = scale * tile[tx][r];
-            *dp             = is_assign ? v : *dp + v;
+        const int64_t q0 = bq * TQ, p0 = bp * TP;
+        s_so[threadIdx.x] = (int) (so + q0 * sq + p0);
+        s_do[threadIdx.x] = (int) (doff + q0 + p0 * dp);
+        s_nq[threadIdx.x] = (int) min((int64_t) TQ, Dq - q0);
+        s_np[threadIdx.x] = (int) min((int64_t) TP, Dp - p0);
+      }
+      __syncthreads();
+      // flat element order within the unit: (sub-tile, q row, p column) on the way in,
+      // (sub-tile, p row, q column) on the way out; x / d for x < 2^16 and 8 <= d <= 64
+      // as umulhi(x, ceil(2^32 / d)) (Granlund and Montgomery, division by invariant
+      // integers using multiplication)
+      const unsigned mq = 0xFFFFFFFFu / TQ + 1, mp = 0xFFFFFFFFu / TP + 1;
+      const int      n  = nt * TQ * TP;
+      for(int e0 = threadIdx.x; e0 < n; e0 += kThreads * kAsgElems) {
+        double v[kAsgElems];
+#pragma unroll
+        for(int j = 0; j < kAsgElems; j++) {
+          const int e = e0 + j * kThreads;
+          v[j]        = 0.0;
+          if(e < n) {
+            const int row = (int) __umulhi((unsigned) e, mp), ip = e - row * TP;
+            const int k = (int) __umulhi((unsigned) row, mq), iq = row - k * TQ;
+            if(iq < s_nq[k] && ip < s_np[k]) v[j] = __ldg(s0 + s_so[k] + iq * sq + ip);
           }
         }
-        __syncthreads();
+#pragma unroll
+        for(int j = 0; j < kAsgElems; j++) {
+          const int e = e0 + j * kThreads;
+          if(e < n) {
+            const int row = (int) __umulhi((unsigned) e, mp), ip = e - row * TP;
+            tile[row * pitch + ip] = v[j];
+          }
+        }
       }
+      __syncthreads();
+      for(int e0 = threadIdx.x; e0 < n; e0 += kThreads * kAsgElems) {
+        double old[kAsgElems];
+        int    out[kAsgElems], at[kAsgElems]; // offset in the destination block (-1: none), in tile
+#pragma unroll
+        for(int j = 0; j < kAsgElems; j++) {
+          const int e = e0 + j * kThreads;
+          old[j]      = 0.0;
+          out[j]      = -1;
+          at[j]       = 0;
+          if(e < n) {
+            const int row = (int) __umulhi((unsigned) e, mq), iq = e - row * TQ;
+            const int k = (int) __umulhi((unsigned) row, mp), ip = row - k * TP;
+            if(iq < s_nq[k] && ip < s_np[k]) {
+              out[j] = s_do[k] + ip * dp + iq;
+              at[j]  = (k * TQ + iq) * pitch + ip;
+              if(!is_assign) old[j] = d0[out[j]];
+            }
+          }
+        }
+#pragma unroll
+        for(int j = 0; j < kAsgElems; j++) // product rounded before the add, as in a plain loop
+          if(out[j] >= 0) {
+            const double v = __dmul_rn(scale, tile[at[j]]);
+            d0[out[j]]     = is_assign ? v : old[j] + v;
+          }
+      }
+      __syncthreads();
     }
     else {
-      const int64_t stride = (int64_t) gridDim.x * blockDim.x;
-      for(int64_t lin = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; lin < a.total; lin += stride) {
+      const int64_t beg = lu * a.per_unit, end = min(a.total, beg + a.per_unit);
+      for(int64_t lin = beg + threadIdx.x; lin < end; lin += kThreads) {
         int64_t x = lin, so = 0, doff = 0;
 #pragma unroll
         for(int k = 3; k >= 0; k--) {
@@ -393,7 +513,7 @@ __global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__
           doff += i * a.dld[k];
           x = qk;
         }
-        const double v = scale * __ldg(s0 + so);
+        const double v = __dmul_rn(scale, __ldg(s0 + so));
         d0[doff]       = is_assign ? v : d0[doff] + v;
       }
     }
@@ -401,10 +521,10 @@ __global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__
 }
 
 void launch_assign_blocks(double* dst, double scale, const double* src, const BlockAssign* blocks, int nblocks,
-                          int is_assign, cudaStream_t stream) {
-  if(nblocks <= 0) return;
-  const dim3 grid(8, (unsigned) std::min(nblocks, 8192));
-  k_assign_blocks<<<grid, kThreads, 0, stream>>>(dst, scale, src, blocks, nblocks, is_assign);
+                          int64_t nunits, int is_assign, cudaStream_t stream) {
+  if(nblocks <= 0 || nunits <= 0) return;
+  k_assign_blocks<<<resident_grid(k_assign_blocks, nunits), kThreads, 0, stream>>>(dst, scale, src, blocks, nblocks,
+                                                                                     nunits, is_assign);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -414,37 +534,124 @@ void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t
   TB_CUDA(cudaGetLastError());
 }
 
-// SetOp over a list of blocks in one launch: blocks (offset, element count) pairs in
-// device memory; CTA (x, y) fills blocks y, y + gridDim.y, ... with gridDim.x CTAs per
-// block, two elements per thread and step (16-byte stores where aligned).
-__global__ void __launch_bounds__(kThreads) k_fill_blocks(double* __restrict__ x, const int64_t* __restrict__ pairs,
-                                                          int nblocks, double v, int is_assign) {
-  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
-    double* const xb     = x + pairs[2 * blk];
-    const int64_t n      = pairs[2 * blk + 1];
-    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 2;
-    for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
-      if(i + 1 < n && ((reinterpret_cast<uintptr_t>(xb + i) & 15) == 0)) {
-        double2 d;
-        if(is_assign) d = make_double2(v, v);
-        else {
-          d = *reinterpret_cast<double2*>(xb + i);
-          d.x += v;
-          d.y += v;
+constexpr int kSegVec = 4; // 16-byte accesses in flight per thread
+
+// A CTA's share of a segment list: elements [N b / G, N (b + 1) / G) of the runs'
+// concatenation (N elements in all, G CTAs), walked run by run; body(dst offset, src
+// offset, lo, hi) gets the part [lo, hi) of each run it overlaps.
+template <class Body>
+__device__ __forceinline__ void walk_segments(const int64_t* __restrict__ seg, int nseg, Body body) {
+  __shared__ int s_first;
+  const int64_t  N  = seg[4 * (nseg - 1) + 3] + seg[4 * (nseg - 1) + 2];
+  const int64_t  e0 = N * blockIdx.x / gridDim.x, e1 = N * (blockIdx.x + 1) / gridDim.x;
+  if(e0 >= e1) return;
+  if(threadIdx.x == 0) { // last run with first <= e0
+    int lo = 0, hi = nseg - 1;
+    while(lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if(seg[4 * mid + 3] <= e0) lo = mid;
+      else hi = mid - 1;
+    }
+    s_first = lo;
+  }
+  __syncthreads();
+  for(int r = s_first; r < nseg && seg[4 * r + 3] < e1; r++) {
+    const int64_t f = seg[4 * r + 3], n = seg[4 * r + 2];
+    const int64_t lo = max(e0, f) - f, hi = min(e1, f + n) - f;
+    if(lo < hi) body(seg[4 * r], seg[4 * r + 1], lo, hi);
+  }
+}
+
+// y[lo, hi) = g(x[lo, hi), y[lo, hi)) elementwise (x may be null: zeros; x may equal
+// y; y read only when READY): one element before the first 16-byte boundary of y, then
+// double2 accesses with kSegVec in flight per thread when x shares y's alignment, else
+// scalar ones.
+template <bool READY, class G>
+__device__ __forceinline__ void seg_apply(double* y, const double* x, int64_t lo, int64_t hi, G g) {
+  int64_t a = lo;
+  if((reinterpret_cast<uintptr_t>(y + a) & 15) != 0) {
+    if(threadIdx.x == 0) y[a] = g(x ? x[a] : 0.0, READY ? y[a] : 0.0);
+    a++;
+  }
+  if(a >= hi) return;
+  if(x == nullptr || (reinterpret_cast<uintptr_t>(x + a) & 15) == 0) {
+    const int64_t  nv = (hi - a) >> 1;
+    double2* const y2 = reinterpret_cast<double2*>(y + a);
+    const double2* x2 = x ? reinterpret_cast<const double2*>(x + a) : nullptr;
+    for(int64_t i = threadIdx.x; i < nv; i += (int64_t) kThreads * kSegVec) {
+      double2 xv[kSegVec], yv[kSegVec];
+#pragma unroll
+      for(int j = 0; j < kSegVec; j++) {
+        const int64_t k = i + (int64_t) j * kThreads;
+        xv[j] = yv[j] = make_double2(0.0, 0.0);
+        if(k < nv) {
+          if(x2) xv[j] = x2[k];
+          if(READY) yv[j] = y2[k];
         }
-        *reinterpret_cast<double2*>(xb + i) = d;
       }
-      else
-        for(int64_t j = i; j < i + 2 && j < n; j++) xb[j] = is_assign ? v : xb[j] + v;
+#pragma unroll
+      for(int j = 0; j < kSegVec; j++) {
+        const int64_t k = i + (int64_t) j * kThreads;
+        if(k < nv) y2[k] = make_double2(g(xv[j].x, yv[j].x), g(xv[j].y, yv[j].y));
+      }
+    }
+    if(threadIdx.x == 0 && a + 2 * nv < hi) y[hi - 1] = g(x ? x[hi - 1] : 0.0, READY ? y[hi - 1] : 0.0);
+  }
+  else {
+    for(int64_t i = a + threadIdx.x; i < hi; i += (int64_t) kThreads * kSegVec) {
+      double xv[kSegVec], yv[kSegVec];
+#pragma unroll
+      for(int j = 0; j < kSegVec; j++) {
+        const int64_t k = i + (int64_t) j * kThreads;
+        xv[j] = yv[j] = 0.0;
+        if(k < hi) {
+          xv[j] = x[k];
+          if(READY) yv[j] = y[k];
+        }
+      }
+#pragma unroll
+      for(int j = 0; j < kSegVec; j++) {
+        const int64_t k = i + (int64_t) j * kThreads;
+        if(k < hi) y[k] = g(xv[j], yv[j]);
+      }
     }
   }
 }
 
-void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double value, int is_assign,
+std::vector<int64_t> seg_list(const std::vector<int64_t>& tri) {
+  std::vector<int64_t> out;
+  int64_t              first = 0;
+  for(size_t i = 0; i + 2 < tri.size(); i += 3) {
+    const int64_t d = tri[i], s = tri[i + 1], n = tri[i + 2];
+    if(n <= 0) continue;
+    const size_t m = out.size();
+    if(m > 0 && out[m - 4] + out[m - 2] == d &&
+       ((s < 0 && out[m - 3] < 0) || (s >= 0 && out[m - 3] >= 0 && out[m - 3] + out[m - 2] == s)))
+      out[m - 2] += n;
+    else {
+      out.push_back(d);
+      out.push_back(s);
+      out.push_back(n);
+      out.push_back(first);
+    }
+    first += n;
+  }
+  return out;
+}
+
+__global__ void __launch_bounds__(kThreads) k_fill_blocks(double* __restrict__ x, const int64_t* __restrict__ segs,
+                                                          int nseg, double v, int is_assign) {
+  walk_segments(segs, nseg, [&](int64_t off, int64_t, int64_t lo, int64_t hi) {
+    if(is_assign) seg_apply<false>(x + off, nullptr, lo, hi, [v](double, double) { return v; });
+    else seg_apply<true>(x + off, nullptr, lo, hi, [v](double, double y) { return y + v; });
+  });
+}
+
+void launch_fill_blocks(double* x, const int64_t* segs, int nseg, int64_t total, double value, int is_assign,
                         cudaStream_t stream) {
-  if(nblocks <= 0) return;
-  const dim3 grid(4, (unsigned) std::min(nblocks, 2048));
-  k_fill_blocks<<<grid, kThreads, 0, stream>>>(x, pairs, nblocks, value, is_assign);
+  if(nseg <= 0 || total <= 0) return;
+  k_fill_blocks<<<resident_grid(k_fill_blocks, (total + 4095) / 4096), kThreads, 0, stream>>>(x, segs, nseg, value,
+                                                                                              is_assign);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -463,35 +670,21 @@ __device__ __forceinline__ double map_fn(int fn, double x, double p) {
   }
 }
 
-// Element function over a list of blocks: a CTA row (blockIdx.y) per block, 16-byte
-// accesses where both sides are aligned.
+// Element function over a segment list, each CTA on an equal share of its elements.
 __global__ void __launch_bounds__(kThreads) k_map_blocks(double* __restrict__ dst, const double* __restrict__ src,
-                                                         const int64_t* __restrict__ tri, int nblocks, int fn,
+                                                         const int64_t* __restrict__ segs, int nseg, int fn,
                                                          double p) {
-  for(int blk = blockIdx.y; blk < nblocks; blk += gridDim.y) {
-    double* const       d      = dst + tri[3 * blk];
-    const int64_t       so     = tri[3 * blk + 1];
-    const double* const sp     = so >= 0 ? src + so : nullptr;
-    const int64_t       n      = tri[3 * blk + 2];
-    const int64_t       stride = (int64_t) gridDim.x * blockDim.x * 2;
-    for(int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
-      const bool vec = i + 1 < n && ((reinterpret_cast<uintptr_t>(d + i) & 15) == 0) &&
-                       (sp == nullptr || (reinterpret_cast<uintptr_t>(sp + i) & 15) == 0);
-      if(vec) {
-        const double2 x = sp ? *reinterpret_cast<const double2*>(sp + i) : make_double2(0.0, 0.0);
-        *reinterpret_cast<double2*>(d + i) = make_double2(map_fn(fn, x.x, p), map_fn(fn, x.y, p));
-      }
-      else
-        for(int64_t j = i; j < i + 2 && j < n; j++) d[j] = map_fn(fn, sp ? sp[j] : 0.0, p);
-    }
-  }
+  walk_segments(segs, nseg, [&](int64_t doff, int64_t soff, int64_t lo, int64_t hi) {
+    seg_apply<false>(dst + doff, soff >= 0 ? src + soff : nullptr, lo, hi,
+              [fn, p](double x, double) { return map_fn(fn, x, p); });
+  });
 }
 
-void launch_map_blocks(double* dst, const double* src, const int64_t* triples, int nblocks, int fn, double p,
-                       cudaStream_t stream) {
-  if(nblocks <= 0) return;
-  const dim3 grid(8, (unsigned) std::min(nblocks, 4096));
-  k_map_blocks<<<grid, kThreads, 0, stream>>>(dst, src, triples, nblocks, fn, p);
+void launch_map_blocks(double* dst, const double* src, const int64_t* segs, int nseg, int64_t total, int fn,
+                       double p, cudaStream_t stream) {
+  if(nseg <= 0 || total <= 0) return;
+  k_map_blocks<<<resident_grid(k_map_blocks, (total + 4095) / 4096), kThreads, 0, stream>>>(dst, src, segs, nseg, fn,
+                                                                                             p);
   TB_CUDA(cudaGetLastError());
 }
 

@@ -163,28 +163,40 @@ AssignLoop plan_assign(const int64_t* ddims, const int* dlabels, int nd, const i
 void launch_assign(const AssignLoop& lp, double* dst, double scale, const double* src,
                    int is_assign, cudaStream_t stream);
 // One block pair of a permuted AddOp: offsets and the loop of plan_assign, with the
-// position of the source's stride-1 loop mode when the pair goes through the 32x32
-// shared-memory transpose (-1: streamed).
+// position of the source's stride-1 loop mode when the pair goes through the
+// shared-memory transpose (-1: streamed).  The pair's work is cut into `units` work
+// units (`per_unit` sub-tiles of at most 64x64 of the transposed plane, or `per_unit`
+// elements when streamed), numbered from `first` across the launch.
 struct BlockAssign {
   int64_t dst_off, src_off;
   int32_t nd, p;
   int64_t dims[4], dld[4], sld[4];
   int64_t outer_total, total;
+  int64_t first;
+  int32_t units, per_unit;
 };
-BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off);
-// All block pairs of an AddOp in one launch (device array of nblocks BlockAssign).
+// `first` is the number of work units of the pairs before this one in the launch.
+BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off, int64_t first);
+// All block pairs of an AddOp in one launch (device array of nblocks BlockAssign
+// holding nunits work units in all).
 void launch_assign_blocks(double* dst, double scale, const double* src, const BlockAssign* blocks, int nblocks,
-                          int is_assign, cudaStream_t stream);
+                          int64_t nunits, int is_assign, cudaStream_t stream);
 void launch_fill(double* x, int64_t n, double value, int is_assign, cudaStream_t stream);
-// x[off .. off + n) (=|+=) value for each (off, n) pair of a device array
-void launch_fill_blocks(double* x, const int64_t* pairs, int nblocks, double value, int is_assign,
+// Segment lists of the block-wise fill and map: per run of blocks (dst offset, src
+// offset or -1, n, first), `first` the sum of n over the runs before it.
+// seg_list merges blocks that are adjacent on both sides into one run.
+std::vector<int64_t> seg_list(const std::vector<int64_t>& triples);
+// x[off .. off + n) (=|+=) value for each run of a device segment list holding
+// `total` elements
+void launch_fill_blocks(double* x, const int64_t* segs, int nseg, int64_t total, double value, int is_assign,
                         cudaStream_t stream);
 void launch_axpby(double alpha, const double* x, double beta, double* y, int64_t n,
                   cudaStream_t stream);
-// For each (dst offset, src offset or -1, n) triple of a device array:
-// dst[0:n) = f(src[0:n)) with f = TB_MAP_* and parameter p (src -1: zeros).
-void launch_map_blocks(double* dst, const double* src, const int64_t* triples, int nblocks, int fn, double p,
-                       cudaStream_t stream);
+// For each run (dst offset, src offset or -1, n, first) of a device segment list
+// holding `total` elements: dst[0:n) = f(src[0:n)) with f = TB_MAP_* and parameter p
+// (src -1: zeros).
+void launch_map_blocks(double* dst, const double* src, const int64_t* segs, int nseg, int64_t total, int fn,
+                       double p, cudaStream_t stream);
 double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stream);
 // *out = scale * x.y (root: scale * sqrt(x.x)), staying on the device; part holds
 // 1024 doubles of scratch.  y == nullptr means x.x.

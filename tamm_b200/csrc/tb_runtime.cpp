@@ -642,9 +642,10 @@ void Sched::run(Op& op) {
             tri.push_back(n);
           } while(!it.empty() && next_tuple(it, nt));
         TB_EXPECTS(tri.size() / 3 < (1u << 31), "too many blocks in one map");
-        int64_t*  d   = nullptr;
-        const int dev = ctx->device;
-        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * std::max<size_t>(tri.size(), 1)));
+        const std::vector<int64_t> segs = seg_list(tri);
+        int64_t*                   d    = nullptr;
+        const int                  dev  = ctx->device;
+        TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * std::max<size_t>(segs.size(), 1)));
         cached = std::shared_ptr<int64_t>(d, [dev](int64_t* q) {
           int cur = -1;
           cudaGetDevice(&cur);
@@ -652,14 +653,16 @@ void Sched::run(Op& op) {
           cudaFree(q);
           if(cur >= 0) cudaSetDevice(cur);
         });
-        if(!tri.empty())
-          TB_CUDA(cudaMemcpy(d, tri.data(), sizeof(int64_t) * tri.size(), cudaMemcpyHostToDevice));
-        count = (int) (tri.size() / 3);
+        if(!segs.empty())
+          TB_CUDA(cudaMemcpy(d, segs.data(), sizeof(int64_t) * segs.size(), cudaMemcpyHostToDevice));
+        count           = (int) (segs.size() / 4);
+        seg_total[key]  = segs.empty() ? 0 : segs[segs.size() - 1] + segs[segs.size() - 2];
       }
-      op.map_dev = cached;
-      op.map_n   = count;
+      op.map_dev   = cached;
+      op.map_n     = count;
+      op.map_total = seg_total[key];
     }
-    launch_map_blocks(op.lhs.t->data, op.a.t->data, op.map_dev.get(), op.map_n, op.fn, op.value, st);
+    launch_map_blocks(op.lhs.t->data, op.a.t->data, op.map_dev.get(), op.map_n, op.map_total, op.fn, op.value, st);
     return;
   }
   if(op.kind == Op::Set) {
@@ -693,9 +696,16 @@ void Sched::run(Op& op) {
         if(op.fill_key.empty()) op.fill_key = "S|" + signature(op);
         auto& cached = fill_cache[op.fill_key];
         if(!cached) {
-          int64_t*  d   = nullptr;
-          const int dev = ctx->device;
-          TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * op.set_blocks->size()));
+          std::vector<int64_t> tri;
+          for(size_t i = 0; i < nb; i++) {
+            tri.push_back((*op.set_blocks)[2 * i]);
+            tri.push_back(-1);
+            tri.push_back((*op.set_blocks)[2 * i + 1]);
+          }
+          const std::vector<int64_t> segs = seg_list(tri);
+          int64_t*                   d    = nullptr;
+          const int                  dev  = ctx->device;
+          TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d), sizeof(int64_t) * std::max<size_t>(segs.size(), 1)));
           cached = std::shared_ptr<int64_t>(d, [dev](int64_t* p) {
             int cur = -1;
             cudaGetDevice(&cur);
@@ -703,12 +713,16 @@ void Sched::run(Op& op) {
             cudaFree(p);
             if(cur >= 0) cudaSetDevice(cur);
           });
-          TB_CUDA(cudaMemcpy(d, op.set_blocks->data(), sizeof(int64_t) * op.set_blocks->size(),
-                             cudaMemcpyHostToDevice));
+          if(!segs.empty())
+            TB_CUDA(cudaMemcpy(d, segs.data(), sizeof(int64_t) * segs.size(), cudaMemcpyHostToDevice));
+          map_count[op.fill_key] = (int) (segs.size() / 4);
+          seg_total[op.fill_key] = segs.empty() ? 0 : segs[segs.size() - 1] + segs[segs.size() - 2];
         }
-        op.set_dev = cached;
+        op.set_dev   = cached;
+        op.set_nseg  = map_count[op.fill_key];
+        op.set_total = seg_total[op.fill_key];
       }
-      launch_fill_blocks(op.lhs.t->data, op.set_dev.get(), (int) nb, op.value, op.is_assign, st);
+      launch_fill_blocks(op.lhs.t->data, op.set_dev.get(), op.set_nseg, op.set_total, op.value, op.is_assign, st);
     }
     return;
   }
@@ -769,11 +783,14 @@ void Sched::run(Op& op) {
       auto&             count  = map_count[key];
       if(!cached) {
         std::vector<BlockAssign> list;
+        int64_t                  units = 0;
         for(const auto& ab: *op.add_blocks) {
           AssignLoop lp = plan_assign(ab.ddims, op.lhs.labels.data(), op.lhs.t->nmodes, ab.sdims,
                                       op.a.labels.data(), op.a.t->nmodes);
-          list.push_back(make_block_assign(lp, ab.dst_off, ab.src_off));
+          list.push_back(make_block_assign(lp, ab.dst_off, ab.src_off, units));
+          units += list.back().units;
         }
+        add_units[key] = units;
         TB_EXPECTS(list.size() < (1u << 31), "too many block pairs in one add");
         BlockAssign* d   = nullptr;
         const int    dev = ctx->device;
@@ -789,11 +806,12 @@ void Sched::run(Op& op) {
           TB_CUDA(cudaMemcpy(d, list.data(), sizeof(BlockAssign) * list.size(), cudaMemcpyHostToDevice));
         count = (int) list.size();
       }
-      op.add_dev = cached;
-      op.add_n   = count;
+      op.add_dev   = cached;
+      op.add_n     = count;
+      op.add_units = add_units[key];
     }
     launch_assign_blocks(op.lhs.t->data, op.alpha, op.a.t->data, reinterpret_cast<const BlockAssign*>(op.add_dev.get()),
-                         op.add_n, op.is_assign, st);
+                         op.add_n, op.add_units, op.is_assign, st);
     return;
   }
   if(op.kind == Op::Dot) {

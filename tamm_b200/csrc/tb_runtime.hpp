@@ -190,12 +190,16 @@ struct Op {
   std::shared_ptr<std::vector<AddBlock>> add_blocks;
   std::shared_ptr<int64_t>               add_dev;   // device BlockAssign list (scheduler's cache)
   int                                    add_n = 0;
+  int64_t                                add_units = 0; // work units of the list
   int                                    fn = 0;     // Map: element function
-  std::shared_ptr<int64_t>               map_dev;    // Map: device (dst, src, n) triples
-  int                                    map_n = 0;  // number of triples
+  std::shared_ptr<int64_t>               map_dev;    // Map: device segment list (seg_list)
+  int                                    map_n = 0;  // runs in the list
+  int64_t                                map_total = 0; // elements in the list
   bool                                   flat = false;
   std::shared_ptr<std::vector<int64_t>>  set_blocks; // (offset, size) pairs; empty = whole store
-  std::shared_ptr<int64_t>               set_dev;    // device copy of set_blocks (from the scheduler's cache)
+  std::shared_ptr<int64_t>               set_dev;    // set_blocks as a device segment list (scheduler's cache)
+  int                                    set_nseg = 0;
+  int64_t                                set_total = 0;
   std::string                            fill_key;   // its key in that cache
   // an assignment C = alpha * A * B queued as Set(0) + Mult runs fused on one rank in
   // FP64: the Mult stores its result (store), the Set zeroes only the output blocks the
@@ -245,6 +249,8 @@ struct Sched {
   // (or, for the fill of a fused assignment, its contraction's), uploaded once
   std::map<std::string, std::shared_ptr<int64_t>>  fill_cache;
   std::map<std::string, int>                        map_count; // triples of each cached map list
+  std::map<std::string, int64_t>                    add_units; // work units of each cached add list
+  std::map<std::string, int64_t>                    seg_total; // elements of each cached segment list
   // intermediates of multi-factor products (tb_sched_mult_n), by signature; freed with
   // the scheduler
   std::map<std::string, std::unique_ptr<Tensor>>    temps;

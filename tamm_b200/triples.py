@@ -34,7 +34,7 @@ import numpy as np
 
 from . import workloads as W
 from .tamm import (ExecutionContext, ExecutionHW, IndexSpace, Precision, Scheduler, Tensor, TiledIndexSpace,
-                   mult_info)
+                   _device_array, mult_info)
 
 SLOT_E = 2
 
@@ -49,8 +49,14 @@ class TriplesProblem:
     Vd: TiledIndexSpace    # virtual, tiling of the summed d
     eps: np.ndarray
     T: dict
-    buffer: object
+    buffer: int            # device address of the W storage, from the context's arena
     most: int
+
+    def release(self):
+        """Returns the W storage to the context's arena."""
+        if self.buffer:
+            self.ec.free(self.buffer)
+            self.buffer = 0
 
 
 def _dense_t2(oa, va, eps, seed):
@@ -69,7 +75,6 @@ def _dense_t2(oa, va, eps, seed):
 
 def build(oa: int, va: int, tile: int = 40, jtile: int = 2, dtile: int = 0, seed: int = 4, nchol=None,
           ec: ExecutionContext | None = None):
-    import torch
     is_ = W.mo_index_space(oa, va)
     MOb = TiledIndexSpace(is_, tile)
     MO1 = TiledIndexSpace(is_, 1)
@@ -125,8 +130,7 @@ def build(oa: int, va: int, tile: int = 40, jtile: int = 2, dtile: int = 0, seed
     for i in (0, oa):
         for jt in range(Oj.num_tiles):
             most = max(most, _w_tensor(V, O1, Oj, Ob, i, jt).nelems)
-    buf = torch.empty(most * 8 + 256, dtype=torch.uint8, device=f"cuda:{ec.device}")
-    return TriplesProblem(ec, V, Ob, O1, Oj, Vd, eps, T, buf, most)
+    return TriplesProblem(ec, V, Ob, O1, Oj, Vd, eps, T, ec.alloc(most * 8), most)
 
 
 def _w_tensor(V, O1, Oj, Ob, i, jt):
@@ -142,7 +146,7 @@ def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int):
     """Queues W(a,b,c,k) for occupied index i and j block jt, and slot SLOT_E +=
     sum W^2 / D.  Returns (W tensor, FP64 FLOPs of the two contractions)."""
     Wt = _w_tensor(P.V, P.O1, P.Oj, P.Ob, i, jt)
-    Wt.attach(P.ec, (P.buffer.data_ptr() + 255) // 256 * 256, P.most * 8)
+    Wt.attach(P.ec, P.buffer, P.most * 8)
     a, b, c = P.V.labels(3)
     (d,) = P.Vd.labels(1)
     k, l = P.Ob.labels(2)
@@ -204,7 +208,6 @@ def main(argv=None):
     out = {"workload": f"triples_energy_O{2 * args.oa}_V{2 * args.va}_tile{args.tile}_jtile{args.jtile}_dtile{args.dtile}",
            "sampled_steps": sample, "steps_total": len(allsteps)}
     res, wref = {}, None
-    base = (P.buffer.data_ptr() + 255) // 256 * 256 - P.buffer.data_ptr()
     for name, mode in (("fp64", Precision.FP64), ("int8", Precision.INT8)):
         ec.set_precision(mode, 1e-11)
         sch = Scheduler(ec)
@@ -215,7 +218,7 @@ def main(argv=None):
         # W of the first sampled step, kept on the device for the comparison
         Wt, _ = queue_pair(P, sch, *sample[0])
         sch.execute(ExecutionHW.GPU)
-        wv = P.buffer[base:base + 8 * Wt.nelems].view(torch.float64)
+        wv = _device_array(P.buffer, Wt.nelems, ec.device)
         if wref is None:
             wref = wv.clone()
         else:  # chunked, to keep temporaries small

@@ -98,11 +98,11 @@ def orbital_energies(oa: int, va: int, seed: int):
 
 def ladder(oa: int, va: int, seed: int = 1, tile_lo: int = 24, tile_hi: int = 48, nchol=None,
            ec: ExecutionContext | None = None, pool_bytes: int = 0, build_v: bool = True,
-           chol_tile: int = 1000) -> Ladder:
+           chol_tile: int = 1000, alloc_v: bool = True) -> Ladder:
     """Config of the CCSD particle-particle ladder: O = 2*oa, V = 2*va, virtual tiles
     U{tile_lo..tile_hi}, v from Cholesky vectors L(Q,a,c), Q = 5*(O+V),
     L ~ N(0,1)/sqrt(Q) * exp(-|a-c|/50) for same-spin (a,c), t2 ~ N(0, 0.1^2) /
-    (e_a + e_b - e_i - e_j)."""
+    (e_a + e_b - e_i - e_j).  alloc_v=False (with build_v=False) leaves v unallocated."""
     rng = np.random.default_rng(seed)
     occ_t = random_tiles(oa, tile_lo, tile_hi, rng)
     virt_t = random_tiles(va, tile_lo, tile_hi, rng)
@@ -115,7 +115,11 @@ def ladder(oa: int, va: int, seed: int = 1, tile_lo: int = 24, tile_hi: int = 48
     v = Tensor([V, V, V, V], spin=(2, 2))
     t2 = Tensor([V, V, O, O], spin=(2, 2))
     r2 = Tensor([V, V, O, O], spin=(2, 2))
-    sch.allocate(v, t2, r2)
+    if build_v and not alloc_v:
+        raise ValueError("building v needs it allocated")
+    if alloc_v:
+        sch.allocate(v)
+    sch.allocate(t2, r2)
     nocc = 2 * oa
     e_occ, e_virt = orbital_energies(oa, va, seed)
     eps = np.concatenate([e_occ, e_occ, e_virt, e_virt])

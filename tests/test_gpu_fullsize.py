@@ -174,6 +174,7 @@ def test_config5_w_step_tile40(big_ec):
         # W's spin rule stores only admitted t3 blocks; the formula is zero elsewhere
         errs[name] = float(np.max(np.abs(got - want))) / float(np.max(np.abs(want)))
         assert errs[name] <= tol, f"{name}: {errs[name]:.3e}"
+    P.release()
     assert no == 20
     print(f"config5 tile 40 O=20 V=160 step {step}: max rel err of W FP64 {errs['fp64']:.2e} "
           f"split-INT8 {errs['int8']:.2e}")

@@ -65,5 +65,6 @@ def test_streamed_triples_energy(ec, mode, tol, dtile):
         e, flops, _ = triples.energy(P, triples.steps(P), tb.Scheduler(ec))
     finally:
         ec.set_precision(tb.Precision.FP64)
+        P.release()
     assert flops > 0 and want < 0
     assert abs(e - want) <= tol * abs(want)
