@@ -107,7 +107,6 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return e;
 }
 
-constexpr int kStagedWarps = 16; // consumer warps of k_split_staged (plus one producer warp)
 
 // round(x * 2^sh) + bias as a 64-bit word whose bytes are the balanced digits + 128.
 // For S <= 6 (|X| < 2^47) one FMA against 1.5 * 2^52 leaves the integer, rounded to
@@ -324,205 +323,244 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
 
 // Staged split for operand blocks whose rows lie one after another in memory (K
 // contiguous and row r at element offset r * K: e.g. v(a,b,c,d) split as rows (a,b) by
-// K = (c,d)).  Each unit of R rows (8, or 4 when K is long) is one contiguous range of
-// R * K doubles, brought into shared memory by one bulk copy; a producer warp keeps
-// NST units in flight in a ring of shared-memory stages, so every element is read from
-// HBM exactly once and both the row maximum and the digit conversion read shared
-// memory.  Consumers (8 warps): row max -> exponent, then thread (row, quad) turns 4
-// consecutive k into S digit words stored as in k_split_fused (core matrices of 8 rows
-// x 16 bytes; a 4-row unit fills half of each).  The copy covers the 16-byte aligned
-// interior [floor16(start), floor16(end)) of the unit's bytes; a last element past
-// floor16(end) is loaded with a plain load.  Waits are bounded: a timeout records
-// `code` in *err and the consumers agree (bar.red) to leave together.
-struct StageMeta {
-  int32_t blk, row0, nlive, delta, tail, pad;
+// K = (c,d)).  The unit of work is a pair of rows, one contiguous range of 2K doubles,
+// brought into shared memory by one bulk copy; every element is read from HBM once, and
+// both the row maxima and the digit conversion read shared memory.
+//   Producer (warp 0): resolves 32 units at a time, one per lane (block by binary
+// search over the per-block chunk prefix, then the unit's copy range and the fields the
+// consumers need), and issues their copies in order into the stage of the group that
+// takes each unit; the unit records travel in shared memory beside the stages, so a
+// consumer reads no block record from global memory.
+//   Consumers: independent groups of kSplitGroup warps, each group with two stages of
+// its own, so a group's only synchronisation is a named barrier of its own warps.
+// Warp h of a group takes the h-th K range of the row maxima and every kSplitGroup-th
+// group of four 16-k chunks of the digits.  Lane (row, chunk c, quad q) reads its four
+// values in an order rotated by (q + c) mod 4, so that the 16 lanes of a row hit 16
+// distinct bank pairs, and the final byte permute puts the digits back in k order;
+// each warp store covers the two rows of 32-byte sectors.
+//   The copy covers the 16-byte aligned interior [floor16(start), floor16(end)) of the
+// pair; a last element past floor16(end) is loaded with a plain load.  Units made of
+// padding rows only write their exponents.  Waits are bounded: a timeout records
+// `code` in *err and the warps of a group agree (bar.red) to leave together.
+struct UnitMeta {
+  int64_t tail_src; // element index of the unit's last element (the tail load)
+  int64_t dst_off;  // byte offset of the block's digits
+  int32_t exp_base; // exponent index of the unit's first row
+  int32_t id, K, K_pad, tile_rows, row0, nlive, delta, tail;
+  int32_t pad[3];
 };
+static_assert(sizeof(UnitMeta) == 64, "unit record size");
 
-constexpr int64_t kStagedSmem = 227 * 1024; // dynamic shared memory of one staged-split CTA, at most
-constexpr int64_t kStagedHead = 1024;       // barriers, stage records, row maxima, before the ring
-// bytes of one stage of R rows of K doubles (+16 for the aligned start), 128-byte multiple
-__host__ __device__ constexpr int64_t staged_stage_bytes(int R, int64_t K) {
-  return (R * K * 8 + 16 + 127) / 128 * 128;
+constexpr int     kSplitGroup     = 2;            // consumer warps per group
+constexpr int     kSplitMaxGroups = 8;            // groups per CTA, at most
+constexpr int64_t kStagedSmem     = 227 * 1024;   // dynamic shared memory of one CTA, at most
+constexpr int64_t kStagedHead     = 2048;         // barriers, unit records, partial maxima
+// bytes of one stage of 2 rows of K doubles (+16 for the aligned start), 128-byte multiple
+__host__ __device__ constexpr int64_t staged_stage_bytes(int64_t K) {
+  return (2 * K * 8 + 16 + 127) / 128 * 128;
 }
 
-template<int S, int R>
-__global__ void __launch_bounds__(32 * (kStagedWarps + 1), 1) k_split_staged(const SplitBlock* __restrict__ blocks,
-                                                        const int32_t* __restrict__ chunk_begin, int nblocks,
-                                                        int nchunks, int nst, uint32_t stage_bytes,
-                                                        const double* __restrict__ src, uint8_t* __restrict__ dst,
-                                                        int32_t* __restrict__ exps, int32_t* __restrict__ blockmax,
-                                                        int* err) {
+// TR: rows per operand tile (128 for A; 0 = read from the unit record).
+template<int S, int TR>
+__global__ void __launch_bounds__(32 * (1 + kSplitMaxGroups * kSplitGroup), 1)
+  k_split_staged(const SplitBlock* __restrict__ blocks, const int32_t* __restrict__ chunk_begin, int nblocks,
+                 int nchunks, int ngroups, uint32_t stage_bytes, const double* __restrict__ src,
+                 uint8_t* __restrict__ dst, int32_t* __restrict__ exps, int32_t* __restrict__ blockmax, int* err) {
+  constexpr int G = kSplitGroup;
   extern __shared__ __align__(128) uint8_t sm[];
-  constexpr int UPC = 8 / R; // units per 8-row chunk
-  uint64_t*     full  = reinterpret_cast<uint64_t*>(sm);
-  uint64_t*     empty = full + 8;
-  StageMeta*    meta  = reinterpret_cast<StageMeta*>(empty + 8);
-  float*        pmax  = reinterpret_cast<float*>(meta + 8); // unused padding keeps 128-byte alignment below
-  double*       part  = reinterpret_cast<double*>(sm + 384);   // [2][kStagedWarps] partial row maxima
-  int32_t*      shift = reinterpret_cast<int32_t*>(part + 2 * kStagedWarps); // [2][8] digit shifts
-  uint8_t*      ring  = sm + 1024;
-  (void) pmax;
+  uint64_t*     full  = reinterpret_cast<uint64_t*>(sm);           // [2 per group]
+  uint64_t*     empty = full + 2 * kSplitMaxGroups;                // [2 per group]
+  UnitMeta*     meta  = reinterpret_cast<UnitMeta*>(sm + 256);     // [2 per group]
+  double*       part  = reinterpret_cast<double*>(sm + 1280);      // [group][parity][warp][row]
+  uint8_t*      ring  = sm + kStagedHead;
+  static_assert(4 * kSplitMaxGroups * 8 <= 256 && 256 + 2 * kSplitMaxGroups * 64 <= 1280, "stage records");
+  static_assert(1280 + 2 * kSplitMaxGroups * G * 2 * 8 <= kStagedHead, "partial maxima");
   const int     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int     nunits = nchunks * UPC;
-  const uint64_t bias = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
+  const int     nunits = nchunks * 4; // two rows per unit, four units per 8-row chunk
   if(threadIdx.x == 0) {
-    for(int x = 0; x < nst; x++) {
+    for(int x = 0; x < 2 * ngroups; x++) {
       mbar_init(&full[x], 1);
-      mbar_init(&empty[x], kStagedWarps); // one arrival per consumer warp
+      mbar_init(&empty[x], G); // one arrival per warp of the group
     }
     fence_mbarrier_init();
   }
   __syncthreads();
   if(warp == 0) {
-    // ---------------- producer: block lookup and one bulk copy per unit ----------------
-    // Block of chunk c: chunk_begin[lo] <= c < chunk_begin[lo + 1]; units come in
-    // increasing order, so the cursor only moves forward (32 blocks per ballot).
-    int      lo = 0, slot = 0;
-    uint32_t ph = 0;
-    for(int u = blockIdx.x; u < nunits; u += gridDim.x) {
-      const int c = u / UPC;
-      while(true) {
-        const int      idx = lo + 1 + lane;
-        const unsigned le  = __ballot_sync(0xffffffffu, idx < nblocks && __ldg(chunk_begin + idx) <= c);
-        lo += __popc(le);
-        if(le != 0xffffffffu) break;
-      }
-      if(!mbar_wait(&empty[slot], ph ^ 1, err, 21)) break; // (every lane polls; all agree on success)
-      if(lane == 0) {
+    // ---------------- producer: 32 unit records at a time, copies in unit order -------
+    // The CTA's j-th unit (u = blockIdx.x + j * gridDim.x) goes to group j mod ngroups,
+    // that group's stage (j / ngroups) mod 2.
+    for(int ub = blockIdx.x, jb = 0; ub < nunits; ub += 32 * gridDim.x, jb += 32) {
+      const int u = ub + lane * gridDim.x;
+      UnitMeta  mine{};
+      uintptr_t a16   = 0;
+      uint32_t  bytes = 0;
+      if(u < nunits) {
+        const int c = u >> 2;
+        int       lo = 0, hi = nblocks - 1; // last block whose first chunk is <= c
+        while(lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if(__ldg(chunk_begin + mid) <= c) lo = mid;
+          else hi = mid - 1;
+        }
         const SplitBlock& b    = blocks[lo];
-        const int         row0 = 8 * (c - __ldg(chunk_begin + lo)) + (u % UPC) * R;
-        const int         nl   = max(0, min(R, b.rows - row0));
-        StageMeta         m{lo, row0, nl, 0, 0, 0};
-        uint32_t          bytes = 0;
-        uintptr_t         a16   = 0;
+        const int         row0 = 8 * (c - __ldg(chunk_begin + lo)) + (u & 3) * 2;
+        const int         K    = b.K;
+        const int         nl   = max(0, min(2, b.rows - row0));
+        mine.dst_off   = b.dst_off;
+        mine.exp_base  = b.exp_off + row0;
+        mine.id        = b.id;
+        mine.K         = K;
+        mine.K_pad     = b.K_pad;
+        mine.tile_rows = b.tile_rows;
+        mine.row0      = row0;
+        mine.nlive     = nl;
+        mine.tail_src  = b.src_off + (int64_t) (row0 + nl) * K - 1;
         if(nl > 0) {
-          const uintptr_t start = reinterpret_cast<uintptr_t>(src + b.src_off + (int64_t) row0 * b.K);
-          const uintptr_t end   = start + (uintptr_t) nl * b.K * 8;
+          const uintptr_t start = reinterpret_cast<uintptr_t>(src + b.src_off + (int64_t) row0 * K);
+          const uintptr_t end   = start + (uintptr_t) nl * K * 8;
           a16                   = start & ~uintptr_t(15);
           bytes                 = (uint32_t) ((end & ~uintptr_t(15)) - a16);
-          m.delta               = (int32_t) (start - a16);
-          m.tail                = (end & 15) ? 1 : 0;
+          mine.delta            = (int32_t) (start - a16);
+          mine.tail             = (end & 15) ? 1 : 0;
         }
-        meta[slot] = m;
-        mbar_arrive_expect_tx(&full[slot], bytes);
-        if(bytes > 0) bulk_g2s(ring + (size_t) slot * stage_bytes, reinterpret_cast<const void*>(a16), bytes,
-                               &full[slot]);
       }
-      __syncwarp();
-      if(++slot == nst) {
-        slot = 0;
-        ph ^= 1;
+      for(int t = 0; t < 32; t++) {
+        if(ub + t * gridDim.x >= nunits) break;
+        const int      j     = jb + t;
+        const int      x     = 2 * (j % ngroups) + ((j / ngroups) & 1);
+        const uint32_t round = (uint32_t) (j / (2 * ngroups));
+        if(!mbar_wait(&empty[x], (round & 1) ^ 1, err, 21)) return; // (every lane polls; all agree)
+        if(lane == t) {
+          meta[x] = mine;
+          mbar_arrive_expect_tx(&full[x], bytes);
+          if(bytes > 0)
+            bulk_g2s(ring + (size_t) x * stage_bytes, reinterpret_cast<const void*>(a16), bytes, &full[x]);
+        }
+        __syncwarp();
       }
     }
     return;
   }
-  // ---------------- consumers: warps 1..kStagedWarps ----------------
-  const int cw  = warp - 1;
-  const int ctid = threadIdx.x - 32;
-  int       slot = 0;
-  uint32_t  ph   = 0;
-  for(int u = blockIdx.x, it = 0; u < nunits; u += gridDim.x, it++) {
+  // ---------------- consumers: groups of G warps ----------------
+  const int cw = warp - 1, grp = cw / G, h = cw % G;
+  if(grp >= ngroups) return;
+  const int      barid = 1 + grp; // named barrier of the group (0 is __syncthreads)
+  const uint64_t bias  = S >= 8 ? 0x8080808080808080ull : ((1ull << (8 * S)) - 1) / 255 * 128;
+  const int      rr = lane >> 4, c = (lane >> 2) & 3, q = lane & 3; // row of the pair, chunk, quad
+  const int      rot = (q + c) & 3;
+  uint32_t       sel2 = 0; // byte permute taking the rotated values back to k order
+#pragma unroll
+  for(int pos = 0; pos < 4; pos++) {
+    const int t = (pos - rot) & 3;
+    sel2 |= (uint32_t) (t < 2 ? t : t + 2) << (4 * pos);
+  }
+  for(int j = grp;; j += ngroups) {
+    const int u = blockIdx.x + j * gridDim.x;
+    if(u >= nunits) break;
+    const int      par   = (j / ngroups) & 1, x = 2 * grp + par;
+    const uint32_t round = (uint32_t) (j / (2 * ngroups));
     {
-      const bool got = mbar_wait(&full[slot], ph, err, 22);
+      const bool got = mbar_wait(&full[x], round & 1, err, 22);
       uint32_t   anyfail;
       asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
-                   "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                   "bar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
                    : "=r"(anyfail)
-                   : "r"((uint32_t) got), "n"(32 * kStagedWarps)
+                   : "r"((uint32_t) got), "r"(barid), "n"(32 * G)
                    : "memory");
       if(anyfail) return;
     }
-    const StageMeta    m   = meta[slot];
-    const SplitBlock&  b   = blocks[m.blk];
-    uint8_t*           buf = ring + (size_t) slot * stage_bytes;
-    const double*      rowbase = reinterpret_cast<const double*>(buf + m.delta);
-    const int          K   = b.K;
-    const int          par = it & 1;
-    if(m.tail && ctid == 0) { // the last element, past the copy's 16-byte aligned end
-      const_cast<double*>(rowbase)[(int64_t) m.nlive * K - 1] =
-        __ldg(src + b.src_off + (int64_t) (m.row0 + m.nlive) * K - 1);
-      // ordered before the bulk copy that later refills this stage
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    }
-    if(m.tail) asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
-    // row maxima: kStagedWarps / R warps per row, each over its share of K
-    {
-      constexpr int WPR = kStagedWarps / R;
-      const int     r = cw % R, sh = cw / R;
-      double        mx = 0.0;
-      if(r < m.nlive) {
-        const double* x  = rowbase + (int64_t) r * K;
-        const int     k0 = sh * ((K + WPR - 1) / WPR), k1 = min(K, k0 + (K + WPR - 1) / WPR);
-        for(int k = k0 + lane; k < k1; k += 32) mx = fmax(mx, fabs(x[k]));
+    const UnitMeta m       = meta[x];
+    const int      K       = m.K;
+    const int      tr      = TR > 0 ? TR : m.tile_rows;
+    double*        rowbase = reinterpret_cast<double*>(ring + (size_t) x * stage_bytes + m.delta);
+    if(m.tail) { // the last element, past the copy's 16-byte aligned end
+      if(h == 0 && lane == 0) {
+        rowbase[(int64_t) m.nlive * K - 1] = __ldg(src + m.tail_src);
+        // ordered before the bulk copy that later refills this stage
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       }
+      asm volatile("bar.sync %0, %1;\n" ::"r"(barid), "n"(32 * G) : "memory");
+    }
+    // row maxima: 16 lanes per row over this warp's K range, then over the group
+    const double* xr   = rowbase + (int64_t) rr * K;
+    const bool    live = rr < m.nlive;
+    double        mx   = 0.0;
+    if(live) {
+      const int span = (K + G - 1) / G, kb = h * span, ke = min(K, kb + span);
+      double    m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+      int       k = kb + (lane & 15);
+      for(; k + 48 < ke; k += 64) {
+        m0 = fmax(m0, fabs(xr[k]));
+        m1 = fmax(m1, fabs(xr[k + 16]));
+        m2 = fmax(m2, fabs(xr[k + 32]));
+        m3 = fmax(m3, fabs(xr[k + 48]));
+      }
+      for(; k < ke; k += 16) m0 = fmax(m0, fabs(xr[k]));
+      mx = fmax(fmax(m0, m1), fmax(m2, m3));
+    }
 #pragma unroll
-      for(int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if(lane == 0) part[par * kStagedWarps + cw] = mx;
+    for(int o = 8; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    // partials alternate between two buffers by unit parity: a warp writes this buffer
+    // again only after the group's next barrier, which every reader of it has passed
+    double* pp = part + (grp * 2 + par) * G * 2;
+    if((lane & 15) == 0) pp[h * 2 + rr] = mx;
+    asm volatile("bar.sync %0, %1;\n" ::"r"(barid), "n"(32 * G) : "memory");
+    mx = 0.0;
+#pragma unroll
+    for(int w = 0; w < G; w++) mx = fmax(mx, pp[w * 2 + rr]);
+    const int e = row_exponent(mx);
+    if(h == 0 && (lane & 15) == 0) {
+      exps[m.exp_base + rr] = e;
+      if(mx > 0.0) atomicMax(blockmax + m.id, e);
     }
-    asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
-    if(ctid < R) {
-      const int r   = ctid;
-      double    mx  = 0.0;
-      for(int w = r; w < kStagedWarps; w += R) mx = fmax(mx, part[par * kStagedWarps + w]);
-      const bool live = r < m.nlive;
-      const int  e    = row_exponent(mx);
-      shift[par * 8 + r] = live ? 8 * S - 1 - e : kPadRow;
-      exps[b.exp_off + m.row0 + r] = e;
-      if(mx > 0.0) atomicMax(blockmax + b.id, e);
-    }
-    asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kStagedWarps) : "memory");
-    // digits: lanes per 16-wide k chunk = 4 R (row, quad); 32 / (4 R) chunks per warp step
-    {
-      constexpr int LPC = 4 * R, CPW = 32 / LPC;
-      const int     rr = (lane % LPC) >> 2, q = lane & 3, sub = lane / LPC;
-      const int     sh = shift[par * 8 + rr];
-      const bool    live = sh != kPadRow;
-      // 2^sh in one factor where it is a normal double, else as two (tiny rows)
-      const bool    wide = live && (sh > 1000 || sh < -1000);
-      const double  f1 = ldexp(1.0, live ? (wide ? sh / 2 : sh) : 0), f2 = ldexp(1.0, wide ? sh - sh / 2 : 0);
-      const int     row = m.row0 + rr; // row within the block
-      const int     nkc = b.K_pad / KC;
-      uint8_t*      out = dst + b.dst_off + (int64_t) (row / b.tile_rows) * nkc * S * b.tile_rows * KC +
-                     ((row % b.tile_rows) >> 3) * 128 + (row & 7) * 16 + q * 4;
-      const double* x   = rowbase + (int64_t) rr * K;
-      const int     n16 = b.K_pad / 16;
-      for(int k16 = cw * CPW + sub; k16 < n16; k16 += kStagedWarps * CPW) {
+    if(m.nlive > 0) {
+      // digits: 2^sh in one factor where it is a normal double, else as two (tiny rows)
+      const int     sh   = live ? 8 * S - 1 - e : 0;
+      const bool    wide = sh > 1000 || sh < -1000;
+      const double  f1 = ldexp(1.0, wide ? sh / 2 : sh), f2 = ldexp(1.0, wide ? sh - sh / 2 : 0);
+      const int     row   = m.row0 + rr;
+      const int     nkc   = m.K_pad / KC;
+      const int64_t dstep = (int64_t) S * tr * 16; // one K half of a 32-byte K chunk
+      uint8_t*      o = dst + m.dst_off + (int64_t) (row / tr) * nkc * S * tr * KC + ((row % tr) >> 3) * 128 +
+                   (row & 7) * 16 + q * 4 + ((c >> 1) * 2 + (c & 1) + (int64_t) h * 4) * dstep;
+      const int     n16     = m.K_pad / 16;
+      const bool    anywide = __any_sync(0xffffffffu, wide && live);
+      for(int k16 = 4 * h + c; k16 < n16; k16 += 4 * G, o += 4 * G * dstep) {
         const int k0 = k16 * 16 + q * 4;
         double    v[4];
 #pragma unroll
-        for(int t = 0; t < 4; t++) v[t] = (live && k0 + t < K) ? x[k0 + t] : 0.0;
+        for(int t = 0; t < 4; t++) {
+          const int kk = k0 + ((t + rot) & 3);
+          v[t]         = (live && kk < K) ? xr[kk] : 0.0;
+        }
+        if(anywide)
+#pragma unroll
+          for(int t = 0; t < 4; t++) v[t] *= f2;
         uint32_t lo[4], hi[4];
 #pragma unroll
         for(int t = 0; t < 4; t++) {
-          const uint64_t Y = digit_word<S>(wide ? v[t] * f2 : v[t], f1, bias);
+          const uint64_t Y = digit_word<S>(v[t], f1, bias);
           lo[t]            = (uint32_t) Y;
           hi[t]            = (uint32_t) (Y >> 32);
         }
-        uint8_t* o = out + (int64_t) (k16 >> 1) * S * b.tile_rows * KC + (k16 & 1) * S * b.tile_rows * 16;
 #pragma unroll
         for(int i = 0; i < S; i++) {
           const int p = S - 1 - i; // byte of Y holding digit i
-          uint32_t  w;
+          uint32_t  t0, t1;
           if(p < 4) {
-            const uint32_t t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
-            const uint32_t t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
-            w                 = __byte_perm(t0, t1, 0x5410);
+            t0 = __byte_perm(lo[0], lo[1], p | ((p + 4) << 4));
+            t1 = __byte_perm(lo[2], lo[3], p | ((p + 4) << 4));
           }
           else {
-            const uint32_t t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
-            const uint32_t t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
-            w                 = __byte_perm(t0, t1, 0x5410);
+            t0 = __byte_perm(hi[0], hi[1], (p - 4) | (p << 4));
+            t1 = __byte_perm(hi[2], hi[3], (p - 4) | (p << 4));
           }
-          __stcs(reinterpret_cast<unsigned int*>(o + (int64_t) i * b.tile_rows * 16), w ^ 0x80808080u);
+          __stcs(reinterpret_cast<unsigned int*>(o + (int64_t) i * tr * 16), __byte_perm(t0, t1, sel2) ^ 0x80808080u);
         }
       }
     }
     __syncwarp();
-    if(lane == 0) mbar_arrive(&empty[slot]); // this warp is done with the stage
-    if(++slot == nst) {
-      slot = 0;
-      ph ^= 1;
-    }
+    if(lane == 0) mbar_arrive(&empty[x]); // this warp is done with the stage
   }
 }
 
@@ -1104,8 +1142,8 @@ SplitBlock view_block(const int32_t* dims, int nmodes, const int8_t* rpos, int n
   return b;
 }
 
-// Staged-kernel eligibility: K contiguous, row r at element offset r * K, and two
-// 4-row stages of the longest row fit in shared memory.
+// Staged-kernel eligibility: K contiguous, row r at element offset r * K, and the two
+// stages of one warp group (two rows each) fit in shared memory.
 bool staged_ok(const SplitBlock& b, int esize) {
   if(esize != 1 || !b.kcontig) return false;
   int64_t st = b.K;
@@ -1113,7 +1151,7 @@ bool staged_ok(const SplitBlock& b, int esize) {
     if(b.rstr[j] != st) return false;
     st *= b.rdim[j];
   }
-  return staged_stage_bytes(4, b.K) * 2 + kStagedHead <= kStagedSmem;
+  return staged_stage_bytes(b.K) * 2 + kStagedHead <= kStagedSmem;
 }
 
 void chunk_table(const std::vector<SplitBlock>& bl, std::vector<int32_t>& out) {
@@ -1302,23 +1340,24 @@ int sm_count() {
   return n;
 }
 
-template<int S, int R>
+template<int S, int TR>
 void launch_staged(const SplitSet& x, const double* src, uint8_t* slices, int32_t* exps,
                    int32_t* blockmax, int* err, cudaStream_t st) {
   const int      nblocks = (int) x.cbegin.size() - 1, nchunks = x.cbegin.back();
-  const uint32_t sb      = (uint32_t) staged_stage_bytes(R, x.kmax);
-  const int      nst     = (int) std::min<int64_t>(8, (kStagedSmem - kStagedHead) / sb);
-  const size_t   smem    = kStagedHead + (size_t) nst * sb;
+  const uint32_t sb      = (uint32_t) staged_stage_bytes(x.kmax);
+  const int      ngroups = (int) std::min<int64_t>(kSplitMaxGroups, (kStagedSmem - kStagedHead) / (2 * (int64_t) sb));
+  TB_EXPECTS(ngroups >= 1, "staged split: one group's stages must fit in shared memory");
+  const size_t   smem    = kStagedHead + (size_t) 2 * ngroups * sb;
   static bool    configured[64] = {false};
   int            dev            = 0;
   TB_CUDA(cudaGetDevice(&dev));
   if(dev < 64 && !configured[dev]) {
-    TB_CUDA(cudaFuncSetAttribute(k_split_staged<S, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem));
+    TB_CUDA(cudaFuncSetAttribute(k_split_staged<S, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem));
     configured[dev] = true;
   }
-  const int grid = std::min(nchunks * (8 / R), sm_count());
-  k_split_staged<S, R><<<grid, 32 * (kStagedWarps + 1), smem, st>>>(x.d_blocks, x.d_cbegin, nblocks, nchunks, nst, sb, src, slices, exps,
-                                                blockmax, err);
+  const int grid = (int) std::min<int64_t>((int64_t) nchunks * 4, sm_count());
+  k_split_staged<S, TR><<<grid, 32 * (1 + ngroups * kSplitGroup), smem, st>>>(
+    x.d_blocks, x.d_cbegin, nblocks, nchunks, ngroups, sb, src, slices, exps, blockmax, err);
 }
 
 // Splits the blocks of one operand: the staged kernel for the blocks with contiguous
@@ -1334,10 +1373,9 @@ void split_sets(const SplitSet& staged, const SplitSet& general, const double* s
   }
   if constexpr(!BF) {
     if(!staged.blocks.empty() && staged.cbegin.back() > 0) {
-      // 8-row units while three stages of the longest row fit, else 4-row units
-      if(kStagedHead + 3 * staged_stage_bytes(8, staged.kmax) <= kStagedSmem)
-        launch_staged<S, 8>(staged, src, slices, exps, blockmax, err, st);
-      else launch_staged<S, 4>(staged, src, slices, exps, blockmax, err, st);
+      // A tiles (128 rows) with the row count fixed at compile time, B tiles read it
+      if(staged.blocks.front().tile_rows == MT) launch_staged<S, MT>(staged, src, slices, exps, blockmax, err, st);
+      else launch_staged<S, 0>(staged, src, slices, exps, blockmax, err, st);
     }
   }
 }
