@@ -607,6 +607,8 @@ struct I8Params {
   const uint8_t*  tslices; // digit count of each task (1..S)
   int*            ctr;     // next output tile to hand out (zero at launch)
   int             xpose;   // C is contiguous along the tile's columns: transposed reductions
+  int             store;   // C = alpha * result (an assignment whose output blocks this
+                           // launch covers completely) instead of C += alpha * result
 };
 
 template<int S, int NT>
@@ -967,7 +969,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       if(!ok) break;
       // C (+)= alpha * result: one reduction per element (c + alpha * r, rounded once,
       // as a load-add-store would be; every element of C belongs to exactly one output
-      // tile), performed at L2, so the epilogue does not wait for C's memory.
+      // tile), performed at L2, so the epilogue does not wait for C's memory; a plain
+      // store for an assignment (p.store).
       // A thread holds one row of the tile; when C is contiguous along the columns
       // instead, the warp passes its values through shared memory kXCols columns at a
       // time so that each reduction instruction covers 4 rows x 8 adjacent columns.
@@ -986,7 +989,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
             for(int it = 0; it < kXCols; it++) { // rows it * 4 + rsub
               const int     r  = it * (32 / kXCols) + rsub;
               const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
-              if(ro >= 0 && o >= 0) atomicAdd(p.C + ro + o, xb[csub * kXStride + r]);
+              if(ro >= 0 && o >= 0) {
+                if(p.store) p.C[ro + o] = xb[csub * kXStride + r];
+                else atomicAdd(p.C + ro + o, xb[csub * kXStride + r]);
+              }
             }
             __syncwarp(); // the next columns overwrite the buffer
           }
@@ -998,7 +1004,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
 #pragma unroll
         for(int x = 0; x < NH; x++) {
           const int o = nof[col0 + x];
-          if(o >= 0) atomicAdd(crow + o, p.alpha * racc[x]);
+          if(o >= 0) {
+            if(p.store) crow[o] = p.alpha * racc[x];
+            else atomicAdd(crow + o, p.alpha * racc[x]);
+          }
         }
       }
     }
@@ -1028,7 +1037,7 @@ struct SplitSet {
 // tensor's modes), kept in the context's arena while the tensor stays read-only, so
 // that constant operands (the integrals) are split once instead of in every
 // contraction that reads them.
-struct DigitEntry {
+struct DigitEntry final : DigitCacheEntry {
   Arena*                        arena = nullptr;
   int64_t*                      used  = nullptr; // the context's cache account
   int64_t                       bytes = 0;
@@ -1040,18 +1049,24 @@ struct DigitEntry {
   SplitSet                      staged, general;
   const double*                 src    = nullptr; // the tensor's packed store
   bool                          filled = false;   // digits written (stream order)
-  ~DigitEntry() {
-    for(SplitSet* x: {&staged, &general}) {
-      cudaFree(x->d_blocks);
-      cudaFree(x->d_cbegin);
-    }
-    cudaFree(err);
+  void                          retire() override {
     if(arena) {
       arena->deallocate(slices);
       arena->deallocate(exps);
       arena->deallocate(blockmax);
     }
     if(used) *used -= bytes;
+    arena = nullptr, used = nullptr, bytes = 0;
+    slices = nullptr, exps = nullptr, blockmax = nullptr;
+    filled = false;
+  }
+  ~DigitEntry() override {
+    for(SplitSet* x: {&staged, &general}) {
+      cudaFree(x->d_blocks);
+      cudaFree(x->d_cbegin);
+    }
+    cudaFree(err);
+    retire();
   }
 };
 
@@ -1407,7 +1422,7 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
 
 template<int S, int NT, bool BF>
 void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha,
-                 const uint8_t* slices, const int32_t* exps, double* C, cudaStream_t st) {
+                 const uint8_t* slices, const int32_t* exps, double* C, bool store, cudaStream_t st) {
   if(L.items.empty()) return;
   I8Params p;
   p.a_slices = L.a_cache ? L.a_cache->slices : slices;
@@ -1426,6 +1441,7 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   p.ctr     = L.d_ctr;
   // transposed reductions when C's last mode (stride 1) is a column label of the tile
   p.xpose = xpose_fits<S, NT>() && lc.nn > 0 && lc.n_c[lc.nn - 1] == lc.nc - 1 ? 1 : 0;
+  p.store = store ? 1 : 0;
   TB_CUDA(cudaMemsetAsync(L.d_ctr, 0, sizeof(int), st));
   const size_t smem = smem_bytes<S, NT>();
   static bool  configured[64] = {false};
@@ -1442,17 +1458,17 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
 
 template<int S, bool BF = false>
 void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha, const double* A,
-           const double* B, double* C, uint8_t* slices, int32_t* exps, cudaStream_t st,
+           const double* B, double* C, uint8_t* slices, int32_t* exps, bool store, cudaStream_t st,
            cudaEvent_t* ev) {
   if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
   launch_split<S, BF>(L, wl, A, B, slices, exps, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
   // output tile width: 80 columns by default for S <= 6 (S x NT <= 512 TMEM columns)
   if constexpr(S * 80 <= 512) {
-    if(L.NT == 80) launch_gemm<S, 80, BF>(L, wl, lc, alpha, slices, exps, C, st);
+    if(L.NT == 80) launch_gemm<S, 80, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
   }
-  if(L.NT == 64) launch_gemm<S, 64, BF>(L, wl, lc, alpha, slices, exps, C, st);
-  if(L.NT == 48) launch_gemm<S, 48, BF>(L, wl, lc, alpha, slices, exps, C, st);
+  if(L.NT == 64) launch_gemm<S, 64, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
+  if(L.NT == 48) launch_gemm<S, 48, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
 }
 
@@ -1543,7 +1559,7 @@ void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* 
   const LabelClasses& lc = plan.lc;
   if(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0) {
     // Hadamard / one-sided reduction labels and outer products run on the FP64 path.
-    launch_contract_fp64(plan, wl, alpha, 1.0, 0, A, B, C, stream);
+    launch_contract_fp64(plan, wl, alpha, 1.0, plan.store ? 1 : 0, A, B, C, stream);
     return;
   }
   const int S     = bf ? 2 : (plan.nslices > 0 ? std::min(std::max(plan.nslices, 3), 8) : slices_for(plan.err_target));
@@ -1569,14 +1585,15 @@ void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* 
     for(auto& e: evs) TB_CUDA(cudaEventCreate(&e));
     ev = evs;
   }
-  if(bf) run_s<2, true>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev);
+  const bool st = plan.store;
+  if(bf) run_s<2, true>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev);
   else switch(S) {
-    case 3: run_s<3>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
-    case 4: run_s<4>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
-    case 5: run_s<5>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
-    case 6: run_s<6>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
-    case 7: run_s<7>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
-    default: run_s<8>(*L, wl, lc, alpha, A, B, C, slices, exps, stream, ev); break;
+    case 3: run_s<3>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
+    case 4: run_s<4>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
+    case 5: run_s<5>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
+    case 6: run_s<6>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
+    case 7: run_s<7>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
+    default: run_s<8>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;
   }
   if(plan.pinned) {
     plan.pinned->put(exps);

@@ -368,7 +368,8 @@ bool Tensor::block_is_zero(const int64_t* blockid) const {
 // context's stream (after the work already enqueued there, which includes the waits
 // for asynchronous host writes) for blocks whose elements are all zero.
 void set_read_only(Tensor& T, bool on) {
-  T.digit_cache.clear(); // (entries still used by cached layouts live until those go)
+  for(auto& kv: T.digit_cache) kv.second->retire(); // memory back now, even if a layout refers to it
+  T.digit_cache.clear();
   if(!on) {
     T.read_only = false;
     T.zero_block.clear();
@@ -930,12 +931,11 @@ void Sched::prepare_mult(Op& op) {
 }
 
 // Assignment C = alpha * A * B, queued as Set(0) + Mult (MultOp::canonicalize,
-// multop.hpp:255-269), on one rank under an FP64 request: the FP64 kernel stores its
-// result into the output blocks of groups with tasks (every element of those blocks is
-// written once), and the Set zeroes only the blocks of groups without tasks.  Saves
-// the fill of C and the read of every C element.  (The split kernels keep the fill
-// and their one atomic add per element: plain stores from their epilogue measured
-// slower on large outputs.)
+// multop.hpp:255-269), on one rank: the contraction kernel (FP64, or the split kernels'
+// epilogue) stores its result into the output blocks of groups with tasks (every
+// element of those blocks is written once), and the Set zeroes only the blocks of
+// groups without tasks.  Saves the fill of C and the read (or the atomic add) of every
+// C element.
 void Sched::fuse_assign(Op& set, Op& mult) {
   prepare_mult(mult);
   mult.store = true;
@@ -1300,7 +1300,7 @@ void Sched::execute(bool profile) {
       ops[i + 1].za = known(ops[i + 1].a.t);
       ops[i + 1].zb = known(ops[i + 1].b.t);
     }
-    if(nranks == 1 && ctx->mode == TB_MODE_FP64 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
+    if(nranks == 1 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
        ops[i].is_assign && ops[i].value == 0.0 &&
        ops[i + 1].kind == Op::Mult && same_target(ops[i].lhs, ops[i + 1].lhs) &&
        ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t && // C read as an operand needs the fill

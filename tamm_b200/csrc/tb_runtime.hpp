@@ -109,6 +109,16 @@ struct TIS {
   int64_t find_root(int64_t r) const;
 };
 
+// Kept split digits of a read-only tensor under one operand view (defined by the
+// split-INT8 contraction).  retire() returns the entry's device memory and its share
+// of the context's cache budget at once, also while a cached contraction layout still
+// refers to the entry (that layout is rebuilt before its next launch); the arena's
+// frees are stream ordered, so work already enqueued still reads valid memory.
+struct DigitCacheEntry {
+  virtual ~DigitCacheEntry() = default;
+  virtual void retire()      = 0;
+};
+
 struct Tensor {
   Serial                            serial;
   int                               nmodes = 0;
@@ -131,8 +141,8 @@ struct Tensor {
   uint64_t                          ro_serial = 0;
   std::vector<uint8_t>              zero_block;
   // split digits of this (read-only) tensor per operand view, kept by the split-INT8
-  // contraction (opaque here; dropped whenever the read-only mark changes)
-  mutable std::map<std::string, std::shared_ptr<void>> digit_cache;
+  // contraction (retired whenever the read-only mark changes or the storage goes)
+  mutable std::map<std::string, std::shared_ptr<DigitCacheEntry>> digit_cache;
   // lambda tensor (tb_tensor_create_lambda / _built): no storage, blocks on demand
   tb_block_fn                       lambda_block = nullptr;
   tb_batch_fn                       lambda_batch = nullptr;

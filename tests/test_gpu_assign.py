@@ -1,8 +1,9 @@
 """Assignments C = alpha * A * B (queued as Set(0) + Mult, as TAMM's
-MultOp::canonicalize does, multop.hpp:255-269).  On one rank under an FP64 request
-the scheduler runs the pair fused: the FP64 kernel stores its result without reading
-C, and the fill touches only the output blocks that receive no task; the split modes
-run the pair as queued.
+MultOp::canonicalize does, multop.hpp:255-269).  On one rank the scheduler runs the
+pair fused: the contraction kernel (FP64, or the split kernels' epilogue) stores its
+result without reading C, and the fill touches only the output blocks that receive no
+task.  The output is written both with its last mode a column label of the tile (the
+split epilogue's transposed stores) and a row label (one row per thread).
 
 C(a,b) is dense while A(a,c) and B(c,b) conserve spin, so C's mixed-spin blocks have
 no task and must still come out zero; C starts out holding garbage.  Checked in FP64
@@ -44,9 +45,10 @@ def spaces():
     return MO("virt")
 
 
+@pytest.mark.parametrize("transposed", [False, True])
 @pytest.mark.parametrize("mode,tol", [(tb.Precision.FP64, 1e-12), (tb.Precision.INT8, 1e-11),
                                       (tb.Precision.BF16X3, 5e-5)])
-def test_assign_stores_and_zeroes_blocks_without_tasks(ec, spaces, mode, tol):
+def test_assign_stores_and_zeroes_blocks_without_tasks(ec, spaces, mode, tol, transposed):
     V = spaces
     rng = np.random.default_rng(5)
     A = tb.Tensor([V, V], spin=(1, 1)).allocate(ec)
@@ -56,13 +58,16 @@ def test_assign_stores_and_zeroes_blocks_without_tasks(ec, spaces, mode, tol):
     B.write(rng.normal(0, 1e-2, size=B.nelems))
     C.write(np.full(C.nelems, 7.0))
     want = -0.5 * _dense(A) @ _dense(B)
+    if transposed:
+        want = want.T
     a, b, c = V.labels(3)
     ec.set_precision(mode, 1e-11)
     try:
         sch = tb.Scheduler(ec)
         for _ in range(2):  # the second run reuses the scheduler's cached plan and work list
             C.write(np.full(C.nelems, 7.0))
-            sch(C(a, b).assign(-0.5 * A(a, c) * B(c, b))).execute(tb.ExecutionHW.GPU)
+            lhs = C(b, a) if transposed else C(a, b)
+            sch(lhs.assign(-0.5 * A(a, c) * B(c, b))).execute(tb.ExecutionHW.GPU)
             got = _dense(C)
             assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want))
             assert np.all(got[want == 0.0] == 0.0)  # mixed-spin blocks: no task, zero fill

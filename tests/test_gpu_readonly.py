@@ -177,7 +177,8 @@ def test_structural_zeros_within_one_execute(ec):
 def test_digit_cache_bitwise_and_bounded(ec):
     """With the digit cache on, the read-only v is split once and kept: two contractions
     in a row give the bits of the per-call split, the cache holds bytes, a budget too
-    small keeps nothing, and clearing the mark releases them."""
+    small keeps nothing, and clearing the mark releases them at once, while the
+    scheduler still holds the contraction's cached layout."""
     lad, vh, zero = _ladder_with_zero_blocks(ec, seed=13)
     a, b, c, d, i, j = lad.labels
     want = _oracle(lad, vh)
@@ -198,7 +199,8 @@ def test_digit_cache_bitwise_and_bounded(ec):
         assert np.array_equal(first, plain) and np.array_equal(second, plain)
         assert rel_err(second, want) <= 1e-11
         lad.v.set_read_only(False)  # drops the entries (and the work lists keyed by the mark)
-        run()
+        assert ec.digit_cache_info()[0] == 0
+        assert rel_err(run(), want) <= 1e-11
         lad.v.set_read_only(True)
         ec.set_digit_cache(1)  # too small for any entry: split per call, same bits
         assert np.array_equal(run(), plain)
