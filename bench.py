@@ -43,6 +43,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FP64-accurate TFLOP/s, block-sparse CC contractions: split-INT8 vs plain FP64"
 
+# k_contract_i8<6, 80> on the ladder: DRAM bytes (read + write) per INT8 tensor op from one
+# ncu launch of the O=40/V=160 ladder (1.883e9 B read + 0.167e9 B written for 4.571e12
+# ops incl. tile padding)
+I8_DRAM_BYTES_PER_OP = (1.883e9 + 0.167e9) / 4.571e12
+I8_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_contract_i8<6,80> launch of the "
+                     "O=40/V=160 ladder (2.05 GB for 4.57e12 INT8 ops), scaled by this launch's INT8 ops")
+
+
+def gemm_bytes_alg(lad, v_zero_elems, S):
+    """Algorithmic DRAM bytes of one ladder GEMM launch: every digit of the nonzero v
+    blocks and of t2 read once, r2 read and written once."""
+    return S * (lad.v.nelems - v_zero_elems + lad.t2.nelems) + 16.0 * lad.r2.nelems
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -562,6 +575,13 @@ def main():
         nsplit = lad.v.nelems - v_zero_elems + lad.t2.nelems  # blocks of v that take part
         split_bytes = nsplit * (8 + S * (2 if headline == "bf16x3" else 1)) + 0.0
         hbm = peaks.get("hbm_gbs")
+        if headline == "int8":
+            # DRAM traffic per launch from ncu: one launch of the O=40/V=160 ladder (same
+            # output width N = 400, so the same re-reads of A digits per op), scaled by
+            # the INT8 ops of this launch
+            roof["traffic"] = st["int8_ops"] * I8_DRAM_BYTES_PER_OP
+            roof["traffic_source"] = I8_TRAFFIC_SOURCE
+            roof["traffic_algorithmic"] = gemm_bytes_alg(lad, v_zero_elems, S)
         roof["split"] = {"bound": "hbm", "achieved": split_bytes / (st["split_ms"] * 1e-3) / 1e9,
                          "peak": hbm, "unit": "GB/s",
                          "frac": (split_bytes / (st["split_ms"] * 1e-3) / 1e9 / hbm) if hbm else None,

@@ -329,8 +329,12 @@ __global__ void __launch_bounds__(256) k_split_fused(const SplitBlock* __restric
 //   Producer (warp 0): resolves 32 units at a time, one per lane (block by binary
 // search over the per-block chunk prefix, then the unit's copy range and the fields the
 // consumers need), and issues their copies in order into the stage of the group that
-// takes each unit; the unit records travel in shared memory beside the stages, so a
-// consumer reads no block record from global memory.
+// takes each unit.  A CTA owns whole 8-row chunks: the four units of a chunk fill the
+// same 128-byte lines of every digit plane, and lines completed by one SM within a
+// short time leave L2 whole (units spread over SMs measured 1.4x slower at the size
+// of the O=40/V=360 ladder's v, while as fast on a quarter of it).  The unit records
+// travel in shared memory beside the stages, so a consumer reads no block record from
+// global memory.
 //   Consumers: independent groups of kSplitGroup warps, each group with two stages of
 // its own, so a group's only synchronisation is a named barrier of its own warps.
 // Warp h of a group takes the h-th K range of the row maxima and every kSplitGroup-th
@@ -351,8 +355,8 @@ struct UnitMeta {
 };
 static_assert(sizeof(UnitMeta) == 64, "unit record size");
 
-constexpr int     kSplitGroup     = 2;            // consumer warps per group
-constexpr int     kSplitMaxGroups = 8;            // groups per CTA, at most
+constexpr int     kSplitGroup     = 4;            // consumer warps per group
+constexpr int     kSplitMaxGroups = 4;            // groups per CTA, at most
 constexpr int64_t kStagedSmem     = 227 * 1024;   // dynamic shared memory of one CTA, at most
 constexpr int64_t kStagedHead     = 2048;         // barriers, unit records, partial maxima
 // bytes of one stage of 2 rows of K doubles (+16 for the aligned start), 128-byte multiple
@@ -377,6 +381,8 @@ __global__ void __launch_bounds__(32 * (1 + kSplitMaxGroups * kSplitGroup), 1)
   static_assert(1280 + 2 * kSplitMaxGroups * G * 2 * 8 <= kStagedHead, "partial maxima");
   const int     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int     nunits = nchunks * 4; // two rows per unit, four units per 8-row chunk
+  // units of this CTA: the four of each of its chunks
+  const int     myunits = ((nchunks - (int) blockIdx.x + (int) gridDim.x - 1) / (int) gridDim.x) * 4;
   if(threadIdx.x == 0) {
     for(int x = 0; x < 2 * ngroups; x++) {
       mbar_init(&full[x], 1);
@@ -387,10 +393,13 @@ __global__ void __launch_bounds__(32 * (1 + kSplitMaxGroups * kSplitGroup), 1)
   __syncthreads();
   if(warp == 0) {
     // ---------------- producer: 32 unit records at a time, copies in unit order -------
-    // The CTA's j-th unit (u = blockIdx.x + j * gridDim.x) goes to group j mod ngroups,
-    // that group's stage (j / ngroups) mod 2.
-    for(int ub = blockIdx.x, jb = 0; ub < nunits; ub += 32 * gridDim.x, jb += 32) {
-      const int u = ub + lane * gridDim.x;
+    // The CTA's j-th unit is unit j mod 4 of 8-row chunk blockIdx.x + (j / 4) * gridDim.x
+    // (the four units of a chunk, whose digits share every 128-byte line, are written
+    // by one SM close together in time); it goes to group j mod ngroups, that group's
+    // stage (j / ngroups) mod 2.
+    for(int jb = 0; jb < myunits; jb += 32) {
+      const int jl = jb + lane;
+      const int u  = jl < myunits ? ((int) blockIdx.x + (jl >> 2) * (int) gridDim.x) * 4 + (jl & 3) : nunits;
       UnitMeta  mine{};
       uintptr_t a16   = 0;
       uint32_t  bytes = 0;
@@ -425,7 +434,7 @@ __global__ void __launch_bounds__(32 * (1 + kSplitMaxGroups * kSplitGroup), 1)
         }
       }
       for(int t = 0; t < 32; t++) {
-        if(ub + t * gridDim.x >= nunits) break;
+        if(jb + t >= myunits) break;
         const int      j     = jb + t;
         const int      x     = 2 * (j % ngroups) + ((j / ngroups) & 1);
         const uint32_t round = (uint32_t) (j / (2 * ngroups));
@@ -454,9 +463,7 @@ __global__ void __launch_bounds__(32 * (1 + kSplitMaxGroups * kSplitGroup), 1)
     const int t = (pos - rot) & 3;
     sel2 |= (uint32_t) (t < 2 ? t : t + 2) << (4 * pos);
   }
-  for(int j = grp;; j += ngroups) {
-    const int u = blockIdx.x + j * gridDim.x;
-    if(u >= nunits) break;
+  for(int j = grp; j < myunits; j += ngroups) {
     const int      par   = (j / ngroups) & 1, x = 2 * grp + par;
     const uint32_t round = (uint32_t) (j / (2 * ngroups));
     {
@@ -1370,7 +1377,7 @@ void launch_staged(const SplitSet& x, const double* src, uint8_t* slices, int32_
     TB_CUDA(cudaFuncSetAttribute(k_split_staged<S, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem));
     configured[dev] = true;
   }
-  const int grid = (int) std::min<int64_t>((int64_t) nchunks * 4, sm_count());
+  const int grid = (int) std::min<int64_t>((int64_t) nchunks, sm_count()); // whole chunks per CTA
   k_split_staged<S, TR><<<grid, 32 * (1 + ngroups * kSplitGroup), smem, st>>>(
     x.d_blocks, x.d_cbegin, nblocks, nchunks, ngroups, sb, src, slices, exps, blockmax, err);
 }
