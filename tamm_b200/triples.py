@@ -161,24 +161,38 @@ def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int):
     return Wt, mult_info(*x)[2] + mult_info(*y)[2]
 
 
-def energy(P: TriplesProblem, pairs, sch: Scheduler):
-    """E summed over the given steps (i, j block); returns (E, FP64 FLOPs, device ms)."""
+def energy(P: TriplesProblem, pairs, sch: Scheduler, release_every: int = 8):
+    """E summed over the given steps (i, j block); returns (E, FP64 FLOPs, device ms).
+
+    The steps are enqueued back to back (tb_sched_execute_async): the host builds the
+    next step's work lists while the device runs the current one, and the device time
+    is that of the whole sample, one pair of CUDA events around it.  The cached plans
+    and work lists of finished steps (they never recur) are dropped every
+    `release_every` steps, after the device has finished them."""
     import torch
     stream = torch.cuda.ExternalStream(P.ec.stream)
     sch.set_scalar(SLOT_E, 0.0).execute()
-    flops, ms, keep = 0.0, 0.0, []
-    for i, j in pairs:
+    flops, keep = 0.0, []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for n, (i, j) in enumerate(pairs):
         Wt, fl = queue_pair(P, sch, i, j)
         keep.append(Wt)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        sch.execute(ExecutionHW.GPU)
-        e1.record(stream)
-        e1.synchronize()
-        ms += e0.elapsed_time(e1)
+        sch.execute_async()
         flops += fl
-        sch.release()  # this step's work lists never recur
-        Wt.deallocate()
+        if (n + 1) % release_every == 0 and n + 1 < len(pairs):
+            sch.wait()
+            sch.release()
+            for t in keep:
+                t.deallocate()
+            keep = []
+    e1.record(stream)
+    sch.wait()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sch.release()
+    for t in keep:
+        t.deallocate()
     return float(sch.scalars(SLOT_E + 1)[SLOT_E]), flops, ms
 
 
