@@ -24,7 +24,9 @@ path on one GPU (a one-rank NCCL group).
 After the ladder, the full doubles-residual iteration (O=60, V=480, tiles U{20..64},
 seed 2; one CUDA graph per mode) is timed in FP64, autotuned split-INT8 and BF16x3 and
 reported under "ccsd_iteration" with a sampled reference-CPU baseline (--no-ccsd skips
-it).
+it); on one GPU the energy gradient (O=30, V=240) and sampled steps of the streamed
+triples energy (O=50, V=500) follow under "adjoint" and "triples" (--no-adjoint,
+--no-triples skip them).
 """
 from __future__ import annotations
 
@@ -74,8 +76,12 @@ def parse():
     p.add_argument("--ccsd-oa", type=int, default=30)
     p.add_argument("--ccsd-va", type=int, default=240)
     p.add_argument("--shard", action="store_true", help="owner-computes path with an all-reduce even at N=1")
-    p.add_argument("--adjoint", action="store_true", help="also time the energy gradient (O=30, V=240)")
-    p.add_argument("--triples", action="store_true", help="also time sampled triples-energy steps (O=50, V=500)")
+    p.add_argument("--adjoint", action="store_true",
+                   help="time the energy gradient (O=30, V=240) also with several ranks (default: one rank only)")
+    p.add_argument("--triples", action="store_true",
+                   help="time sampled triples-energy steps (O=50, V=500) also with several ranks (default: one rank only)")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the energy-gradient measurement")
+    p.add_argument("--no-triples", action="store_true", help="skip the triples-energy measurement")
     p.add_argument("--triples-steps", type=int, default=4)
     p.add_argument("--pool-gib", type=float, default=150.0,
                    help="device arena of the ladder workloads (small cases: a few GiB)")
@@ -311,6 +317,7 @@ def measure_triples(ec, torch, nsteps):
     rng = np.random.default_rng(9)
     sample = [allsteps[int(x)] for x in rng.choice(len(allsteps), size=nsteps, replace=False)]
     out, es = {"workload": "triples_energy_O50_V500_tile40", "sampled_steps": sample, "steps_total": len(allsteps)}, {}
+    out["digit_cache_bytes_before"] = ec.digit_cache_info()[0]
     ec.set_digit_cache(int(24 * 2 ** 30))
     for name, mode in (("fp64", tb.Precision.FP64), ("int8", tb.Precision.INT8)):
         ec.set_precision(mode, 1e-11)
@@ -318,7 +325,8 @@ def measure_triples(ec, torch, nsteps):
         T3.energy(P, sample[:1], sch)  # warm-up
         e, fl, ms = T3.energy(P, sample, sch)
         es[name] = e
-        out[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9}
+        out[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9,
+                     "digit_cache_bytes": ec.digit_cache_info()[0]}
     ec.set_precision(tb.Precision.FP64)
     ec.set_digit_cache(0)
     out["speedup_int8_vs_fp64"] = out["fp64"]["ms"] / out["int8"]["ms"]
@@ -608,20 +616,10 @@ def main():
             m["tflops_graph"] = world * P.flops["contractions"] / m["graph_ms"] / 1e9
         for m in ("int8", "bf16x3"):
             res[m]["speedup_vs_fp64"] = res["fp64"]["graph_ms"] / res[m]["graph_ms"]
-        cpu3 = None
-        if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            # the reference's block_multiply on a fixed-seed sample of the iteration's
-            # particle-ladder triples (its largest contraction), extrapolated
-            cpu3 = cpu_baseline_sample(ladder_triples(args.ccsd_oa, args.ccsd_va, 2, 20, 64), args.cpu_seconds / 2,
-                                       os.cpu_count() or 1,
-                                       f"the O={2 * args.ccsd_oa}/V={2 * args.ccsd_va} particle ladder "
-                                       f"(tiles U{{20..64}}, seed 2)")
-            cpu3["iteration_s_extrapolated"] = P.flops["contractions"] / (cpu3["value"] * 1e12)
-            cpu3["speedup_int8_graph_vs_cpu"] = cpu3["iteration_s_extrapolated"] / (res["int8"]["graph_ms"] * 1e-3)
         ccsd_line = {"workload": f"ccsd_doubles_iteration_O{2 * args.ccsd_oa}_V{2 * args.ccsd_va}",
                      "unit": "TFLOP/s (admitted FP64 FLOPs of the iteration's contractions / graph replay time)",
                      "flops": P.flops, "ops_per_iteration": len(CC._ops(P)) + 3,
-                     "ladder_batches": P.ladder_batches, **res, "cpu_baseline": cpu3}
+                     "ladder_batches": P.ladder_batches, **res, "cpu_baseline": None}
         for t in P.T.values():  # the iteration's arena memory goes back before the next workload
             if getattr(t, "ec", None) is not None:
                 t.set_read_only(False)
@@ -629,15 +627,32 @@ def main():
         del P
         import gc
         gc.collect()
-    adjoint_line = measure_adjoint(ec, torch) if args.adjoint else None
-    triples_line = measure_triples(ec, torch, args.triples_steps) if args.triples else None
+    # configs 4 and 5 beside the ladder on one GPU (several ranks: only when asked for;
+    # the triples problem stages 5 GB of dense amplitudes on the host per rank)
+    do_adjoint = not args.no_adjoint and (world == 1 or args.adjoint)
+    do_triples = not args.no_triples and (world == 1 or args.triples)
+    adjoint_line = measure_adjoint(ec, torch) if do_adjoint else None
+    triples_line = measure_triples(ec, torch, args.triples_steps) if do_triples else None
     if world > 1:
         dist.barrier()
     if rank == 0:
+        # the reference's CPU path, after every GPU measurement (its BLAS threads on all
+        # host cores would otherwise slow the host side of the GPU runs that follow)
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             cpu = cpu_baseline_sample(ladder_triples(args.oa, args.va, args.seed), args.cpu_seconds,
                                       os.cpu_count() or 1)
+            if ccsd_line is not None:
+                # the reference's block_multiply on a fixed-seed sample of the iteration's
+                # particle-ladder triples (its largest contraction), extrapolated
+                cpu3 = cpu_baseline_sample(ladder_triples(args.ccsd_oa, args.ccsd_va, 2, 20, 64),
+                                           args.cpu_seconds / 2, os.cpu_count() or 1,
+                                           f"the O={2 * args.ccsd_oa}/V={2 * args.ccsd_va} particle ladder "
+                                           f"(tiles U{{20..64}}, seed 2)")
+                cpu3["iteration_s_extrapolated"] = ccsd_line["flops"]["contractions"] / (cpu3["value"] * 1e12)
+                cpu3["speedup_int8_graph_vs_cpu"] = cpu3["iteration_s_extrapolated"] / (
+                    ccsd_line["int8"]["graph_ms"] * 1e-3)
+                ccsd_line["cpu_baseline"] = cpu3
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

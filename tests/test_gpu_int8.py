@@ -25,11 +25,14 @@ INT8_TOL = 1e-11
     (("abij", "abcd", "cdij"), dict(a=1, b=1, c=1, d=1, i=1, j=1)),
     (("abij", "abcd", "cdij"), dict(a=48, b=48, c=48, d=48, i=20, j=20)),
     (("ab", "ak", "kb"), dict(a=300, b=170, k=700)),
-    # both operands with contiguous rows (staged split of A and B): odd K in 4-row
-    # units (K = 1369), odd K in 8-row units, one-element rows
+    # both operands with contiguous rows (staged split of A and B): odd K (K = 1369),
+    # short rows, one-element rows
     (("abij", "abcd", "ijcd"), dict(a=13, b=11, c=37, d=37, i=7, j=5)),
     (("abij", "abcd", "ijcd"), dict(a=9, b=17, c=5, d=7, i=6, j=3)),
     (("abij", "abcd", "ijcd"), dict(a=19, b=3, c=1, d=1, i=5, j=9)),
+    # long contiguous rows: K = 4209 (one warp group's two stages fill shared memory),
+    # a ragged last element and rows of padding in the last tile
+    (("abij", "abcd", "ijcd"), dict(a=11, b=13, c=61, d=69, i=3, j=7)),
 ])
 def test_int8_block_multiply(labels, shape):
     cl, al, bl = labels
