@@ -341,7 +341,8 @@ def measure_triples(ec, torch, nsteps):
 def run_blockops(args, torch, tb, W, local):
     """The HBM-bound block kernels at the ladder's sizes (r2, t2: O=40, V=360 spin-blocked,
     7.8e7 elements, 0.62 GB each, beyond L2): permuted add r2(a,b,i,j) += X(b,a,j,i)
-    (k_assign_blocks, 24 B/element), flat add r2 += X (k_axpby, 24), dot r2.t2 and norm
+    (k_assign_blocks, 24 B/element; also X(a,b,j,i) and the streamed X(b,a,i,j), the other
+    adds of the P(ab)P(ij) symmetrisation), flat add r2 += X (k_axpby, 24), dot r2.t2 and norm
     (k_dot_partial, 16 and 8), denominator update t2 += r2 / D (k_denom, 24) and an
     in-place map r2 = 2 r2 (k_map_blocks, 16).  Each timed over `steps` launches after
     `warmup` with CUDA events on the context's stream; GB/s of algorithmic bytes."""
@@ -361,6 +362,8 @@ def run_blockops(args, torch, tb, W, local):
     hbm = peaks.get("hbm_gbs")
     cases = {
         "permuted_add k_assign_blocks": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(b, a, j, i)))),
+        "permuted_add_abji k_assign_blocks": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(a, b, j, i)))),
+        "permuted_add_baij k_assign_blocks (streamed rows)": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(b, a, i, j)))),
         "flat_add k_axpby": (24, lambda s: s(lad.r2(a, b, i, j).iadd(X(a, b, i, j)))),
         "dot k_dot_partial": (16, lambda s: s.dot(0, lad.r2(a, b, i, j), lad.t2(a, b, i, j))),
         "norm k_dot_partial": (8, lambda s: s.norm(1, lad.r2(a, b, i, j))),

@@ -325,74 +325,225 @@ int resident_grid(K kernel, int64_t want) {
   return (int) std::max<int64_t>(1, std::min<int64_t>(want, (int64_t) nsm * k));
 }
 
-constexpr int kAsgEdge       = 64;                          // sub-tile edge along q and p
-constexpr int kAsgCap        = kAsgEdge * (kAsgEdge + 1);   // doubles of shared memory per CTA
-constexpr int kAsgMaxSub     = 32;                          // sub-tiles per work unit
-constexpr int kAsgStreamUnit = 8192;                        // elements per streamed work unit
-constexpr int kAsgElems      = 8;                           // elements in flight per thread
+constexpr int kAsgElems  = 8;                           // elements per thread and work unit
+constexpr int kAsgN      = kThreads * kAsgElems;        // elements per work unit at most
+constexpr int kAsgQ      = 64;                          // sub-tile extent along q at most
+constexpr int kAsgP      = 32;                          // sub-tile extent along p at most
+constexpr int kAsgStage  = kAsgQ * (kAsgP + 1);         // doubles of one shared-memory stage
+constexpr int kAsgMaxSub = 32;                          // sub-tiles per work unit at most
+constexpr int kAsgRows   = 256;                         // streamed rows per work unit at most
+
+// Multiplier of x / d for 0 <= x < 2^32 and 2 <= d < 2^32: umul64hi(x, ceil(2^64 / d))
+// (Granlund and Montgomery, division by invariant integers using multiplication: the
+// rounding error x * (m - 2^64 / d) / 2^64 < 2^-32 stays below 1 / d).  0 for d = 1.
+static uint64_t asg_magic64(int64_t d) { return d <= 1 ? 0 : ~uint64_t(0) / (uint64_t) d + 1; }
 
 BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off, int64_t first) {
   BlockAssign b{};
-  b.dst_off = dst_off;
-  b.src_off = src_off;
-  b.nd      = lp.nd;
-  b.total   = 1;
-  b.first   = first;
-  for(int k = 0; k < lp.nd; k++) b.total *= lp.dims[k];
+  b.dst_off    = dst_off;
+  b.src_off    = src_off;
+  b.nd         = lp.nd;
+  b.first      = first;
+  int64_t total = 1;
+  for(int k = 0; k < lp.nd; k++) total *= lp.dims[k];
   int p = -1;
   for(int k = 0; k < lp.nd; k++)
     if(lp.sld[k] == 1 && lp.dims[k] > 1) p = k;
   const int q = lp.nd - 1;
   const bool tiled = lp.nd >= 2 && p >= 0 && p != q && lp.dld[q] == 1 && lp.dims[q] >= 8 && lp.dims[p] >= 8;
-  b.p           = tiled ? p : -1;
-  b.outer_total = 1;
-  for(int k = 0; k < 4; k++) {
-    b.dims[k] = k < lp.nd ? lp.dims[k] : 1;
-    b.dld[k]  = k < lp.nd ? lp.dld[k] : 0;
-    b.sld[k]  = k < lp.nd ? lp.sld[k] : 0;
-    if(tiled && k < lp.nd && k != p && k != q) b.outer_total *= lp.dims[k];
-  }
+  b.p   = tiled ? p : -1;
+  b.upr = 1;
+  b.nbq = b.nbp = 1;
+  b.per_unit    = 1;
+  b.tq = b.tp   = 1;
   int64_t units = 0;
-  if(b.total == 0) b.per_unit = 1;
-  else if(tiled) {
-    // offsets within a transposed block pair are 32-bit
+  if(total > 0) {
+    // counts, strides and offsets within one block pair are 32-bit
     int64_t ssize = 1, dsize = 1;
     for(int k = 0; k < lp.nd; k++) {
       ssize += (lp.dims[k] - 1) * lp.sld[k];
       dsize += (lp.dims[k] - 1) * lp.dld[k];
     }
-    TB_EXPECTS(ssize < (int64_t(1) << 31) && dsize < (int64_t(1) << 31), "block too large");
-    const int64_t tq = std::min<int64_t>(b.dims[q], kAsgEdge), tp = std::min<int64_t>(b.dims[p], kAsgEdge);
-    const int64_t ntiles = b.outer_total * ((b.dims[q] + tq - 1) / tq) * ((b.dims[p] + tp - 1) / tp);
-    b.per_unit = (int) std::max<int64_t>(1, std::min<int64_t>(kAsgMaxSub, kAsgCap / (tq * (tp | 1))));
-    units      = (ntiles + b.per_unit - 1) / b.per_unit;
-  }
-  else {
-    b.per_unit = kAsgStreamUnit;
-    units      = (b.total + kAsgStreamUnit - 1) / kAsgStreamUnit;
+    TB_EXPECTS(ssize < (int64_t(1) << 31) && dsize < (int64_t(1) << 31) && total < (int64_t(1) << 31),
+               "block too large");
+    for(int k = 0; k < 4; k++) {
+      b.dims[k] = (int32_t) (k < lp.nd ? lp.dims[k] : 1);
+      b.dld[k]  = (int32_t) (k < lp.nd ? lp.dld[k] : 0);
+      b.sld[k]  = (int32_t) (k < lp.nd ? lp.sld[k] : 0);
+      b.mag[k]  = asg_magic64(b.dims[k]);
+    }
+    if(tiled) { // sub-tiles of nearly equal extents: a ragged block costs few idle lanes
+      int64_t outer = 1;
+      for(int k = 0; k < lp.nd; k++)
+        if(k != p && k != q) outer *= lp.dims[k];
+      const int64_t nbq = (lp.dims[q] + kAsgQ - 1) / kAsgQ, nbp = (lp.dims[p] + kAsgP - 1) / kAsgP;
+      const int64_t tq = (lp.dims[q] + nbq - 1) / nbq, tp = (lp.dims[p] + nbp - 1) / nbp;
+      b.nbq      = (int32_t) nbq;
+      b.nbp      = (int32_t) nbp;
+      b.tq       = (int32_t) tq;
+      b.tp       = (int32_t) tp;
+      b.nsub     = (int32_t) (outer * nbq * nbp);
+      b.per_unit = (int32_t) std::max<int64_t>(
+          1, std::min<int64_t>({(int64_t) kAsgMaxSub, kAsgN / (tq * tp), kAsgStage / (tq * (tp | 1))}));
+      units = (b.nsub + b.per_unit - 1) / b.per_unit;
+    }
+    else { // rows of the destination's last mode (one row of length 1 for a scalar block)
+      const int64_t len = lp.nd > 0 ? lp.dims[q] : 1;
+      b.tq              = (int32_t) len;
+      b.nsub            = (int32_t) (total / len);
+      if(len <= kAsgN) {
+        b.per_unit = (int32_t) std::min<int64_t>(kAsgRows, kAsgN / len);
+        units      = (b.nsub + b.per_unit - 1) / b.per_unit;
+      }
+      else {
+        b.upr = (int32_t) ((len + kAsgN - 1) / kAsgN);
+        units = (int64_t) b.nsub * b.upr;
+      }
+    }
+    b.mag[4] = asg_magic64(b.nbq);
+    b.mag[5] = asg_magic64(b.nbp);
   }
   TB_EXPECTS(units < (int64_t(1) << 31), "block pair too large");
-  b.units = (int) units;
+  b.units = (int32_t) units;
   return b;
 }
 
+namespace {
+
+// x / d for 0 <= x < 2^11 and 1 <= d <= 2^20, with m = asg_magic(d): umulhi(x, ceil(2^32 / d))
+// (Granlund and Montgomery; the rounding error x * (m - 2^32 / d) / 2^32 < 2^-21 stays
+// below 1 / d).  d = 1 has no 32-bit multiplier and returns x.
+__device__ __forceinline__ unsigned asg_magic(unsigned d) { return d == 1 ? 0u : 0xFFFFFFFFu / d + 1; }
+__device__ __forceinline__ int asg_div(int x, unsigned m) { return m == 0 ? x : (int) __umulhi((unsigned) x, m); }
+// x / d for 0 <= x < 2^31 with the host's 64-bit multiplier (asg_magic64)
+__device__ __forceinline__ int asg_div64(int x, uint64_t m) {
+  return m == 0 ? x : (int) __umul64hi((uint64_t) (uint32_t) x, m);
+}
+
+__device__ __forceinline__ void asg_cp8(uint32_t saddr, const double* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void asg_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void asg_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Per-unit records, kept in one slot of a three-slot ring: origins (source and
+// destination offsets within the pair's blocks) and extents (nq | np << 16) of a
+// transposed unit's sub-tiles, or the row origins of a streamed unit.
+struct AsgRing {
+  int so[3][kAsgRows];
+  int dof[3][kAsgRows];
+  int ext[3][kAsgMaxSub];
+};
+
+// Elements of unit lu of pair a: sub-tiles x tq x tp, rows x row length, or one chunk of a long row.
+__device__ __forceinline__ int asg_unit_elems(const BlockAssign& a, int lu) {
+  if(a.p >= 0) return min(a.per_unit, a.nsub - lu * a.per_unit) * a.tq * a.tp;
+  if(a.upr == 1) return min(a.per_unit, a.nsub - lu * a.per_unit) * a.tq;
+  const int c = lu % a.upr;
+  return min(kAsgN, a.tq - c * kAsgN);
+}
+
+// Records of unit lu of pair a into ring slot s (threads below the unit's record count).
+__device__ __forceinline__ void asg_records(const BlockAssign& a, int lu, AsgRing& r, int s) {
+  const int t = threadIdx.x;
+  if(a.p >= 0) {
+    const int q = a.nd - 1, p = a.p, t0 = lu * a.per_unit;
+    if(t < a.per_unit && t0 + t < a.nsub) {
+      int       x  = t0 + t;
+      int       y  = asg_div64(x, a.mag[4]);
+      const int bq = x - y * a.nbq;
+      x            = asg_div64(y, a.mag[5]);
+      const int bp = y - x * a.nbp;
+      int       so = 0, doff = 0;
+      for(int k = a.nd - 1; k >= 0; k--) {
+        if(k == q || k == p) continue;
+        const int z = asg_div64(x, a.mag[k]), i = x - z * a.dims[k];
+        x           = z;
+        so += i * a.sld[k];
+        doff += i * a.dld[k];
+      }
+      const int q0 = bq * a.tq, p0 = bp * a.tp;
+      r.so[s][t]   = so + q0 * a.sld[q] + p0;
+      r.dof[s][t]  = doff + q0 + p0 * a.dld[p];
+      r.ext[s][t]  = min(a.tq, a.dims[q] - q0) | (min(a.tp, a.dims[p] - p0) << 16);
+    }
+    return;
+  }
+  const int r0 = a.upr == 1 ? lu * a.per_unit : lu / a.upr;
+  const int nr = a.upr == 1 ? min(a.per_unit, a.nsub - r0) : 1;
+  if(t < nr) {
+    int x = r0 + t, so = 0, doff = 0;
+    for(int k = a.nd - 2; k >= 0; k--) {
+      const int z = asg_div64(x, a.mag[k]), i = x - z * a.dims[k];
+      x           = z;
+      so += i * a.sld[k];
+      doff += i * a.dld[k];
+    }
+    r.so[s][t]  = so;
+    r.dof[s][t] = doff;
+  }
+}
+
+// Issue the source loads of unit lu of pair a into a shared-memory stage (8-byte
+// cp.async per element, this thread's elements only): a transposed unit's sub-tiles
+// row by row along p (odd row pitch), a streamed unit in element order.
+__device__ __forceinline__ void asg_load(const BlockAssign& a, int lu, const AsgRing& r, int s,
+                                         const double* __restrict__ src, uint32_t stage) {
+  const double* s0 = src + a.src_off;
+  const int     n  = asg_unit_elems(a, lu);
+  if(a.p >= 0) {
+    const int      TQ = a.tq, TP = a.tp, pitch = TP | 1, sq = a.sld[a.nd - 1];
+    const unsigned mq = asg_magic(TQ), mp = asg_magic(TP);
+#pragma unroll
+    for(int j = 0; j < kAsgElems; j++) {
+      const int e = threadIdx.x + j * kThreads;
+      if(e < n) {
+        const int row = asg_div(e, mp), ip = e - row * TP;
+        const int k = asg_div(row, mq), iq = row - k * TQ;
+        const int ext = r.ext[s][k];
+        if(iq < (ext & 0xFFFF) && ip < (ext >> 16))
+          asg_cp8(stage + (uint32_t) (row * pitch + ip) * 8u, s0 + r.so[s][k] + iq * sq + ip);
+      }
+    }
+    return;
+  }
+  const int      L  = a.tq;
+  const int      sq = a.nd > 0 ? a.sld[a.nd - 1] : 0;
+  const unsigned mL = asg_magic(L);
+  const int      c0 = a.upr == 1 ? 0 : (lu % a.upr) * kAsgN;
+#pragma unroll
+  for(int j = 0; j < kAsgElems; j++) {
+    const int e = threadIdx.x + j * kThreads;
+    if(e < n) {
+      const int row = a.upr == 1 ? asg_div(e, mL) : 0, col = c0 + e - row * L;
+      asg_cp8(stage + (uint32_t) e * 8u, s0 + r.so[s][row] + col * sq);
+    }
+  }
+}
+
+} // namespace
+
 // The block pairs of an AddOp in one launch.  Work units (a batch of sub-tiles of one
-// pair's transposed (q, p) plane, or a run of a streamed pair's elements) are split
-// into equal contiguous ranges, one per CTA.  A transposing unit loads its sub-tiles
-// along the source's stride-1 mode p into shared memory (odd row pitch),
-// then writes them row by row along the destination's stride-1 mode q.  Threads walk
-// the unit's elements in flat order (kAsgElems loads in flight each), and sub-tiles
-// have the exact extents of the blocks (at most 64 x 64), so no lanes are spent on
-// padding for small tiles.
-__global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__ dst, double scale,
-                                                            const double* __restrict__ src,
-                                                            const BlockAssign* __restrict__ blocks, int nblocks,
-                                                            int64_t nunits, int is_assign) {
-  __shared__ double  tile[kAsgCap];
-  __shared__ int     s_so[kAsgMaxSub], s_do[kAsgMaxSub]; // sub-tile origins within the blocks
-  __shared__ int     s_nq[kAsgMaxSub], s_np[kAsgMaxSub];
-  __shared__ int     s_pair;
-  const int64_t u0 = nunits * blockIdx.x / gridDim.x, u1 = nunits * (blockIdx.x + 1) / gridDim.x;
+// pair's transposed (q, p) plane, or rows of a streamed pair) are split into equal
+// contiguous ranges, one per CTA.  Each CTA runs its units through a two-stage
+// pipeline: while unit u is written, unit u+1's source elements are already on their
+// way into the other shared-memory stage (cp.async) and unit u+2's records are
+// computed; unit u's old destination values are loaded before the wait for its
+// source, so both reads of a unit overlap.  A transposing unit lands its sub-tiles
+// along the source's stride-1 mode p (odd row pitch) and is written row by row along
+// the destination's stride-1 mode q; a streamed unit is written in element order.
+// Sub-tiles have the blocks' own extents (at most 64 x 32, nearly equal), so few
+// lanes go to padding.  All index arithmetic is 32-bit, divisions by the blocks'
+// extents multiply by constants the host computed.
+__global__ void __launch_bounds__(kThreads, 4) k_assign_blocks(double* __restrict__ dst, double scale,
+                                                               const double* __restrict__ src,
+                                                               const BlockAssign* __restrict__ blocks, int nblocks,
+                                                               int nunits, int is_assign) {
+  __shared__ __align__(16) double tile[2][kAsgStage];
+  __shared__ AsgRing              ring;
+  __shared__ int                  s_pair;
+  const int u0 = (int) ((int64_t) nunits * blockIdx.x / gridDim.x);
+  const int u1 = (int) ((int64_t) nunits * (blockIdx.x + 1) / gridDim.x);
   if(u0 >= u1) return;
   if(threadIdx.x == 0) { // the pair holding unit u0: last pair with first <= u0
     int lo = 0, hi = nblocks - 1;
@@ -404,127 +555,96 @@ __global__ void __launch_bounds__(kThreads) k_assign_blocks(double* __restrict__
     s_pair = lo;
   }
   __syncthreads();
-  int pi = s_pair;
-  for(int64_t u = u0; u < u1; u++) {
+  const uint32_t st0 = (uint32_t) __cvta_generic_to_shared(&tile[0][0]);
+  const uint32_t st1 = (uint32_t) __cvta_generic_to_shared(&tile[1][0]);
+  auto pair_of = [&](int pi, int u) {
     while(u >= blocks[pi].first + blocks[pi].units) pi++;
+    return pi;
+  };
+  int pi = pair_of(s_pair, u0);
+  asg_records(blocks[pi], u0 - (int) blocks[pi].first, ring, 0);
+  __syncthreads();
+  asg_load(blocks[pi], u0 - (int) blocks[pi].first, ring, 0, src, st0);
+  asg_commit();
+  int pn = pi; // pair of unit u + 1
+  if(u0 + 1 < u1) {
+    pn = pair_of(pi, u0 + 1);
+    asg_records(blocks[pn], u0 + 1 - (int) blocks[pn].first, ring, 1);
+  }
+  __syncthreads();
+  int slot = 0, stage = 0;
+  for(int u = u0; u < u1; u++) {
+    const int sn = slot == 2 ? 0 : slot + 1, sn2 = sn == 2 ? 0 : sn + 1;
+    if(u + 1 < u1) asg_load(blocks[pn], u + 1 - (int) blocks[pn].first, ring, sn, src, stage ? st0 : st1);
+    asg_commit();
+    const int pn2 = u + 2 < u1 ? pair_of(pn, u + 2) : pn;
+    if(u + 2 < u1) asg_records(blocks[pn2], u + 2 - (int) blocks[pn2].first, ring, sn2);
     const BlockAssign& a  = blocks[pi];
+    const int          lu = u - (int) a.first;
+    const int          n  = asg_unit_elems(a, lu);
     double* const      d0 = dst + a.dst_off;
-    const double*      s0 = src + a.src_off;
-    const int64_t      lu = u - a.first;
+    double             old[kAsgElems];
+    int                out[kAsgElems], at[kAsgElems]; // destination offset (-1: none), stage slot
     if(a.p >= 0) {
-      const int     q = a.nd - 1, p = a.p;
-      const int64_t Dq = a.dims[q], Dp = a.dims[p];
-      const int     TQ = (int) min(Dq, (int64_t) kAsgEdge), TP = (int) min(Dp, (int64_t) kAsgEdge);
-      const int     pitch = TP | 1;
-      const int64_t nbq = (Dq + TQ - 1) / TQ, nbp = (Dp + TP - 1) / TP;
-      const int64_t ntiles = a.outer_total * nbq * nbp;
-      const int64_t t0 = lu * a.per_unit;
-      const int     nt = (int) min((int64_t) a.per_unit, ntiles - t0);
-      const int     sq = (int) a.sld[q], dp = (int) a.dld[p];
-      if(threadIdx.x < nt) { // origin and extents of each sub-tile of the unit
-        int64_t       x  = t0 + threadIdx.x;
-        const int64_t bq = x % nbq;
-        x /= nbq;
-        const int64_t bp = x % nbp;
-        x /= nbp;
-        int64_t so = 0, doff = 0;
-        for(int k = a.nd - 1; k >= 0; k--) {
-          if(k == q || k == p) continue;
-          const int64_t dk = a.dims[k];
-          const int64_t i  = x % dk;
-          x /= dk;
-          so += i * a.sld[k];
-          doff += i * a.dld[k];
-        }
-        const int64_t q0 = bq * TQ, p0 = bp * TP;
-        s_so[threadIdx.x] = (int) (so + q0 * sq + p0);
-        s_do[threadIdx.x] = (int) (doff + q0 + p0 * dp);
-        s_nq[threadIdx.x] = (int) min((int64_t) TQ, Dq - q0);
-        s_np[threadIdx.x] = (int) min((int64_t) TP, Dp - p0);
-      }
-      __syncthreads();
-      // flat element order within the unit: (sub-tile, q row, p column) on the way in,
-      // (sub-tile, p row, q column) on the way out; x / d for x < 2^16 and 8 <= d <= 64
-      // as umulhi(x, ceil(2^32 / d)) (Granlund and Montgomery, division by invariant
-      // integers using multiplication)
-      const unsigned mq = 0xFFFFFFFFu / TQ + 1, mp = 0xFFFFFFFFu / TP + 1;
-      const int      n  = nt * TQ * TP;
-      for(int e0 = threadIdx.x; e0 < n; e0 += kThreads * kAsgElems) {
-        double v[kAsgElems];
+      const int      TQ = a.tq, TP = a.tp, pitch = TP | 1, dp = a.dld[a.p];
+      const unsigned mq = asg_magic(TQ), mp = asg_magic(TP);
 #pragma unroll
-        for(int j = 0; j < kAsgElems; j++) {
-          const int e = e0 + j * kThreads;
-          v[j]        = 0.0;
-          if(e < n) {
-            const int row = (int) __umulhi((unsigned) e, mp), ip = e - row * TP;
-            const int k = (int) __umulhi((unsigned) row, mq), iq = row - k * TQ;
-            if(iq < s_nq[k] && ip < s_np[k]) v[j] = __ldg(s0 + s_so[k] + iq * sq + ip);
-          }
-        }
-#pragma unroll
-        for(int j = 0; j < kAsgElems; j++) {
-          const int e = e0 + j * kThreads;
-          if(e < n) {
-            const int row = (int) __umulhi((unsigned) e, mp), ip = e - row * TP;
-            tile[row * pitch + ip] = v[j];
+      for(int j = 0; j < kAsgElems; j++) {
+        const int e = threadIdx.x + j * kThreads;
+        out[j]      = -1;
+        at[j]       = 0;
+        if(e < n) {
+          const int row = asg_div(e, mq), iq = e - row * TQ;
+          const int k = asg_div(row, mp), ip = row - k * TP;
+          const int ext = ring.ext[slot][k];
+          if(iq < (ext & 0xFFFF) && ip < (ext >> 16)) {
+            out[j] = ring.dof[slot][k] + ip * dp + iq;
+            at[j]  = (k * TQ + iq) * pitch + ip;
           }
         }
       }
-      __syncthreads();
-      for(int e0 = threadIdx.x; e0 < n; e0 += kThreads * kAsgElems) {
-        double old[kAsgElems];
-        int    out[kAsgElems], at[kAsgElems]; // offset in the destination block (-1: none), in tile
-#pragma unroll
-        for(int j = 0; j < kAsgElems; j++) {
-          const int e = e0 + j * kThreads;
-          old[j]      = 0.0;
-          out[j]      = -1;
-          at[j]       = 0;
-          if(e < n) {
-            const int row = (int) __umulhi((unsigned) e, mq), iq = e - row * TQ;
-            const int k = (int) __umulhi((unsigned) row, mp), ip = row - k * TP;
-            if(iq < s_nq[k] && ip < s_np[k]) {
-              out[j] = s_do[k] + ip * dp + iq;
-              at[j]  = (k * TQ + iq) * pitch + ip;
-              if(!is_assign) old[j] = d0[out[j]];
-            }
-          }
-        }
-#pragma unroll
-        for(int j = 0; j < kAsgElems; j++) // product rounded before the add, as in a plain loop
-          if(out[j] >= 0) {
-            const double v = __dmul_rn(scale, tile[at[j]]);
-            d0[out[j]]     = is_assign ? v : old[j] + v;
-          }
-      }
-      __syncthreads();
     }
     else {
-      const int64_t beg = lu * a.per_unit, end = min(a.total, beg + a.per_unit);
-      for(int64_t lin = beg + threadIdx.x; lin < end; lin += kThreads) {
-        int64_t x = lin, so = 0, doff = 0;
+      const int      L  = a.tq;
+      const int      dq = a.nd > 0 ? a.dld[a.nd - 1] : 0;
+      const unsigned mL = asg_magic(L);
+      const int      c0 = a.upr == 1 ? 0 : (lu % a.upr) * kAsgN;
 #pragma unroll
-        for(int k = 3; k >= 0; k--) {
-          if(k >= a.nd) continue;
-          const int64_t dk = a.dims[k];
-          const int64_t qk = x / dk;
-          const int64_t i  = x - qk * dk;
-          so += i * a.sld[k];
-          doff += i * a.dld[k];
-          x = qk;
+      for(int j = 0; j < kAsgElems; j++) {
+        const int e = threadIdx.x + j * kThreads;
+        out[j]      = -1;
+        at[j]       = e;
+        if(e < n) {
+          const int row = a.upr == 1 ? asg_div(e, mL) : 0, col = c0 + e - row * L;
+          out[j]        = ring.dof[slot][row] + col * dq;
         }
-        const double v = __dmul_rn(scale, __ldg(s0 + so));
-        d0[doff]       = is_assign ? v : d0[doff] + v;
       }
     }
+#pragma unroll
+    for(int j = 0; j < kAsgElems; j++) old[j] = (!is_assign && out[j] >= 0) ? d0[out[j]] : 0.0;
+    asg_wait_prev(); // this thread's copies of unit u have landed
+    __syncthreads(); // and every other thread's
+    const double* t = tile[stage];
+#pragma unroll
+    for(int j = 0; j < kAsgElems; j++) // product rounded before the add, as in a plain loop
+      if(out[j] >= 0) {
+        const double v = __dmul_rn(scale, t[at[j]]);
+        d0[out[j]]     = is_assign ? v : old[j] + v;
+      }
+    __syncthreads(); // stage and slot free for units u + 2 and u + 3
+    pi    = pn;
+    pn    = pn2;
+    slot  = sn;
+    stage ^= 1;
   }
 }
 
 void launch_assign_blocks(double* dst, double scale, const double* src, const BlockAssign* blocks, int nblocks,
                           int64_t nunits, int is_assign, cudaStream_t stream) {
   if(nblocks <= 0 || nunits <= 0) return;
+  TB_EXPECTS(nunits < (int64_t(1) << 31), "too many work units in one add");
   k_assign_blocks<<<resident_grid(k_assign_blocks, nunits), kThreads, 0, stream>>>(dst, scale, src, blocks, nblocks,
-                                                                                     nunits, is_assign);
+                                                                                     (int) nunits, is_assign);
   TB_CUDA(cudaGetLastError());
 }
 
@@ -739,20 +859,6 @@ double reduce_dot(const double* x, const double* y, int64_t n, cudaStream_t stre
   return h;
 }
 
-// 1/D by Newton-Raphson refinement of the hardware approximation rcp.approx.ftz.f64:
-// each step x <- x + x (1 - D x) squares the relative error (quadratic convergence), so
-// two steps take the approximation's error e to e^4, below double rounding; the result
-// is within a unit or two in the last place of the correctly rounded 1/D.  D must be a
-// normal, nonzero double (denormals are flushed to zero).
-__device__ __forceinline__ double recip_nr(double D) {
-  double x;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(D));
-  double e = fma(-D, x, 1.0);
-  x        = fma(x, e, x);
-  e        = fma(-D, x, 1.0);
-  return fma(x, e, x);
-}
-
 // Orbital-energy denominators over the admitted blocks of a tensor: for element
 // (x_0, ..., x_last) of a block, D = sum_m s_m * eps[first_m + x_m].  The work is
 // cut into units of consecutive rows of one block (a row: all modes but the last;
@@ -919,6 +1025,13 @@ void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks
     k_denom<true><<<grid, kThreads, 0, stream>>>(const_cast<double*>(w), nullptr, 0.0, blocks, units, nunits, nmodes,
                                                  eps, signs, part);
   k_denom_energy_final<<<1, 1024, 0, stream>>>(part, grid, scale, out);
+  TB_CUDA(cudaGetLastError());
+}
+
+void launch_energy_final(const double* part, int64_t np, double scale, double* out, cudaStream_t stream) {
+  if(np <= 0) return;
+  TB_EXPECTS(np < (int64_t(1) << 31), "too many partial sums");
+  k_denom_energy_final<<<1, 1024, 0, stream>>>(part, (int) np, scale, out);
   TB_CUDA(cudaGetLastError());
 }
 

@@ -100,6 +100,46 @@ struct WorkList {
 class Arena;
 struct Tensor;
 
+// Energy epilogue of a contraction (tb_sched_mult_energy): instead of C (+)= alpha * A * B
+// the kernels add sum (C + alpha * A * B)^2 / D over the elements of the output groups
+// with tasks and leave C unchanged; D = sum_m sg[m] * eps[estart[group * nc + m] + x_m]
+// is the orbital-energy denominator of element (x_0, ..., x_(nc-1)) of the group's
+// block.  Each warp of a tile writes one partial sum into `part` (tile index x warps).
+struct EnergyArgs {
+  const double*  eps    = nullptr;
+  const int32_t* estart = nullptr;
+  double*        part   = nullptr;
+  double         sg[kMaxModes] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+#ifdef __CUDACC__
+// 1 / D for a normal, nonzero double: two Newton-Raphson steps x' = x + x (1 - D x)
+// from the hardware's approximate reciprocal (rcp.approx.ftz.f64); the denominator
+// kernels and the energy epilogues share it, so their sums see the same 1 / D.
+__device__ __forceinline__ double recip_nr(double D) {
+  double x;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(D));
+  double e = fma(-D, x, 1.0);
+  x        = fma(x, e, x);
+  e        = fma(-D, x, 1.0);
+  return fma(x, e, x);
+}
+
+// The part of D over `n` modes of a C block: x decomposed over dims[0..n) (last
+// fastest), sum_j sg[cm[j]] * eps[start[cm[j]] + x_j].
+__device__ __forceinline__ double energy_part(int32_t x, int n, const int32_t* dims, const int8_t* cm,
+                                              const EnergyArgs& en, const int32_t* start) {
+  double d = 0.0;
+  for(int j = n - 1; j >= 0; j--) {
+    const int32_t q = x / dims[j];
+    const int     c = cm[j];
+    d += en.sg[c] * __ldg(en.eps + start[c] + (x - q * dims[j]));
+    x = q;
+  }
+  return d;
+}
+#endif
+
 // Scratch of a captured CUDA graph: buffers stay allocated for the graph's lifetime;
 // ops of the graph run in stream order, so a buffer returned by one op can serve the
 // next.  The graph holds the largest scratch of one op, not the sum.
@@ -129,6 +169,11 @@ struct Plan {
   // belongs to exactly one output tile); blocks of groups without tasks are left
   // untouched
   bool         store        = false;
+  // energy epilogue (EnergyArgs): *energy_out += energy_scale * the kernels' partial
+  // sums; null for a plain contraction
+  const EnergyArgs* energy       = nullptr;
+  double*           energy_out   = nullptr;
+  double            energy_scale = 1.0;
   // read-only operands whose split digits may be kept (tb_ctx_set_digit_cache), and the
   // context's cache account
   const Tensor* cache_a = nullptr;
@@ -164,16 +209,24 @@ void launch_assign(const AssignLoop& lp, double* dst, double scale, const double
                    int is_assign, cudaStream_t stream);
 // One block pair of a permuted AddOp: offsets and the loop of plan_assign, with the
 // position of the source's stride-1 loop mode when the pair goes through the
-// shared-memory transpose (-1: streamed).  The pair's work is cut into `units` work
-// units (`per_unit` sub-tiles of at most 64x64 of the transposed plane, or `per_unit`
-// elements when streamed), numbered from `first` across the launch.
+// shared-memory transpose (-1: streamed by rows of the destination's last mode).  The
+// pair's work is cut into `units` work units of at most 2048 elements, numbered from
+// `first` across the launch: `per_unit` sub-tiles of tq x tp (q: the destination's
+// last mode, tq <= 64; p: the source's stride-1 mode, tp <= 32) of the transposed
+// plane, or `per_unit` rows of tq elements when streamed (`upr` > 1: a row longer
+// than a unit, cut into upr units).
+// Counts, strides and offsets within one pair are below 2^31; `mag` holds the 64-bit
+// multipliers of the divisions the kernel makes (x / d = umul64hi(x, mag) for d >= 2).
 struct BlockAssign {
-  int64_t dst_off, src_off;
-  int32_t nd, p;
-  int64_t dims[4], dld[4], sld[4];
-  int64_t outer_total, total;
-  int64_t first;
-  int32_t units, per_unit;
+  int64_t  dst_off, src_off;
+  int64_t  first;
+  int32_t  nd, p;
+  int32_t  dims[4], dld[4], sld[4];
+  int32_t  units, per_unit;
+  int32_t  tq, tp, upr;
+  int32_t  nsub;     // sub-tiles (transposed) or rows (streamed) of the pair
+  int32_t  nbq, nbp; // sub-tiles along q and p
+  uint64_t mag[6];   // multipliers for dims[0..3], nbq, nbp (0: divisor 1)
 };
 // `first` is the number of work units of the pairs before this one in the launch.
 BlockAssign make_block_assign(const AssignLoop& lp, int64_t dst_off, int64_t src_off, int64_t first);
@@ -227,6 +280,8 @@ void launch_denom_energy(const double* w, double scale, const DenomBlock* blocks
                          int nunits, int nmodes, const double* eps, DenomSigns signs, double* part, double* out,
                          cudaStream_t stream);
 void launch_set_scalar(double* out, double v, cudaStream_t stream);
+// *out += scale * sum part[0 .. np), summed in a fixed order (deterministic).
+void launch_energy_final(const double* part, int64_t np, double scale, double* out, cudaStream_t stream);
 // nonzero[b] = 1 if x[off_b, off_b + n_b) holds an element other than +0.0 / -0.0, else
 // 0, for the (off, n) pairs of a device array (the launcher clears nonzero first).
 void launch_block_nonzero(const double* x, const int64_t* pairs, int nblocks, uint32_t* nonzero,

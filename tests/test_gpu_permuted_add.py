@@ -4,9 +4,10 @@ TAMM's AddOp runs kernels::block_add / assign per block pair (addop.hpp:230-275,
 kernels/assign.hpp:467-485): dst(labels) (=|+=) alpha * src(permuted labels).  Here
 all block pairs go through one launch; a pair whose destination stride-1 mode is not
 the source's goes through the shared-memory transpose in sub-tiles of at most
-64 x 64 (ragged when a tile is larger), a pair with a mode below 8 or the same
-stride-1 mode streams.  The product is rounded before the add, so the result equals
-numpy's R + alpha * X bit for bit.
+64 x 32 (nearly equal extents when a tile is larger), a pair with a mode below 8 or
+the same stride-1 mode streams by rows of the destination's last mode (a row longer
+than one 2048-element work unit is cut into several).  The product is rounded before
+the add, so the result equals numpy's R + alpha * X bit for bit.
 """
 import numpy as np
 import pytest
@@ -51,6 +52,8 @@ CASES = [
     ([20, 24, 30], [20, 12], "abij", "baij"),   # same stride-1 mode: streamed
     ([100, 70], [66, 9], "abi", "iba"),         # planes above 64 x 64: ragged sub-tiles
     ([5, 7, 3], [6, 2], "abij", "baji"),        # tiles below 8: streamed
+    ([2500, 40], [3, 2], "ia", "ai"),           # streamed rows longer than a work unit
+    ([2100, 9], [5, 3], "ija", "jia"),          # long rows and many-row units in one launch
 ]
 
 
