@@ -461,6 +461,14 @@ int tb_sched_denom(tb_sched s, tb_labeled t, double alpha, tb_labeled r, const d
  * (no counterpart in TAMM's ops).  tb_sched_set_scalar queues slot = value. */
 int tb_sched_denom_energy(tb_sched s, int slot, double alpha, tb_labeled w, const double* eps, int64_t neps,
                           const double* signs);
+/* slot += scale * sum (lhs + alpha * a * b)^2 / D over the elements of the output
+ * blocks the contraction addresses, D as in tb_sched_denom, lhs left unchanged: the
+ * MultOp lhs += alpha * a * b (multop.hpp:576-893) with tb_sched_denom_energy fused
+ * into the contraction's epilogue, so the summed tensor is read once and never
+ * written (no counterpart in TAMM's ops).  Blocks without contributions enter with
+ * their stored values.  Lambda operands are not supported (TB_ERR_NOT_IMPLEMENTED). */
+int tb_sched_mult_energy(tb_sched s, int slot, double scale, tb_labeled lhs, double alpha, tb_labeled a,
+                         tb_labeled b, const double* eps, int64_t neps, const double* signs);
 int tb_sched_set_scalar(tb_sched s, int slot, double value);
 /* Autotuner (no counterpart in TAMM): with enable != 0, the first execution of each
  * contraction under a split-INT8 request times the candidate kernels (FP64; split-

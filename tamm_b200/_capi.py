@@ -148,6 +148,8 @@ PROTOS = {
     "tb_sched_scalars": [h, dp, C.c_int],
     "tb_sched_denom": [h, tb_labeled, C.c_double, tb_labeled, dp, C.c_int64, dp],
     "tb_sched_denom_energy": [h, C.c_int, C.c_double, tb_labeled, dp, C.c_int64, dp],
+    "tb_sched_mult_energy": [h, C.c_int, C.c_double, tb_labeled, C.c_double, tb_labeled, tb_labeled, dp, C.c_int64,
+                             dp],
     "tb_sched_set_scalar": [h, C.c_int, C.c_double],
     "tb_sched_autotune": [h, C.c_int],
     "tb_sched_tune_info": [h, C.c_int64, ip, ip, ip, ip, ip, dp, C.c_int],

@@ -1250,6 +1250,34 @@ int tb_sched_denom_energy(tb_sched s, int slot, double alpha, tb_labeled w, cons
   TB_API_END
 }
 
+int tb_sched_mult_energy(tb_sched s, int slot, double scale, tb_labeled lhs, double alpha, tb_labeled a,
+                         tb_labeled b, const double* eps, int64_t neps, const double* signs) {
+  TB_API_BEGIN
+  REQUIRE_ARG(s != nullptr && eps != nullptr && signs != nullptr && neps >= 0);
+  TB_EXPECTS(slot >= 0 && slot < Sched::kSlots, "scalar slot out of range (0..63)");
+  Op op;
+  op.kind   = Op::Mult;
+  op.energy = true;
+  op.lhs    = to_labeled(lhs);
+  op.a      = to_labeled(a);
+  op.b      = to_labeled(b);
+  op.alpha  = alpha;
+  op.slot   = slot;
+  op.value  = scale;
+  (void) classify(op.lhs.labels.data(), (int) op.lhs.labels.size(), op.a.labels.data(),
+                  (int) op.a.labels.size(), op.b.labels.data(), (int) op.b.labels.size());
+  const Tensor& T = *op.lhs.t;
+  TB_EXPECTS(T.nmodes >= 1, "energy epilogue of a scalar output");
+  for(int m = 1; m < T.nmodes; m++)
+    TB_EXPECTS(T.tis[m]->root->is == T.tis[0]->root->is, "energy epilogue: all output modes over one root index space");
+  auto d = std::make_shared<DenomSpec>();
+  d->eps.assign(eps, eps + neps);
+  for(int m = 0; m < T.nmodes; m++) d->signs[m] = signs[m];
+  op.denom = d;
+  s->p->ops.push_back(op);
+  TB_API_END
+}
+
 int tb_sched_set_scalar(tb_sched s, int slot, double value) {
   TB_API_BEGIN
   REQUIRE_ARG(s != nullptr);

@@ -48,9 +48,14 @@ struct Smem {
   int32_t   colB[2][BN];
   int32_t   rowC[BM];
   int32_t   colC[BN];
+  double    rowD[BM]; // energy epilogue: the rows' and columns' parts of the denominators
+  double    colD[BN];
   TaskInfo  ti[2];
   ChunkDesc desc[NSLOT];
 };
+
+// two CTAs per SM (228 KB of shared memory, 1 KB of it reserved per CTA)
+static_assert(2 * (sizeof(Smem<80>) + 1024) <= 228 * 1024, "two FP64 CTAs per SM");
 
 struct Params {
   LabelClasses    lc;
@@ -62,6 +67,8 @@ struct Params {
   const DevItem*  items;
   double          alpha, beta;
   int             is_assign;
+  int             energy = 0; // sum (C + alpha * acc)^2 / D into en.part, C unchanged
+  EnergyArgs      en;
 };
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void* gmem, int bytes) {
@@ -145,6 +152,16 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
     s.rowC[m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, mdim, mstrC) : 0;
   for(int n = tid; n < BN; n += NTHREADS)
     s.colC[n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, ndim, nstrC) : 0;
+  if(p.energy) { // batch labels' part folded into the rows'
+    const int32_t* es = p.en.estart + (int64_t) it.group * lc.nc;
+    double         db = 0.0;
+    for(int j = 0; j < lc.nbatch; j++)
+      db += p.en.sg[lc.batch_c[j]] * __ldg(p.en.eps + es[lc.batch_c[j]] + bidx[j]);
+    for(int m = tid; m < BM; m += NTHREADS)
+      s.rowD[m] = (it.m0 + m < Mtot) ? db + energy_part(it.m0 + m, lc.nm, mdim, lc.m_c, p.en, es) : 0.0;
+    for(int n = tid; n < BN; n += NTHREADS)
+      s.colD[n] = (it.n0 + n < Ntot) ? energy_part(it.n0 + n, lc.nn, ndim, lc.n_c, p.en, es) : 1.0;
+  }
 
   // ---- chunk iterator over (task, reduction step, k0), uniform across the CTA ----
   int  cur_t = tb, cur_s = 0, cur_k0 = 0, cur_K = 0, cur_ARBR = 0, cur_BR = 1;
@@ -378,6 +395,33 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
   }
   cp_async_wait<0>();
 
+  if(p.energy) { // sum (C + alpha * acc)^2 / D over the tile, C unchanged; a partial per warp
+    double e = 0.0;
+#pragma unroll
+    for(int i = 0; i < 2; i++) {
+#pragma unroll
+      for(int hr = 0; hr < 2; hr++) {
+        const int m = wm + 16 * i + 8 * hr + lg;
+        if(it.m0 + m >= Mtot) continue;
+        const int64_t rbase = c_base + s.rowC[m];
+        const double  dr    = s.rowD[m];
+#pragma unroll
+        for(int j = 0; j < NJ; j++) {
+#pragma unroll
+          for(int h = 0; h < 2; h++) {
+            const int n = wn + 8 * j + 2 * lt + h;
+            if(it.n0 + n >= Ntot) continue;
+            const double w = __ldcs(p.C + rbase + s.colC[n]) + p.alpha * acc[i][j][2 * hr + h];
+            e              = fma(w * w, recip_nr(dr + s.colD[n]), e);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if((tid & 31) == 0) p.en.part[(int64_t) blockIdx.x * (NTHREADS / 32) + (tid >> 5)] = e;
+    return;
+  }
   // ---- epilogue: C (=|+=) alpha * acc in C's own layout ----
 #pragma unroll
   for(int i = 0; i < 2; i++) {
@@ -435,10 +479,16 @@ void launch_contract_fp64(const Plan& plan, const WorkList& wl, double alpha, do
   p.alpha     = alpha;
   p.beta      = beta;
   p.is_assign = is_assign;
+  if(plan.energy) {
+    TB_EXPECTS(!is_assign && beta == 1.0, "energy epilogue of an assignment");
+    p.energy = 1;
+    p.en     = *plan.energy;
+  }
   const int64_t nitems = (int64_t) wl.items_fp64.size();
   TB_EXPECTS(nitems < (1ll << 31), "work list too large");
   if(wl.items_bn == 80) launch_k<80>(p, (unsigned) nitems, stream);
   else launch_k<64>(p, (unsigned) nitems, stream);
+  if(plan.energy) launch_energy_final(p.en.part, nitems * (NTHREADS / 32), plan.energy_scale, plan.energy_out, stream);
 }
 
 // Work items of the FP64 kernel: one per (group, batch index, 128-row tile, BN-column

@@ -616,6 +616,8 @@ struct I8Params {
   int             xpose;   // C is contiguous along the tile's columns: transposed reductions
   int             store;   // C = alpha * result (an assignment whose output blocks this
                            // launch covers completely) instead of C += alpha * result
+  int             energy = 0; // set for the EN instantiations: sum (C + alpha * result)^2 / D into en.part
+  EnergyArgs      en;
 };
 
 template<int S, int NT>
@@ -623,7 +625,8 @@ __host__ __device__ constexpr uint32_t stage_bytes() {
   return (uint32_t) S * (MT + NT) * KC;
 }
 
-constexpr int kTail  = 3072; // barriers, column scales and C offsets behind the stages
+constexpr int kTail  = 4096; // barriers, column scales and C offsets behind the stages
+constexpr int kTailD = 2560; // offset in the tail of the columns' denominator parts (2 x NT doubles)
 constexpr int kQueue = 4;    // output tiles in flight between producer, MMA issuer and epilogue
 
 // Pipeline depth: as many stages as fit beside the tail, at most 6.
@@ -649,7 +652,9 @@ constexpr size_t smem_bytes() {
 
 // BF: the BF16x3 mode (S = 2 bf16 pieces, kind::f16 MMAs with FP32 accumulators; both
 // diagonals carry the same power of two, 2^(e_row + e_col)).
-template<int S, int NT, bool BF>
+// EN: the energy epilogue (p.energy) instead of the C update, in instantiations of its
+// own so that the plain kernels' code is unchanged.
+template<int S, int NT, bool BF, bool EN = false>
 __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   static_assert(S * NT <= 512, "TMEM holds 512 columns");
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -667,10 +672,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   int32_t*           noff   = reinterpret_cast<int32_t*>(sc + 2 * NT);       // C column offsets, 2 x NT
   int32_t*           qitem  = noff + 2 * NT;
   uint32_t*          tslot  = reinterpret_cast<uint32_t*>(qitem + kQueue);
+  double*            dcol   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTailD); // 2 x NT
   static_assert(sizeof(uint64_t) * (2 * 6 + 1 + 8 + 2 * kQueue) + (sizeof(double) + sizeof(int32_t)) * 2 * NT +
                     4 * kQueue + 4 <=
-                  kTail,
+                  kTailD,
                 "shared-memory tail");
+  static_assert(kTailD + sizeof(double) * 2 * NT <= kTail, "shared-memory tail (denominators)");
   const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if(threadIdx.x == 0) {
@@ -845,7 +852,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       // tile's column offsets in shared memory (alternating buffers by tile; the first
       // task's barrier below publishes them, the readers two tiles back are done)
       int64_t  rowoff = -1;
+      double   drow   = 0.0; // energy epilogue: the row's part of the denominators
       int32_t* nof    = noff + (icount & 1) * NT;
+      double*  dco    = dcol + (icount & 1) * NT;
       {
         int64_t cstr[kMaxModes];
         int64_t s = 1;
@@ -865,11 +874,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           nstr[j] = (int32_t) cstr[p.lc.n_c[j]];
           N *= ndim[j];
         }
-        const int m = item.mt * MT + row;
-        if(m < M) rowoff = g.c_off + decomp(m, p.lc.nm, mdim, mstr);
+        const int      m  = item.mt * MT + row;
+        const int32_t* es = p.en.estart + (int64_t) item.group * p.lc.nc;
+        if(m < M) {
+          rowoff = g.c_off + decomp(m, p.lc.nm, mdim, mstr);
+          if constexpr(EN) drow = energy_part(m, p.lc.nm, mdim, p.lc.m_c, p.en, es);
+        }
         if(et < NT) {
           const int n = item.nt * NT + et;
           nof[et]     = n < N ? decomp(n, p.lc.nn, ndim, nstr) : -1;
+          if constexpr(EN) dco[et] = n < N ? energy_part(n, p.lc.nn, ndim, p.lc.n_c, p.en, es) : 1.0;
         }
       }
       for(int t = g.task_begin; t < g.task_end; t++, tcount++) {
@@ -974,6 +988,58 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
       }
       if(!ok) break;
+      if constexpr(EN) {
+        // sum (C + alpha * result)^2 / D over the tile; C is read, not written.  One
+        // partial sum per warp and tile (each thread's elements in a fixed order, then
+        // a fixed shuffle tree), so the total does not depend on which CTA took a tile.
+        double e = 0.0;
+        if constexpr(xpose_fits<S, NT>()) {
+          if(p.xpose) { // C contiguous along the columns: each load covers 4 rows x 8 columns
+            double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * kXCols * kXStride;
+            const int rsub = lane / kXCols, csub = lane % kXCols;
+#pragma unroll 1
+            for(int x0 = 0; x0 < NH; x0 += kXCols) {
+#pragma unroll
+              for(int j = 0; j < kXCols; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
+              __syncwarp();
+              const int    o  = nof[col0 + x0 + csub];
+              const double dc = dco[col0 + x0 + csub];
+              double       cv[kXCols];
+#pragma unroll
+              for(int rr = 0; rr < kXCols; rr++) { // the loads first, all in flight
+                const int64_t ro = __shfl_sync(0xffffffffu, rowoff, rr * (32 / kXCols) + rsub);
+                cv[rr]           = (ro >= 0 && o >= 0) ? __ldcs(p.C + ro + o) : 0.0;
+              }
+#pragma unroll
+              for(int rr = 0; rr < kXCols; rr++) {
+                const int     r  = rr * (32 / kXCols) + rsub;
+                const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
+                const double  dr = __shfl_sync(0xffffffffu, drow, r);
+                if(ro >= 0 && o >= 0) {
+                  const double w = cv[rr] + xb[csub * kXStride + r];
+                  e              = fma(w * w, recip_nr(dr + dc), e);
+                }
+              }
+              __syncwarp(); // the next columns overwrite the buffer
+            }
+          }
+        }
+        if(!(xpose_fits<S, NT>() && p.xpose) && rowoff >= 0) {
+          const double* crow = p.C + rowoff;
+#pragma unroll
+          for(int x = 0; x < NH; x++) {
+            const int o = nof[col0 + x];
+            if(o >= 0) {
+              const double w = __ldcs(crow + o) + p.alpha * racc[x];
+              e              = fma(w * w, recip_nr(drow + dco[col0 + x]), e);
+            }
+          }
+        }
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if(lane == 0) p.en.part[(int64_t) it * (NEPI / 32) + (warp - 2)] = e;
+        continue;
+      }
       // C (+)= alpha * result: one reduction per element (c + alpha * r, rounded once,
       // as a load-add-store would be; every element of C belongs to exactly one output
       // tile), performed at L2, so the epilogue does not wait for C's memory; a plain
@@ -1307,26 +1373,56 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
   chunks(L->b_blocks, L->b_cbegin);
   partition_sets(L->a_blocks, esize, L->a_staged, L->a_general);
   partition_sets(L->b_blocks, esize, L->b_staged, L->b_general);
-  // output tiles, longest group first (every tile of a group costs the same, so
-  // ordering the groups orders the tiles)
-  std::vector<std::pair<int64_t, int32_t>> order; // (K steps of a tile, group)
+  // Output tiles, longest group first (every tile of a group costs the same, so
+  // ordering the groups orders the tiles).  Among groups of equal work, those whose
+  // first task reads the same A block (the same rows: e.g. W(a,b,c,..) = v(b,c,..) *
+  // t2(a,..) for every a tile) are interleaved row tile by row tile, so the CTAs that
+  // take consecutive tiles read each A tile's digits from HBM once and from L2 after.
+  struct Ord {
+    int64_t work, akey;
+    int32_t group;
+  };
+  std::vector<Ord> order;
   for(size_t gi = 0; gi < wl.groups.size(); gi++) {
     const DevGroup& g = wl.groups[gi];
     if(g.task_begin == g.task_end) continue;
     int64_t work = 0;
     for(int t = g.task_begin; t < g.task_end; t++) work += L->tasks[t].nkc;
-    order.emplace_back(work, (int32_t) gi);
+    order.push_back(Ord{work, L->tasks[g.task_begin].a_off, (int32_t) gi});
   }
-  std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-  for(const auto& o: order) {
-    const DevGroup& g = wl.groups[o.second];
+  std::stable_sort(order.begin(), order.end(), [](const Ord& a, const Ord& b) {
+    return a.work != b.work ? a.work > b.work : a.akey < b.akey;
+  });
+  auto tiles_of = [&](int32_t gi, int64_t& mts, int64_t& nts) {
+    const DevGroup& g = wl.groups[gi];
     int64_t         M = 1, N = 1;
     for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
     for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
-    const int64_t mts = (M + MT - 1) / MT, nts = (N + L->NT - 1) / L->NT;
+    mts = (M + MT - 1) / MT;
+    nts = (N + L->NT - 1) / L->NT;
+  };
+  for(size_t r0 = 0; r0 < order.size();) {
+    size_t r1 = r0 + 1; // groups [r0, r1): equal work, same first A block
+    while(r1 < order.size() && order[r1].work == order[r0].work && order[r1].akey == order[r0].akey) r1++;
+    int64_t mts = 0;
+    for(size_t r = r0; r < r1; r++) {
+      int64_t gm = 0, gn = 0;
+      tiles_of(order[r].group, gm, gn);
+      mts = std::max(mts, gm);
+    }
     for(int64_t mt = 0; mt < mts; mt++)
-      for(int64_t nt = 0; nt < nts; nt++) L->items.push_back(I8Item{o.second, (int32_t) mt, (int32_t) nt, 0});
-    L->int8_ops += 2.0 * MT * L->NT * kstep * o.first * (S * (S + 1) / 2) * (double) (mts * nts);
+      for(size_t r = r0; r < r1; r++) {
+        int64_t gm = 0, gn = 0;
+        tiles_of(order[r].group, gm, gn);
+        if(mt >= gm) continue;
+        for(int64_t nt = 0; nt < gn; nt++) L->items.push_back(I8Item{order[r].group, (int32_t) mt, (int32_t) nt, 0});
+      }
+    for(size_t r = r0; r < r1; r++) {
+      int64_t gm = 0, gn = 0;
+      tiles_of(order[r].group, gm, gn);
+      L->int8_ops += 2.0 * MT * L->NT * kstep * order[r].work * (S * (S + 1) / 2) * (double) (gm * gn);
+    }
+    r0 = r1;
   }
   TB_CUDA(cudaGetDevice(&L->device));
   auto up = [](auto*& dptr, const auto& vec) {
@@ -1429,7 +1525,7 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
 
 template<int S, int NT, bool BF>
 void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha,
-                 const uint8_t* slices, const int32_t* exps, double* C, bool store, cudaStream_t st) {
+                 const uint8_t* slices, const int32_t* exps, double* C, const Plan& plan, cudaStream_t st) {
   if(L.items.empty()) return;
   I8Params p;
   p.a_slices = L.a_cache ? L.a_cache->slices : slices;
@@ -1448,34 +1544,44 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   p.ctr     = L.d_ctr;
   // transposed reductions when C's last mode (stride 1) is a column label of the tile
   p.xpose = xpose_fits<S, NT>() && lc.nn > 0 && lc.n_c[lc.nn - 1] == lc.nc - 1 ? 1 : 0;
-  p.store = store ? 1 : 0;
+  p.store = plan.store ? 1 : 0;
+  if(plan.energy) {
+    p.energy = 1;
+    p.en     = *plan.energy;
+  }
   TB_CUDA(cudaMemsetAsync(L.d_ctr, 0, sizeof(int), st));
   const size_t smem = smem_bytes<S, NT>();
-  static bool  configured[64] = {false};
+  static bool  configured[64][2] = {};
   int          dev            = 0;
   TB_CUDA(cudaGetDevice(&dev));
-  if(dev < 64 && !configured[dev]) {
-    TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    configured[dev] = true;
+  const int e = plan.energy ? 1 : 0;
+  if(dev < 64 && !configured[dev][e]) {
+    if(e) TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int) smem));
+    else TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    configured[dev][e] = true;
   }
   const int grid = (int) std::min<int64_t>((int64_t) L.items.size(), sm_count());
-  k_contract_i8<S, NT, BF><<<grid, NTHREADS, smem, st>>>(p);
+  if(e) k_contract_i8<S, NT, BF, true><<<grid, NTHREADS, smem, st>>>(p);
+  else k_contract_i8<S, NT, BF><<<grid, NTHREADS, smem, st>>>(p);
   TB_CUDA(cudaGetLastError());
+  if(plan.energy)
+    launch_energy_final(p.en.part, (int64_t) L.items.size() * (NEPI / 32), plan.energy_scale, plan.energy_out, st);
 }
 
 template<int S, bool BF = false>
 void run_s(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha, const double* A,
-           const double* B, double* C, uint8_t* slices, int32_t* exps, bool store, cudaStream_t st,
+           const double* B, double* C, uint8_t* slices, int32_t* exps, const Plan& plan, cudaStream_t st,
            cudaEvent_t* ev) {
   if(ev) TB_CUDA(cudaEventRecord(ev[0], st));
   launch_split<S, BF>(L, wl, A, B, slices, exps, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[1], st));
   // output tile width: 80 columns by default for S <= 6 (S x NT <= 512 TMEM columns)
   if constexpr(S * 80 <= 512) {
-    if(L.NT == 80) launch_gemm<S, 80, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
+    if(L.NT == 80) launch_gemm<S, 80, BF>(L, wl, lc, alpha, slices, exps, C, plan, st);
   }
-  if(L.NT == 64) launch_gemm<S, 64, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
-  if(L.NT == 48) launch_gemm<S, 48, BF>(L, wl, lc, alpha, slices, exps, C, store, st);
+  if(L.NT == 64) launch_gemm<S, 64, BF>(L, wl, lc, alpha, slices, exps, C, plan, st);
+  if(L.NT == 48) launch_gemm<S, 48, BF>(L, wl, lc, alpha, slices, exps, C, plan, st);
   if(ev) TB_CUDA(cudaEventRecord(ev[2], st));
 }
 
@@ -1592,7 +1698,7 @@ void contract_split(Plan& plan, const WorkList& wl, double alpha, const double* 
     for(auto& e: evs) TB_CUDA(cudaEventCreate(&e));
     ev = evs;
   }
-  const bool st = plan.store;
+  const Plan& st = plan;
   if(bf) run_s<2, true>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev);
   else switch(S) {
     case 3: run_s<3>(*L, wl, lc, alpha, A, B, C, slices, exps, st, stream, ev); break;

@@ -610,10 +610,12 @@ std::shared_ptr<WorkList> mult_worklist(const Op& op, const LabelClasses& lc, bo
 
 void run_contract(Plan& plan, const WorkList& wl, double alpha, const double* A, const double* B,
                   double* C, cudaStream_t stream, Arena* arena); // tb_capi.cpp
+static std::shared_ptr<EnergySpec> build_energy(const Op& op, const LabelClasses& lc, const std::shared_ptr<Ctx>& ctx);
 
 void Sched::run(Op& op) {
   cudaStream_t st = ctx->stream;
-  if(op.kind == Op::Set || op.kind == Op::Add || op.kind == Op::Mult || op.kind == Op::Denom || op.kind == Op::Map)
+  if(op.kind == Op::Set || op.kind == Op::Add || (op.kind == Op::Mult && !op.energy) || op.kind == Op::Denom ||
+     op.kind == Op::Map)
     op.lhs.t->require_writable();
   if(op.kind == Op::Map) {
     op.lhs.t->require_allocated();
@@ -850,6 +852,7 @@ void Sched::run(Op& op) {
   }
   // MultOp
   if(op.a.t->is_lambda() || op.b.t->is_lambda()) {
+    if(op.energy) fail(TB_ERR_NOT_IMPLEMENTED, "energy epilogue with a lambda operand");
     run_lambda_mult(op);
     return;
   }
@@ -862,7 +865,13 @@ void Sched::run(Op& op) {
   op.plan->nslices    = ctx->nslices;
   op.plan->tile_n     = 0;
   op.plan->store      = op.store;
-  if(autotune && ctx->mode == TB_MODE_INT8 && !pinned) {
+  if(op.energy) { // the energy epilogue keeps the context's precision (no autotuning)
+    if(!op.espec) op.espec = build_energy(op, op.plan->lc, ctx);
+    op.plan->energy       = &op.espec->args;
+    op.plan->energy_out   = scalars() + op.slot;
+    op.plan->energy_scale = op.value;
+  }
+  else if(autotune && ctx->mode == TB_MODE_INT8 && !pinned) {
     const std::string key = signature(op) + "|" + std::to_string(ctx->err_target) + "|" + std::to_string(ctx->nslices);
     auto              it  = tune_cache.find(key);
     if(it == tune_cache.end()) {
@@ -891,6 +900,15 @@ void Sched::run(Op& op) {
   op.flops              = op.wl->flops;
   run_contract(*op.plan, *op.wl, op.alpha, op.a.t->data, op.b.t->data, op.lhs.t->data, st,
                ctx->arena.get());
+  if(op.energy) {
+    op.plan->energy = nullptr;
+    if(const auto& r = op.espec->rest; r && r->nunits > 0) { // blocks of groups without tasks: C as it is
+      DenomSigns sg{};
+      for(int m = 0; m < kMaxModes; m++) sg.s[m] = r->signs[m];
+      launch_denom_energy(op.lhs.t->data, op.value, r->d_blocks, r->d_units, r->nunits, op.lhs.t->nmodes, r->d_eps,
+                          sg, r->d_part, scalars() + op.slot, st);
+    }
+  }
   op.plan->profile      = false;
   op.plan->pinned       = nullptr;
   op.plan->check_errors = true;
@@ -1030,10 +1048,11 @@ Sched::~Sched() {
 
 // Block table of a denominator op over t's admitted blocks: packed offset, dims and
 // the root orbital index of each mode's first element (uploaded once).
-void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c) {
+void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c, const std::vector<int64_t>* only) {
   std::vector<DenomBlock> blocks;
   std::vector<int64_t>    id(T.nmodes);
   for(size_t bi = 0; bi < T.keys.size(); bi++) {
+    if(only && !std::binary_search(only->begin(), only->end(), T.offsets[bi])) continue;
     int64_t key = T.keys[bi]; // block id in each mode's own tile numbering
     for(int m = T.nmodes - 1; m >= 0; m--) {
       const int64_t n = T.tis[m]->ntiles();
@@ -1073,6 +1092,61 @@ void DenomSpec::build(const Tensor& T, const std::shared_ptr<Ctx>& c) {
   if(!units.empty())
     TB_CUDA(cudaMemcpy(d_units, units.data(), sizeof(DenomUnit) * units.size(), cudaMemcpyHostToDevice));
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_part), sizeof(double) * std::max<size_t>(units.size(), 1)));
+}
+
+EnergySpec::~EnergySpec() {
+  if(ctx) cudaSetDevice(ctx->device);
+  if(args.estart) cudaFree(const_cast<int32_t*>(args.estart));
+  if(args.part) cudaFree(args.part);
+}
+
+// The energy epilogue's device state for a Mult over its work list (see EnergySpec).
+static std::shared_ptr<EnergySpec> build_energy(const Op& op, const LabelClasses& lc, const std::shared_ptr<Ctx>& ctx) {
+  const Tensor&   C  = *op.lhs.t;
+  const WorkList& wl = *op.wl;
+  const int       nc = C.nmodes;
+  auto            es = std::make_shared<EnergySpec>();
+  es->ctx            = ctx;
+  std::vector<int32_t> est(std::max<size_t>(wl.groups.size() * nc, 1), 0);
+  std::vector<int64_t> rest;
+  for(size_t gi = 0; gi < wl.groups.size(); gi++) {
+    const DevGroup& g = wl.groups[gi];
+    auto            o = std::lower_bound(C.offsets.begin(), C.offsets.end(), g.c_off);
+    TB_EXPECTS(o != C.offsets.end() && *o == g.c_off, "energy epilogue: output group is not a stored block");
+    if(g.task_begin == g.task_end) {
+      rest.push_back(g.c_off);
+      continue;
+    }
+    int64_t key = C.keys[o - C.offsets.begin()];
+    int64_t id[kMaxModes];
+    for(int m = nc - 1; m >= 0; m--) {
+      id[m] = key % C.tis[m]->ntiles();
+      key /= C.tis[m]->ntiles();
+    }
+    for(int m = 0; m < nc; m++) {
+      const int64_t first = C.tis[m]->root->offsets[C.tis[m]->tiles[id[m]]];
+      TB_EXPECTS(first + g.cdims[m] <= (int64_t) op.denom->eps.size(),
+                 "orbital energies shorter than the index space");
+      est[gi * nc + m] = (int32_t) first;
+    }
+    // partial sums: 8 warps per output tile, tiles at least 128 x 48 (every kernel's)
+    int64_t M = 1, N = 1, Bt = 1;
+    for(int j = 0; j < lc.nm; j++) M *= g.cdims[lc.m_c[j]];
+    for(int j = 0; j < lc.nn; j++) N *= g.cdims[lc.n_c[j]];
+    for(int j = 0; j < lc.nbatch; j++) Bt *= g.cdims[lc.batch_c[j]];
+    es->npart += 8 * Bt * ((M + 127) / 128) * ((N + 47) / 48);
+  }
+  int32_t* d_est = nullptr;
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_est), sizeof(int32_t) * est.size()));
+  es->args.estart = d_est;
+  TB_CUDA(cudaMemcpy(d_est, est.data(), sizeof(int32_t) * est.size(), cudaMemcpyHostToDevice));
+  TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&es->args.part), sizeof(double) * std::max<int64_t>(es->npart, 1)));
+  std::sort(rest.begin(), rest.end());
+  if(!op.denom->d_eps) op.denom->build(C, ctx, &rest); // eps on the device (and the blocks for `rest`)
+  es->args.eps = op.denom->d_eps;
+  for(int m = 0; m < nc; m++) es->args.sg[m] = op.denom->signs[m];
+  if(!rest.empty()) es->rest = op.denom;
+  return es;
 }
 
 DenomSpec::~DenomSpec() {
@@ -1240,7 +1314,7 @@ void Sched::run_lambda_mult(Op& op) {
 // Updates the blocks known to be zero after `op` ran (see Sched::execute).
 void Sched::note_zeros(const Op& op, std::map<const Tensor*, std::shared_ptr<std::vector<uint8_t>>>& szero) {
   Tensor* t = op.lhs.t;
-  if(t == nullptr || op.kind == Op::Dot || op.kind == Op::DenomEnergy || op.kind == Op::SetScalar) return;
+  if(t == nullptr || op.kind == Op::Dot || op.kind == Op::DenomEnergy || op.kind == Op::SetScalar || op.energy) return;
   if(op.kind == Op::Set) {
     bool whole = op.is_assign && op.value == 0.0;
     for(int m = 0; whole && m < t->nmodes; m++) whole = op.lhs.ltis[m]->tiles == t->tis[m]->tiles;
@@ -1302,7 +1376,7 @@ void Sched::execute(bool profile) {
     }
     if(nranks == 1 && i + 1 < ops.size() && ops[i].kind == Op::Set &&
        ops[i].is_assign && ops[i].value == 0.0 &&
-       ops[i + 1].kind == Op::Mult && same_target(ops[i].lhs, ops[i + 1].lhs) &&
+       ops[i + 1].kind == Op::Mult && !ops[i + 1].energy && same_target(ops[i].lhs, ops[i + 1].lhs) &&
        ops[i + 1].a.t != ops[i].lhs.t && ops[i + 1].b.t != ops[i].lhs.t && // C read as an operand needs the fill
        !ops[i + 1].a.t->is_lambda() && !ops[i + 1].b.t->is_lambda())      // (a batched op adds batch by batch)
       fuse_assign(ops[i], ops[i + 1]);

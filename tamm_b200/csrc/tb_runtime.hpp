@@ -174,6 +174,7 @@ struct Labeled {
 };
 
 struct DenomSpec;
+struct EnergySpec;
 
 // tb_labeled (C ABI) -> Labeled; NULL label spaces mean the tensor's own.
 Labeled labeled_from_c(const tb_labeled& x);
@@ -189,6 +190,11 @@ struct Op {
   int     is_assign = 0;
   int     slot = 0, root = 0;
   std::shared_ptr<DenomSpec> denom;
+  // Mult with the energy epilogue (tb_sched_mult_energy): slot += value * sum
+  // (lhs + alpha * a * b)^2 / D over the output blocks the op addresses, lhs unchanged
+  // (D from `denom`)
+  bool                        energy = false;
+  std::shared_ptr<EnergySpec> espec;
   std::string                tune_key; // set when the autotuner chose this op's kernel
   // cached execution state
   std::shared_ptr<Plan>     plan;
@@ -233,9 +239,23 @@ struct DenomSpec {
   double*                 d_part   = nullptr; // per-CTA partial sums of the energy reduction
                                               // (nunits entries: the grid is never larger)
   int                     nblocks  = 0, nunits = 0;
-  void                    build(const Tensor& t, const std::shared_ptr<Ctx>& ctx);
+  // over the stored blocks of t (only those at the sorted element offsets `only`, if given)
+  void                    build(const Tensor& t, const std::shared_ptr<Ctx>& ctx,
+                                const std::vector<int64_t>* only = nullptr);
   std::shared_ptr<Ctx>    ctx;
   ~DenomSpec();
+};
+
+// Device state of a Mult's energy epilogue, built on its first execution: the
+// denominators' first orbital index of each output mode per work-list group (groups
+// with tasks: the kernels' epilogue), the kernels' partial sums, and a denominator-
+// energy pass over the blocks of groups without tasks.
+struct EnergySpec {
+  EnergyArgs                 args;
+  std::shared_ptr<DenomSpec> rest;
+  int64_t                    npart = 0;
+  std::shared_ptr<Ctx>       ctx;
+  ~EnergySpec();
 };
 
 // Choice of the autotuner for one contraction signature and precision request.

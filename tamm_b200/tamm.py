@@ -783,6 +783,27 @@ class Scheduler:
              e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
         return self
 
+    def mult_energy(self, slot: int, scale: float, spec: _OpSpec, eps, signs):
+        """Queue slot += scale * sum (lhs + alpha * a * b)^2 / D for spec = lhs.iadd(alpha * a * b)
+        (or lhs.isub(...)), D = sum_m signs[m] * eps[orbital index of lhs mode m]: the
+        contraction with the denominator energy fused into its epilogue; lhs is read, not
+        written."""
+        if spec.is_assign:
+            raise ValueError("the energy epilogue adds to lhs's values; an assignment has none")
+        rhs = spec.rhs
+        if not isinstance(rhs, _Product) or len(rhs.factors) != 2:
+            raise TypeError("right-hand side must be a product of two labelled tensors")
+        ids: dict = {}
+        lhs = self._labeled(spec.lhs, ids)
+        a = self._labeled(rhs.factors[0], ids)
+        b = self._labeled(rhs.factors[1], ids)
+        e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64))
+        sg = np.ascontiguousarray(np.asarray(list(signs) + [0.0] * (8 - len(signs)), dtype=np.float64))
+        self._keep += [e, sg]
+        call("tb_sched_mult_energy", self.h, int(slot), float(scale), lhs, spec.sign * rhs.alpha, a, b,
+             e.ctypes.data_as(A.dp), int(e.size), sg.ctypes.data_as(A.dp))
+        return self
+
     def set_scalar(self, slot: int, value: float = 0.0):
         call("tb_sched_set_scalar", self.h, int(slot), float(value))
         return self

@@ -165,7 +165,7 @@ def test_config5_w_step_tile40(big_ec):
         ec.set_precision(mode, 1e-11)
         try:
             sch = tb.Scheduler(ec)
-            Wt, _ = triples.queue_pair(P, sch, *step)
+            Wt, _ = triples.queue_pair(P, sch, *step, fused=False)  # W itself: both terms stored
             sch.execute(tb.ExecutionHW.GPU)
             got = _dense_from(Wt)[:, :, :, 0, :, :]
             Wt.deallocate()

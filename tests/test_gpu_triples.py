@@ -8,7 +8,8 @@ summed over every streaming step:
 with v(b,c,d,k) = sum_Q L(Q,b,d) L(Q,c,k), v(l,c,j,k) = sum_Q L(Q,l,j) L(Q,c,k), the
 Cholesky vectors read back from the device.  TAMM has no triples code, so the
 reference is this restatement (numpy einsum).  Bars: FP64 1e-12, split-INT8 1e-10
-relative to |E|."""
+relative to |E|, for the energy fused into the second contraction's epilogue and for
+the separate W update and denominator-energy ops."""
 import numpy as np
 import pytest
 
@@ -53,16 +54,17 @@ def _reference(P, oa, va, seed):
     return float(np.sum(Wd * Wd / D))
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("dtile", [4, 0])
 @pytest.mark.parametrize("mode,tol", [(tb.Precision.FP64, 1e-12), (tb.Precision.INT8, 1e-10)])
-def test_streamed_triples_energy(ec, mode, tol, dtile):
+def test_streamed_triples_energy(ec, mode, tol, dtile, fused):
     oa, va, seed = 3, 8, 4
     # j blocks of 2, 1 (ragged); d on the output tiling (4) or one tile per spin block (0)
     P = triples.build(oa, va, tile=4, jtile=2, dtile=dtile, seed=seed, ec=ec)
     want = _reference(P, oa, va, seed)
     ec.set_precision(mode, 1e-11)
     try:
-        e, flops, _ = triples.energy(P, triples.steps(P), tb.Scheduler(ec))
+        e, flops, _ = triples.energy(P, triples.steps(P), tb.Scheduler(ec), fused=fused)
     finally:
         ec.set_precision(tb.Precision.FP64)
         P.release()
