@@ -317,7 +317,7 @@ def measure_triples(ec, torch, nsteps):
     rng = np.random.default_rng(9)
     sample = [allsteps[int(x)] for x in rng.choice(len(allsteps), size=nsteps, replace=False)]
     out, es = {"workload": "triples_energy_O50_V500_tile40", "sampled_steps": sample, "steps_total": len(allsteps),
-               "energy": "sum W^2 / D fused into the epilogue of the contraction over l (W read once, not written)"}, {}
+               "energy": "W = t2.v over d (stored), W -= t2.v over l, then sum W^2 / D (k_denom)"}, {}
     out["digit_cache_bytes_before"] = ec.digit_cache_info()[0]
     ec.set_digit_cache(int(24 * 2 ** 30))
     for name, mode in (("fp64", tb.Precision.FP64), ("int8", tb.Precision.INT8)):

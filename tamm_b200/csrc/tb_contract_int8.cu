@@ -886,6 +886,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           if constexpr(EN) dco[et] = n < N ? energy_part(n, p.lc.nn, ndim, p.lc.n_c, p.en, es) : 1.0;
         }
       }
+      if constexpr(EN) {
+        // the tile's C values go to L2 while its MMAs run (the energy epilogue reads them
+        // once they are done): the epilogue warps publish the column offsets first
+        asm volatile("bar.sync 1, %0;\n" ::"n"(NEPI) : "memory");
+        if(rowoff >= 0) {
+          const double* crow = p.C + rowoff;
+#pragma unroll
+          for(int x = 0; x < NH; x += (p.xpose ? kXCols : 1)) { // xpose: a row's columns are contiguous
+            const int o = nof[col0 + x];
+            if(o >= 0) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(crow + o));
+          }
+        }
+      }
       for(int t = g.task_begin; t < g.task_end; t++, tcount++) {
         // The task's metadata and column scales 2^(e_col - 7) are fetched before its
         // accumulators are complete, so their latency overlaps the task's MMAs.  The
@@ -1027,12 +1040,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         if(!(xpose_fits<S, NT>() && p.xpose) && rowoff >= 0) {
           const double* crow = p.C + rowoff;
 #pragma unroll
-          for(int x = 0; x < NH; x++) {
-            const int o = nof[col0 + x];
-            if(o >= 0) {
-              const double w = __ldcs(crow + o) + p.alpha * racc[x];
-              e              = fma(w * w, recip_nr(drow + dco[col0 + x]), e);
+          for(int x0 = 0; x0 < NH; x0 += 8) { // eight loads in flight, then their sums
+            double cv[8];
+#pragma unroll
+            for(int j = 0; j < 8; j++) {
+              const int o = nof[col0 + x0 + j];
+              cv[j]       = o >= 0 ? __ldcs(crow + o) : 0.0;
             }
+#pragma unroll
+            for(int j = 0; j < 8; j++)
+              if(nof[col0 + x0 + j] >= 0) {
+                const double w = cv[j] + p.alpha * racc[x0 + j];
+                e              = fma(w * w, recip_nr(drow + dco[col0 + x0 + j]), e);
+              }
           }
         }
 #pragma unroll

@@ -12,11 +12,13 @@ the denominator-energy op of this library.
 Streaming: a t3 block of one tile tuple holds tile^6 values (4e9 at tile 40), so W
 is formed one step at a time, a step being one occupied index i and one block of
 `jtile` occupied indices j: W(a,b,c,k) for that (i, j-block) is one contraction
-over d into a shared buffer (a fused assignment: the kernel stores), then the
-contraction over l runs with the energy fused into its epilogue
-(Scheduler.mult_energy): each element W1 - t2.v is formed in registers, squared,
-divided by D and summed, so W is read once and never written back.  (`fused=False`
-queues the two separate ops instead: W -= t2.v, then slot += sum W^2 / D.)
+over d into a shared buffer (a fused assignment: the kernel stores), minus one over
+l, then slot += sum W^2 / D.  With `fused=True` the energy instead runs in the
+epilogue of the contraction over d (Scheduler.mult_energy), after W = -t2.v over l:
+each element W + t2.v is formed in registers, squared, divided by D and summed, so W
+is written once and read once.  Both give the same energy up to summation order;
+the separate ops are the default, being the faster on a B200 (both contraction
+kernels are bound by their per-tile epilogue here, not by the bytes of W).
 The streamed labels need finer occupied tiles (i single, j in blocks of jtile)
 while the summed l keeps the uniform tiles, so t2 is held in two tilings
 (t2(a,d,i,j) with i single and j blocked; t2(a,b,i,l) with l uniform) and v(l,c,j,k)
@@ -146,10 +148,10 @@ def steps(P: TriplesProblem):
     return [(i, jt) for i in range(P.O1.num_tiles) for jt in range(P.Oj.num_tiles)]
 
 
-def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int, fused: bool = True):
+def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int, fused: bool = False):
     """Queues W(a,b,c,k) for occupied index i and j block jt, and slot SLOT_E +=
-    sum W^2 / D (fused: in the epilogue of the second contraction, W then holding only
-    the first term afterwards).  Returns (W tensor, FP64 FLOPs of the two contractions)."""
+    sum W^2 / D (fused: in the epilogue of the contraction over d, W then holding only
+    the term over l afterwards).  Returns (W tensor, FP64 FLOPs of the two contractions)."""
     Wt = _w_tensor(P.V, P.O1, P.Oj, P.Ob, i, jt)
     Wt.attach(P.ec, P.buffer, P.most * 8)
     a, b, c = P.V.labels(3)
@@ -161,16 +163,17 @@ def queue_pair(P: TriplesProblem, sch: Scheduler, i: int, jt: int, fused: bool =
     x = (w, T["vx"](b, c, k, d), T["t2x"](a, d, li, lj))
     y = (w, T["t2y"](a, b, li, l), T["vy"](l, c, lj, k))
     signs = [-1, -1, -1, 1, 1, 1]
-    sch(w.assign(x[1] * x[2]))
     if fused:
-        sch.mult_energy(SLOT_E, 1.0, w.isub(y[1] * y[2]), P.eps, signs)
+        sch(w.assign(-1.0 * y[1] * y[2]))
+        sch.mult_energy(SLOT_E, 1.0, w.iadd(x[1] * x[2]), P.eps, signs)
     else:
+        sch(w.assign(x[1] * x[2]))
         sch(w.isub(y[1] * y[2]))
         sch.denom_energy(SLOT_E, 1.0, Wt(a, b, c, li, lj, k), P.eps, signs)
     return Wt, mult_info(*x)[2] + mult_info(*y)[2]
 
 
-def energy(P: TriplesProblem, pairs, sch: Scheduler, release_every: int = 8, fused: bool = True):
+def energy(P: TriplesProblem, pairs, sch: Scheduler, release_every: int = 8, fused: bool = False):
     """E summed over the given steps (i, j block); returns (E, FP64 FLOPs, device ms).
 
     The steps are enqueued back to back (tb_sched_execute_async): the host builds the
@@ -219,8 +222,8 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=4)
     p.add_argument("--steps", type=int, default=8)
     p.add_argument("--pool-gib", type=int, default=80)
-    p.add_argument("--no-fuse", action="store_true",
-                   help="separate ops (W -= t2.v, then the denominator energy) instead of the fused epilogue")
+    p.add_argument("--fuse", action="store_true",
+                   help="energy fused into the epilogue of the contraction over d (Scheduler.mult_energy)")
     p.add_argument("--digit-cache-gib", type=int, default=16,
                    help="split-INT8 digits of the read-only integrals kept across contractions (0: off)")
     args = p.parse_args(argv)
@@ -231,13 +234,13 @@ def main(argv=None):
     rng = np.random.default_rng(args.seed + 5)
     sample = [allsteps[int(x)] for x in rng.choice(len(allsteps), size=min(args.steps, len(allsteps)), replace=False)]
     out = {"workload": f"triples_energy_O{2 * args.oa}_V{2 * args.va}_tile{args.tile}_jtile{args.jtile}_dtile{args.dtile}",
-           "sampled_steps": sample, "steps_total": len(allsteps), "fused_energy": not args.no_fuse}
+           "sampled_steps": sample, "steps_total": len(allsteps), "fused_energy": args.fuse}
     res, wref = {}, None
     for name, mode in (("fp64", Precision.FP64), ("int8", Precision.INT8)):
         ec.set_precision(mode, 1e-11)
         sch = Scheduler(ec)
-        energy(P, sample[:1], sch, fused=not args.no_fuse)  # warm-up: kernels, digit layouts
-        e, fl, ms = energy(P, sample, sch, fused=not args.no_fuse)
+        energy(P, sample[:1], sch, fused=args.fuse)  # warm-up: kernels, digit layouts
+        e, fl, ms = energy(P, sample, sch, fused=args.fuse)
         res[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9,
                      "full_run_s_extrapolated": ms / len(sample) * len(allsteps) / 1e3}
         # W of the first sampled step (both terms: the unfused ops), kept on the device

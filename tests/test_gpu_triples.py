@@ -8,8 +8,8 @@ summed over every streaming step:
 with v(b,c,d,k) = sum_Q L(Q,b,d) L(Q,c,k), v(l,c,j,k) = sum_Q L(Q,l,j) L(Q,c,k), the
 Cholesky vectors read back from the device.  TAMM has no triples code, so the
 reference is this restatement (numpy einsum).  Bars: FP64 1e-12, split-INT8 1e-10
-relative to |E|, for the energy fused into the second contraction's epilogue and for
-the separate W update and denominator-energy ops."""
+relative to |E|, for the separate W update and denominator-energy ops and for the
+energy fused into the epilogue of the contraction over d (Scheduler.mult_energy)."""
 import numpy as np
 import pytest
 
