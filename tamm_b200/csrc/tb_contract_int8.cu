@@ -78,6 +78,20 @@ struct I8Item {
   int32_t group, mt, nt, pad;
 };
 
+// One output tile as the producer hands it to the MMA issuer and the epilogue through a
+// shared-memory queue slot: its item, group and first task, and the row / column
+// geometry of its C block (extents and strides of the row and column labels), worked
+// out once per tile by the producer, off the consumers' critical path, and read by the
+// epilogue threads from shared memory (indexing per-thread arrays by runtime label
+// positions would put them in local memory).
+struct TileRec {
+  int64_t c_off;
+  int32_t group, mt, nt, task_begin, task_end, M, N, a_exp0, b_exp0, st0;
+  int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
+  int32_t pad[4];
+};
+static_assert(sizeof(TileRec) == 128, "tile record size");
+
 __device__ __forceinline__ int32_t decomp(int32_t x, int n, const int32_t* dims, const int32_t* str) {
   int32_t off = 0;
   for(int j = n - 1; j >= 0; j--) {
@@ -625,8 +639,9 @@ __host__ __device__ constexpr uint32_t stage_bytes() {
   return (uint32_t) S * (MT + NT) * KC;
 }
 
-constexpr int kTail  = 4096; // barriers, column scales and C offsets behind the stages
+constexpr int kTail  = 4608; // barriers, column scales, C offsets and tile records behind the stages
 constexpr int kTailD = 2560; // offset in the tail of the columns' denominator parts (2 x NT doubles)
+constexpr int kTailT = 3840; // offset in the tail of the queue slots' tile records
 constexpr int kQueue = 4;    // output tiles in flight between producer, MMA issuer and epilogue
 
 // Pipeline depth: as many stages as fit beside the tail, at most 6.
@@ -673,11 +688,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   int32_t*           qitem  = noff + 2 * NT;
   uint32_t*          tslot  = reinterpret_cast<uint32_t*>(qitem + kQueue);
   double*            dcol   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTailD); // 2 x NT
+  TileRec*           trec   = reinterpret_cast<TileRec*>(smem + STAGES * STAGE + kTailT);  // kQueue
   static_assert(sizeof(uint64_t) * (2 * 6 + 1 + 8 + 2 * kQueue) + (sizeof(double) + sizeof(int32_t)) * 2 * NT +
                     4 * kQueue + 4 <=
                   kTailD,
                 "shared-memory tail");
-  static_assert(kTailD + sizeof(double) * 2 * NT <= kTail, "shared-memory tail (denominators)");
+  static_assert(kTailD + sizeof(double) * 2 * NT <= kTailT, "shared-memory tail (denominators)");
+  static_assert(kTailT + sizeof(TileRec) * kQueue <= kTail, "shared-memory tail (tile records)");
   const int          warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if(threadIdx.x == 0) {
@@ -710,14 +727,58 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         if(!mbar_wait(&qempty[qslot], qph ^ 1, p.err, 5)) goto done_producer;
         const int it = atomicAdd(p.ctr, 1);
         qitem[qslot] = it < p.nitems ? it : -1;
-        mbar_arrive(&qfull[qslot]);
+        I8Item   item{};
+        DevGroup g{};
+        if(it < p.nitems) {
+          item       = p.items[it];
+          g          = p.groups[item.group];
+          TileRec& r = trec[qslot];
+          r.c_off      = g.c_off;
+          r.group      = item.group;
+          r.mt         = item.mt;
+          r.nt         = item.nt;
+          r.task_begin = g.task_begin;
+          r.task_end   = g.task_end;
+          int32_t cstr[kMaxModes]; // C block strides (a block holds fewer than 2^31 elements)
+          int32_t sz = 1;
+          for(int i = p.lc.nc - 1; i >= 0; i--) {
+            cstr[i] = sz;
+            sz *= g.cdims[i];
+          }
+          int32_t M = 1, N = 1;
+          for(int j = 0; j < p.lc.nm; j++) {
+            r.mdim[j] = g.cdims[p.lc.m_c[j]];
+            r.mstr[j] = cstr[p.lc.m_c[j]];
+            M *= r.mdim[j];
+          }
+          for(int j = 0; j < p.lc.nn; j++) {
+            r.ndim[j] = g.cdims[p.lc.n_c[j]];
+            r.nstr[j] = cstr[p.lc.n_c[j]];
+            N *= r.ndim[j];
+          }
+          r.M = M;
+          r.N = N;
+          if(g.task_begin < g.task_end) { // the first task; its row exponents and column scales to L1
+            const I8Task   t0 = p.tasks[g.task_begin];
+            r.a_exp0          = t0.a_exp;
+            r.b_exp0          = t0.b_exp;
+            r.st0             = p.tslices[g.task_begin];
+            const int32_t* ea = p.a_exps + t0.a_exp + item.mt * MT;
+            const int32_t* eb = p.b_exps + t0.b_exp + item.nt * NT;
+#pragma unroll
+            for(int o = 0; o < MT; o += 32) asm volatile("prefetch.global.L1 [%0];\n" ::"l"(ea + o));
+            asm volatile("prefetch.global.L1 [%0];\n" ::"l"(ea + MT - 1));
+#pragma unroll
+            for(int o = 0; o < NT; o += 32) asm volatile("prefetch.global.L1 [%0];\n" ::"l"(eb + o));
+            asm volatile("prefetch.global.L1 [%0];\n" ::"l"(eb + NT - 1));
+          }
+        }
+        mbar_arrive(&qfull[qslot]); // (release: the record is visible to the slot's waiters)
         if(++qslot == kQueue) {
           qslot = 0;
           qph ^= 1;
         }
         if(it >= p.nitems) break;
-        const I8Item   item = p.items[it];
-        const DevGroup g    = p.groups[item.group];
         for(int t = g.task_begin; t < g.task_end; t++) {
           const I8Task   tk = p.tasks[t];
           const uint8_t* ga = p.a_slices + tk.a_off + (int64_t) item.mt * tk.nkc * A_BYTES;
@@ -759,15 +820,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       while(true) {
         if(!mbar_wait(&qfull[qslot], qph, p.err, 6)) goto done_mma;
         const int it = qitem[qslot];
+        int       tb = 0, te = 0;
+        if(it >= 0) {
+          tb = trec[qslot].task_begin;
+          te = trec[qslot].task_end;
+        }
         mbar_arrive(&qempty[qslot]);
         if(++qslot == kQueue) {
           qslot = 0;
           qph ^= 1;
         }
         if(it < 0) break;
-        const I8Item   item = p.items[it];
-        const DevGroup g    = p.groups[item.group];
-        for(int t = g.task_begin; t < g.task_end; t++) {
+        for(int t = tb; t < te; t++) {
           const int nkc = p.tasks[t].nkc;
           const int st  = p.tslices[t];
           for(int kc = 0; kc < nkc; kc++) {
@@ -823,7 +887,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
     int           qslot = 0;
     uint32_t      qph   = 0;
     for(;; icount++) {
-      int it;
+      int it, rslot;
       {
         // the epilogue threads agree on a timeout, so none is left in a barrier
         const bool got = mbar_wait(&qfull[qslot], qph, p.err, 7);
@@ -834,16 +898,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                      : "r"((uint32_t) got), "n"(NEPI)
                      : "memory");
         if(anyfail) break;
-        it = qitem[qslot];
-        mbar_arrive(&qempty[qslot]);
+        it    = qitem[qslot];
+        rslot = qslot;
         if(++qslot == kQueue) {
           qslot = 0;
           qph ^= 1;
         }
       }
-      if(it < 0) break;
-      const I8Item   item = p.items[it];
-      const DevGroup g    = p.groups[item.group];
+      if(it < 0) {
+        mbar_arrive(&qempty[rslot]);
+        break;
+      }
+      // the tile's record: read in shared memory while the C addressing is set up, then
+      // the slot goes back to the producer
+      const TileRec& rec = trec[rslot];
+      const int      imt = rec.mt, int_ = rec.nt, igroup = rec.group, tb = rec.task_begin, te = rec.task_end;
 #pragma unroll
       for(int x = 0; x < NH; x++) racc[x] = 0.0;
       bool ok = true;
@@ -856,36 +925,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       int32_t* nof    = noff + (icount & 1) * NT;
       double*  dco    = dcol + (icount & 1) * NT;
       {
-        int64_t cstr[kMaxModes];
-        int64_t s = 1;
-        for(int i = p.lc.nc - 1; i >= 0; i--) {
-          cstr[i] = s;
-          s *= g.cdims[i];
-        }
-        int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
-        int32_t M = 1, N = 1;
-        for(int j = 0; j < p.lc.nm; j++) {
-          mdim[j] = g.cdims[p.lc.m_c[j]];
-          mstr[j] = (int32_t) cstr[p.lc.m_c[j]];
-          M *= mdim[j];
-        }
-        for(int j = 0; j < p.lc.nn; j++) {
-          ndim[j] = g.cdims[p.lc.n_c[j]];
-          nstr[j] = (int32_t) cstr[p.lc.n_c[j]];
-          N *= ndim[j];
-        }
-        const int      m  = item.mt * MT + row;
-        const int32_t* es = p.en.estart + (int64_t) item.group * p.lc.nc;
-        if(m < M) {
-          rowoff = g.c_off + decomp(m, p.lc.nm, mdim, mstr);
-          if constexpr(EN) drow = energy_part(m, p.lc.nm, mdim, p.lc.m_c, p.en, es);
+        const int      m  = imt * MT + row;
+        const int32_t* es = p.en.estart + (int64_t) igroup * p.lc.nc;
+        if(m < rec.M) {
+          rowoff = rec.c_off + decomp(m, p.lc.nm, rec.mdim, rec.mstr);
+          if constexpr(EN) drow = energy_part(m, p.lc.nm, rec.mdim, p.lc.m_c, p.en, es);
         }
         if(et < NT) {
-          const int n = item.nt * NT + et;
-          nof[et]     = n < N ? decomp(n, p.lc.nn, ndim, nstr) : -1;
-          if constexpr(EN) dco[et] = n < N ? energy_part(n, p.lc.nn, ndim, p.lc.n_c, p.en, es) : 1.0;
+          const int n = int_ * NT + et;
+          nof[et]     = n < rec.N ? decomp(n, p.lc.nn, rec.ndim, rec.nstr) : -1;
+          if constexpr(EN) dco[et] = n < rec.N ? energy_part(n, p.lc.nn, rec.ndim, p.lc.n_c, p.en, es) : 1.0;
         }
       }
+      mbar_arrive(&qempty[rslot]);
       if constexpr(EN) {
         // the tile's C values go to L2 while its MMAs run (the energy epilogue reads them
         // once they are done): the epilogue warps publish the column offsets first
@@ -899,17 +951,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           }
         }
       }
-      for(int t = g.task_begin; t < g.task_end; t++, tcount++) {
+      for(int t = tb; t < te; t++, tcount++) {
         // The task's metadata and column scales 2^(e_col - 7) are fetched before its
         // accumulators are complete, so their latency overlaps the task's MMAs.  The
         // scales alternate between two buffers: the readers of this buffer (two tasks
         // back) all passed the previous task's barrier below.
         const I8Task tk  = p.tasks[t];
         const int    st  = p.tslices[t];
-        const int    er  = __ldg(p.a_exps + tk.a_exp + item.mt * MT + row);
+        const int    er  = __ldg(p.a_exps + tk.a_exp + imt * MT + row);
         double*      scb = sc + (tcount & 1) * NT;
         constexpr int off = BF ? 0 : 7; // digit weights: 2^(e - 7 - 8d) (INT8), 2^e (BF16 pieces)
-        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.b_exps + tk.b_exp + item.nt * NT + et) - off);
+        if(et < NT) scb[et] = ldexp(1.0, __ldg(p.b_exps + tk.b_exp + int_ * NT + et) - off);
         // the epilogue threads agree on a timeout, so none is left in a barrier; the
         // barrier also publishes the scales
         const bool     waited = mbar_wait(tfull, tphase, p.err, 4);
