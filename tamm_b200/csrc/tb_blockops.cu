@@ -883,10 +883,17 @@ __global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, cons
                                                     double* __restrict__ part) {
   __shared__ double drow[kDenRows];
   __shared__ double dcol[kDenCols];
+  __shared__ double s_sg[kMaxModes];
   constexpr int     U    = 8; // loads in flight per thread
   const int         tid  = threadIdx.x;
   const int         last = nmodes - 1;
   double            s    = 0.0;
+  // the signs go to shared memory by static indices, and the blocks' fields are read
+  // through a pointer: indexing a copy of either by a runtime mode would put it in
+  // local memory (published by the first barrier of the unit loop)
+#pragma unroll
+  for(int m = 0; m < kMaxModes; m++)
+    if(tid == m) s_sg[m] = sg.s[m];
   // one element: its value(s) and its denominator
   auto elem = [&](int64_t i, double v, double w, double D) {
     if constexpr(ENERGY) s += v * v * recip_nr(D);
@@ -900,27 +907,27 @@ __global__ void __launch_bounds__(kThreads) k_denom(double* __restrict__ t, cons
     }
   };
   for(int ui = blockIdx.x; ui < nunits; ui += gridDim.x) {
-    const DenomUnit  u    = units[ui];
-    const DenomBlock b    = blocks[u.block];
-    const int32_t    nc   = (int32_t) b.dims[last];
-    const bool       tab  = nc <= kDenCols;
-    const double*    el   = eps + b.first[last];
-    const double     slst = sg.s[last];
+    const DenomUnit                u  = units[ui];
+    const DenomBlock* __restrict__ bp = blocks + u.block;
+    const int32_t                  nc = (int32_t) bp->dims[last];
+    const bool                     tab = nc <= kDenCols;
+    const double*                  el  = eps + bp->first[last];
     __syncthreads(); // the previous unit is done with drow / dcol
+    const double slst = s_sg[last];
     if(tab)
       for(int c = tid; c < nc; c += kThreads) dcol[c] = slst * __ldg(el + c);
     for(int i = tid; i < u.rows; i += kThreads) {
       int32_t x = (int32_t) (u.r0 + i); // a block holds fewer than 2^31 elements
       double  d = 0.0;
       for(int m = last - 1; m >= 0; m--) {
-        const int32_t n = (int32_t) b.dims[m], q = x / n;
-        d += sg.s[m] * __ldg(eps + b.first[m] + (x - q * n));
+        const int32_t n = (int32_t) bp->dims[m], q = x / n;
+        d += s_sg[m] * __ldg(eps + bp->first[m] + (x - q * n));
         x = q;
       }
       drow[i] = d;
     }
     __syncthreads();
-    const int64_t base = b.off + u.r0 * (int64_t) nc;
+    const int64_t base = bp->off + u.r0 * (int64_t) nc;
     if(nc <= kThreads) { // fixed column per thread, P rows per pass of A elements
       const int P = kThreads / nc, A = P * nc;
       if(tid < A) {
