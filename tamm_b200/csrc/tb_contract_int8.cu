@@ -1092,15 +1092,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         if(!(xpose_fits<S, NT>() && p.xpose) && rowoff >= 0) {
           const double* crow = p.C + rowoff;
 #pragma unroll
-          for(int x0 = 0; x0 < NH; x0 += 8) { // eight loads in flight, then their sums
-            double cv[8];
+          constexpr int LB = NH % 8 == 0 ? 8 : 4; // loads in flight per batch
+          static_assert(NH % LB == 0, "energy loads in whole batches of columns");
+          for(int x0 = 0; x0 < NH; x0 += LB) { // a batch of loads in flight, then their sums
+            double cv[LB];
 #pragma unroll
-            for(int j = 0; j < 8; j++) {
+            for(int j = 0; j < LB; j++) {
               const int o = nof[col0 + x0 + j];
               cv[j]       = o >= 0 ? __ldcs(crow + o) : 0.0;
             }
 #pragma unroll
-            for(int j = 0; j < 8; j++)
+            for(int j = 0; j < LB; j++)
               if(nof[col0 + x0 + j] >= 0) {
                 const double w = cv[j] + p.alpha * racc[x0 + j];
                 e              = fma(w * w, recip_nr(drow + dco[col0 + x0 + j]), e);
