@@ -675,6 +675,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr uint32_t A_BYTES = S * MT * KC, B_BYTES = S * NT * KC, STAGE = A_BYTES + B_BYTES;
   constexpr int      kStack  = 256 / NT; // B digits per MMA (UMMA N <= 256)
+  static_assert(kStack >= 3, "a drain group's three B digits fit one MMA");
   constexpr int      STAGES  = stages<S, NT>();
   static_assert(STAGES >= 2, "two pipeline stages at least");
   uint64_t*          full   = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE);
@@ -840,28 +841,49 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
             const uint32_t a0 = smem_u32(smem + stage * STAGE), b0 = a0 + A_BYTES;
             // A digit i times the stacked B digits j0 .. j0 + nd - 1 in one MMA of N =
             // nd * NT: it adds into the adjacent diagonals i + j0 .. i + j0 + nd - 1
-            int waited = 0; // diagonals taken back from the epilogue (first K step)
+            if(kc == 0) {
+              // First K step of a task: the previous task's diagonals must have been read
+              // out.  The products go by the epilogue's drain groups of three diagonals
+              // (the same S(S+1)/2 products in as many MMAs), so those into diagonals 0-2
+              // start as soon as the epilogue has read the first group; in each group the
+              // A digit 0 product comes first and overwrites, the others accumulate.
+              int waited = 0;
 #pragma unroll
-            for(int i = 0; i < S; i++) {
-              if(i >= st) break;
-              const uint64_t ad = umma_desc_kmajor(a0 + i * MT * 16, S * MT * 16, 128);
+              for(int g0 = 0; g0 < S; g0 += 3) {
+                const int gl = S - g0 < 3 ? S - g0 : 3;
+                for(; waited < g0 + gl; waited++) {
+                  if(!mbar_wait(&tempty[waited], tphase ^ 1, p.err, 2)) goto done_mma;
+                  tc_fence_after();
+                }
 #pragma unroll
-              for(int j0 = 0; j0 < S; j0 += kStack) {
-                if(j0 >= st - i) break;
-                const int nd = min(kStack, st - i - j0);
-                if(kc == 0) // the previous task's diagonals must have been read out
-                  for(; waited <= i + j0 + nd - 1; waited++) {
-                    if(!mbar_wait(&tempty[waited], tphase ^ 1, p.err, 2)) goto done_mma;
-                    tc_fence_after();
-                  }
-                const uint64_t bd = umma_desc_kmajor(b0 + j0 * NT * 16, S * NT * 16, 128);
-                if constexpr(BF) mma_f16(tmem + (i + j0) * NT, ad, bd, idesc_bf16(MT, nd * NT), kc > 0 || i > 0);
-                else mma_i8(tmem + (i + j0) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), kc > 0 || i > 0);
+                for(int i = 0; i < S; i++) {
+                  if(i >= st || i > g0 + gl - 1) break;
+                  const int jlo = g0 - i > 0 ? g0 - i : 0;
+                  const int jhi = min(g0 + gl - 1 - i, st - 1 - i);
+                  if(jlo > jhi) continue;
+                  const int      nd = jhi - jlo + 1; // <= 3 <= kStack
+                  const uint64_t ad = umma_desc_kmajor(a0 + i * MT * 16, S * MT * 16, 128);
+                  const uint64_t bd = umma_desc_kmajor(b0 + jlo * NT * 16, S * NT * 16, 128);
+                  if constexpr(BF) mma_f16(tmem + (i + jlo) * NT, ad, bd, idesc_bf16(MT, nd * NT), i > 0);
+                  else mma_i8(tmem + (i + jlo) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), i > 0);
+                }
               }
             }
-            if(kc == 0) // keep the unused diagonals' barriers in phase
-              for(; waited < S; waited++)
-                if(!mbar_wait(&tempty[waited], tphase ^ 1, p.err, 2)) goto done_mma;
+            else {
+#pragma unroll
+              for(int i = 0; i < S; i++) {
+                if(i >= st) break;
+                const uint64_t ad = umma_desc_kmajor(a0 + i * MT * 16, S * MT * 16, 128);
+#pragma unroll
+                for(int j0 = 0; j0 < S; j0 += kStack) {
+                  if(j0 >= st - i) break;
+                  const int      nd = min(kStack, st - i - j0);
+                  const uint64_t bd = umma_desc_kmajor(b0 + j0 * NT * 16, S * NT * 16, 128);
+                  if constexpr(BF) mma_f16(tmem + (i + j0) * NT, ad, bd, idesc_bf16(MT, nd * NT), true);
+                  else mma_i8(tmem + (i + j0) * NT, ad, bd, idesc_i8(MT, nd * NT, true, true), true);
+                }
+              }
+            }
             umma_commit(&empty[stage]); // stage free once these MMAs have read it
             if(++stage == STAGES) {
               stage = 0;

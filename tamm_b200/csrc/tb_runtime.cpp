@@ -20,7 +20,17 @@ Arena::Arena(int device, int64_t bytes): device_(device) {
   TB_EXPECTS(bytes > 0, "arena size must be positive");
   capacity_ = (bytes + 255) & ~int64_t(255);
   TB_CUDA(cudaMalloc(reinterpret_cast<void**>(&base_), (size_t) capacity_));
-  free_[0] = capacity_;
+  add_free(0, capacity_);
+}
+
+void Arena::add_free(int64_t off, int64_t size) {
+  free_[off] = size;
+  by_size_.insert({size, off});
+}
+
+void Arena::drop_free(std::map<int64_t, int64_t>::iterator it) {
+  by_size_.erase({it->second, it->first});
+  free_.erase(it);
 }
 
 Arena::~Arena() {
@@ -36,18 +46,16 @@ Arena::~Arena() {
 void* Arena::allocate(int64_t bytes) {
   if(bytes <= 0) bytes = 1;
   const int64_t need = (bytes + 255) & ~int64_t(255);
-  auto          best = free_.end();
-  for(auto it = free_.begin(); it != free_.end(); ++it) // best fit
-    if(it->second >= need && (best == free_.end() || it->second < best->second)) best = it;
-  if(best == free_.end()) {
+  const auto    fit  = by_size_.lower_bound({need, int64_t(0)}); // best fit: smallest block that holds it
+  if(fit == by_size_.end()) {
     std::ostringstream os;
     os << "device arena exhausted: need " << need << " bytes, " << (capacity_ - used_)
        << " free of " << capacity_ << " (fragmented)";
     fail(TB_ERR_NO_MEMORY, os.str());
   }
-  const int64_t off = best->first, sz = best->second;
-  free_.erase(best);
-  if(sz > need) free_[off + need] = sz - need;
+  const int64_t off = fit->second, sz = fit->first;
+  drop_free(free_.find(off));
+  if(sz > need) add_free(off + need, sz - need);
   inuse_[off] = need;
   used_ += need;
   peak_ = std::max(peak_, used_);
@@ -66,17 +74,19 @@ void Arena::deallocate(void* p) {
   auto    nx    = free_.lower_bound(off); // coalesce with neighbours
   if(nx != free_.end() && nx->first == off + sz) {
     sz += nx->second;
-    nx = free_.erase(nx);
+    auto after = std::next(nx);
+    drop_free(nx);
+    nx = after;
   }
   if(nx != free_.begin()) {
     auto pv = std::prev(nx);
     if(pv->first + pv->second == start) {
       start = pv->first;
       sz += pv->second;
-      free_.erase(pv);
+      drop_free(pv);
     }
   }
-  free_[start] = sz;
+  add_free(start, sz);
 }
 
 void* Scratch::get(int64_t bytes) {

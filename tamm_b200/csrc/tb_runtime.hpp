@@ -8,6 +8,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <utility>
 #include <vector>
@@ -41,6 +42,11 @@ private:
   int64_t                    peak_     = 0;
   std::map<int64_t, int64_t> free_;  // offset -> size
   std::map<int64_t, int64_t> inuse_; // offset -> size
+  // the free blocks again, ordered by (size, offset): best fit in O(log n), ties to the
+  // lowest offset
+  std::set<std::pair<int64_t, int64_t>> by_size_;
+  void                                  add_free(int64_t off, int64_t size);
+  void                                  drop_free(std::map<int64_t, int64_t>::iterator it);
 };
 
 struct Ctx {

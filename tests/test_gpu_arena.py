@@ -24,3 +24,33 @@ def test_alloc_free_accounting(ec):
     with pytest.raises(tb.TambError) as err:
         ec.alloc(cap + 256)
     assert err.value.code == A.TB_ERR_NO_MEMORY
+
+
+def test_best_fit_and_coalescing():
+    """On a fresh 1 MiB arena: a freed 512-byte gap is preferred to a larger free block
+    for a 256-byte request (best fit, lowest offset among equal sizes), and freeing every
+    block coalesces the arena back into one block that a full-size request takes."""
+    ec = tb.ExecutionContext(0, 1 << 20)
+    try:
+        used0, _, cap = ec.arena_info()  # (anything the context holds itself sits below)
+        a = ec.alloc(256)
+        b = ec.alloc(512)
+        c = ec.alloc(256)
+        d = ec.alloc(1024)
+        e = ec.alloc(256)
+        assert [a, b, c, d, e] == [a, a + 256, a + 768, a + 1024, a + 2048]
+        ec.free(b).free(d)                      # gaps of 512 and 1024 bytes, then the tail
+        x = ec.alloc(256)
+        assert x == b                           # the smallest gap that holds it
+        y = ec.alloc(1024)
+        assert y == d                           # an exact fit ahead of the tail
+        z = ec.alloc(256)
+        assert z == b + 256                     # the rest of the first gap
+        for p in (a, c, e, x, y, z):
+            ec.free(p)
+        assert ec.arena_info()[0] == used0
+        whole = ec.alloc(cap - used0)           # one block again: every neighbour merged
+        assert whole == a
+        ec.free(whole)
+    finally:
+        ec.close()
