@@ -1048,6 +1048,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                 if(gl > 1 && g0 + 1 < st) tmem_ld_cols<CH>(tq + (g0 + 1) * NT + c0, v1);
                 if(gl > 2 && g0 + 2 < st) tmem_ld_cols<CH>(tq + (g0 + 2) * NT + c0, v2);
                 tmem_wait_ld();
+                if(c0 + CH >= NH) { // the group's last columns are in registers: its TMEM
+                  tc_fence_before(); // goes back to the MMA issuer before this chunk's math
+                  for(int d = g0; d < g0 + gl; d++) mbar_arrive(&tempty[d]);
+                }
                 const bool has1 = gl > 1 && g0 + 1 < st, has2 = gl > 2 && g0 + 2 < st;
                 if(fast) {
 #pragma unroll
@@ -1068,9 +1072,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
                   }
                 }
               }
-              tc_fence_before();
             }
-            for(int d = g0; d < g0 + gl; d++) mbar_arrive(&tempty[d]);
+            else
+              for(int d = g0; d < g0 + gl; d++) mbar_arrive(&tempty[d]);
           }
         }
       }
