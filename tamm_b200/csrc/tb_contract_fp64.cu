@@ -50,6 +50,11 @@ struct Smem {
   int32_t   colC[BN];
   double    rowD[BM]; // energy epilogue: the rows' and columns' parts of the denominators
   double    colD[BN];
+  // the output block's geometry, worked out by one thread: extents and C strides of the
+  // row / column labels, batch indices of the tile, C offset of its batch
+  int32_t   gmdim[kMaxClass], gmstr[kMaxClass], gndim[kMaxClass], gnstr[kMaxClass], gbidx[kMaxClass];
+  int32_t   gM, gN;
+  int64_t   gcbase;
   TaskInfo  ti[2];
   ChunkDesc desc[NSLOT];
 };
@@ -122,45 +127,50 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
   const DevGroup      g   = p.groups[it.group];
   const int           tb  = g.task_begin, te = g.task_end;
 
-  // ---- output block geometry (uniform) ----
-  int64_t cstr[kMaxModes];
-  strides_of(g.cdims, lc.nc, cstr);
-  int32_t mdim[kMaxClass], ndim[kMaxClass], mstrC[kMaxClass], nstrC[kMaxClass];
-  int32_t Mtot = 1, Ntot = 1;
-  for(int j = 0; j < lc.nm; j++) {
-    mdim[j]  = g.cdims[lc.m_c[j]];
-    mstrC[j] = (int32_t) cstr[lc.m_c[j]];
-    Mtot *= mdim[j];
-  }
-  for(int j = 0; j < lc.nn; j++) {
-    ndim[j]  = g.cdims[lc.n_c[j]];
-    nstrC[j] = (int32_t) cstr[lc.n_c[j]];
-    Ntot *= ndim[j];
-  }
-  int32_t bidx[kMaxClass];
-  {
-    int32_t x = it.batch;
-    for(int j = lc.nbatch - 1; j >= 0; j--) {
-      int32_t d = g.cdims[lc.batch_c[j]];
-      bidx[j]   = x % d;
-      x /= d;
+  // ---- output block geometry (uniform): one thread works it out into shared memory
+  // (per-thread copies indexed by runtime label positions would live in local memory) ----
+  if(tid == 0) {
+    int64_t cstr[kMaxModes];
+    strides_of(g.cdims, lc.nc, cstr);
+    int32_t M = 1, N = 1;
+    for(int j = 0; j < lc.nm; j++) {
+      s.gmdim[j] = g.cdims[lc.m_c[j]];
+      s.gmstr[j] = (int32_t) cstr[lc.m_c[j]];
+      M *= s.gmdim[j];
     }
+    for(int j = 0; j < lc.nn; j++) {
+      s.gndim[j] = g.cdims[lc.n_c[j]];
+      s.gnstr[j] = (int32_t) cstr[lc.n_c[j]];
+      N *= s.gndim[j];
+    }
+    int32_t x  = it.batch;
+    int64_t cb = g.c_off;
+    for(int j = lc.nbatch - 1; j >= 0; j--) {
+      const int32_t d = g.cdims[lc.batch_c[j]];
+      s.gbidx[j]      = x % d;
+      x /= d;
+      cb += s.gbidx[j] * cstr[lc.batch_c[j]];
+    }
+    s.gM     = M;
+    s.gN     = N;
+    s.gcbase = cb;
   }
-  int64_t c_base = g.c_off;
-  for(int j = 0; j < lc.nbatch; j++) c_base += bidx[j] * cstr[lc.batch_c[j]];
+  __syncthreads();
+  const int32_t Mtot = s.gM, Ntot = s.gN;
+  const int64_t c_base = s.gcbase;
   for(int m = tid; m < BM; m += NTHREADS)
-    s.rowC[m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, mdim, mstrC) : 0;
+    s.rowC[m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, s.gmdim, s.gmstr) : 0;
   for(int n = tid; n < BN; n += NTHREADS)
-    s.colC[n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, ndim, nstrC) : 0;
+    s.colC[n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, s.gndim, s.gnstr) : 0;
   if(p.energy) { // batch labels' part folded into the rows'
     const int32_t* es = p.en.estart + (int64_t) it.group * lc.nc;
     double         db = 0.0;
     for(int j = 0; j < lc.nbatch; j++)
-      db += p.en.sg[lc.batch_c[j]] * __ldg(p.en.eps + es[lc.batch_c[j]] + bidx[j]);
+      db += p.en.sg[lc.batch_c[j]] * __ldg(p.en.eps + es[lc.batch_c[j]] + s.gbidx[j]);
     for(int m = tid; m < BM; m += NTHREADS)
-      s.rowD[m] = (it.m0 + m < Mtot) ? db + energy_part(it.m0 + m, lc.nm, mdim, lc.m_c, p.en, es) : 0.0;
+      s.rowD[m] = (it.m0 + m < Mtot) ? db + energy_part(it.m0 + m, lc.nm, s.gmdim, lc.m_c, p.en, es) : 0.0;
     for(int n = tid; n < BN; n += NTHREADS)
-      s.colD[n] = (it.n0 + n < Ntot) ? energy_part(it.n0 + n, lc.nn, ndim, lc.n_c, p.en, es) : 1.0;
+      s.colD[n] = (it.n0 + n < Ntot) ? energy_part(it.n0 + n, lc.nn, s.gndim, lc.n_c, p.en, es) : 1.0;
   }
 
   // ---- chunk iterator over (task, reduction step, k0), uniform across the CTA ----
@@ -221,8 +231,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
         for(int j = 0; j < lc.nn; j++) ti.nstrB[j] = (int32_t) bstr[lc.n_b[j]];
         int64_t ab = tk.a_off, bb = tk.b_off;
         for(int j = 0; j < lc.nbatch; j++) {
-          ab += bidx[j] * astr[lc.batch_a[j]];
-          bb += bidx[j] * bstr[lc.batch_b[j]];
+          ab += s.gbidx[j] * astr[lc.batch_a[j]];
+          bb += s.gbidx[j] * bstr[lc.batch_b[j]];
         }
         ti.a_blk = ab;
         ti.b_blk = bb;
@@ -232,9 +242,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_contract_fp64(const Params p) {
       cur_ARBR = ti.ARBR;
       cur_BR   = ti.BR;
       for(int m = tid; m < BM; m += NTHREADS)
-        s.rowA[buf][m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, mdim, ti.mstrA) : 0;
+        s.rowA[buf][m] = (it.m0 + m < Mtot) ? decompose(it.m0 + m, lc.nm, s.gmdim, ti.mstrA) : 0;
       for(int n = tid; n < BN; n += NTHREADS)
-        s.colB[buf][n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, ndim, ti.nstrB) : 0;
+        s.colB[buf][n] = (it.n0 + n < Ntot) ? decompose(it.n0 + n, lc.nn, s.gndim, ti.nstrB) : 0;
     }
     if(tid == 0) {
       const int ar = cur_s / cur_BR, br = cur_s - (cur_s / cur_BR) * cur_BR;
