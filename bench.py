@@ -25,7 +25,8 @@ After the ladder, the full doubles-residual iteration (O=60, V=480, tiles U{20..
 seed 2; one CUDA graph per mode) is timed in FP64, autotuned split-INT8 and BF16x3 and
 reported under "ccsd_iteration" with a sampled reference-CPU baseline (--no-ccsd skips
 it); on one GPU the energy gradient (O=30, V=240) and sampled steps of the streamed
-triples energy (O=50, V=500) follow under "adjoint" and "triples" (--no-adjoint,
+triples energy (O=50, V=500; each step timed as a CUDA graph replay, the streamed
+run's window beside it) follow under "adjoint" and "triples" (--no-adjoint,
 --no-triples skip them).
 """
 from __future__ import annotations
@@ -309,7 +310,11 @@ def measure_adjoint(ec, torch):
 def measure_triples(ec, torch, nsteps):
     """Sampled steps of the streamed triples energy at O=50, V=500, tile 40 (j blocks of
     2, the summed d one tile per spin block), FP64 and split-INT8 (integrals read-only,
-    their digits kept): device time of the sample, FP64-equivalent TFLOP/s."""
+    their digits kept): device time of the sample (each step's ops captured as one CUDA
+    graph and replayed, as the doubles iteration is timed), FP64-equivalent TFLOP/s; the
+    streamed run's window (steps enqueued back to back, each step's host work - new W
+    tensor, work lists, denominator tables - overlapping the previous step's device
+    work) beside it as stream_ms."""
     import tamm_b200 as tb
     from tamm_b200 import triples as T3
     P = T3.build(25, 250, tile=40, jtile=2, dtile=0, seed=4, ec=ec)
@@ -326,11 +331,29 @@ def measure_triples(ec, torch, nsteps):
         T3.energy(P, sample[:1], sch)  # warm-up
         e, fl, ms = T3.energy(P, sample, sch)
         es[name] = e
-        out[name] = {"energy_sample": e, "flops_sample": fl, "ms": ms, "tflops": fl / ms / 1e9,
+        stream = torch.cuda.ExternalStream(ec.stream)
+        gms = 0.0
+        for (i, j) in sample:  # device time per step: its ops as one graph, replayed twice
+            sg = tb.Scheduler(ec)
+            Wt, _ = T3.queue_pair(P, sg, i, j)
+            g = sg.graph()  # runs the step once, then captures it
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(2):
+                g.launch()
+            e1.record(stream)
+            g.sync()
+            gms += e0.elapsed_time(e1) / 2
+            del g
+            sg.release()
+            Wt.deallocate()
+        out[name] = {"energy_sample": e, "flops_sample": fl, "ms": gms, "tflops": fl / gms / 1e9,
+                     "stream_ms": ms, "stream_tflops": fl / ms / 1e9,
                      "digit_cache_bytes": ec.digit_cache_info()[0]}
     ec.set_precision(tb.Precision.FP64)
     ec.set_digit_cache(0)
     out["speedup_int8_vs_fp64"] = out["fp64"]["ms"] / out["int8"]["ms"]
+    out["speedup_int8_vs_fp64_stream"] = out["fp64"]["stream_ms"] / out["int8"]["stream_ms"]
     out["int8_vs_fp64_energy_rel_err"] = abs(es["int8"] - es["fp64"]) / abs(es["fp64"])
     for t in P.T.values():
         t.set_read_only(False)
