@@ -79,16 +79,16 @@ struct I8Item {
 };
 
 // One output tile as the producer hands it to the MMA issuer and the epilogue through a
-// shared-memory queue slot: its item, group and first task, and the row / column
-// geometry of its C block (extents and strides of the row and column labels), worked
-// out once per tile by the producer, off the consumers' critical path, and read by the
-// epilogue threads from shared memory (indexing per-thread arrays by runtime label
-// positions would put them in local memory).
+// shared-memory queue slot: its item and group, and the row / column geometry of its C
+// block (extents and strides of the row and column labels), worked out once per tile by
+// the producer, off the consumers' critical path, and read by the epilogue threads from
+// shared memory (indexing per-thread arrays by runtime label positions would put them
+// in local memory).
 struct TileRec {
   int64_t c_off;
-  int32_t group, mt, nt, task_begin, task_end, M, N, a_exp0, b_exp0, st0;
+  int32_t group, mt, nt, task_begin, task_end, M, N;
   int32_t mdim[kMaxClass], mstr[kMaxClass], ndim[kMaxClass], nstr[kMaxClass];
-  int32_t pad[4];
+  int32_t pad[7];
 };
 static_assert(sizeof(TileRec) == 128, "tile record size");
 
@@ -759,11 +759,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           }
           r.M = M;
           r.N = N;
-          if(g.task_begin < g.task_end) { // the first task; its row exponents and column scales to L1
+          if(g.task_begin < g.task_end) { // the first task's row exponents and column scales, to L1
             const I8Task   t0 = p.tasks[g.task_begin];
-            r.a_exp0          = t0.a_exp;
-            r.b_exp0          = t0.b_exp;
-            r.st0             = p.tslices[g.task_begin];
             const int32_t* ea = p.a_exps + t0.a_exp + item.mt * MT;
             const int32_t* eb = p.b_exps + t0.b_exp + item.nt * NT;
 #pragma unroll
