@@ -1114,9 +1114,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
         if(!(xpose_fits<S, NT>() && p.xpose) && rowoff >= 0) {
           const double* crow = p.C + rowoff;
-#pragma unroll
           constexpr int LB = NH % 8 == 0 ? 8 : 4; // loads in flight per batch
           static_assert(NH % LB == 0, "energy loads in whole batches of columns");
+#pragma unroll
           for(int x0 = 0; x0 < NH; x0 += LB) { // a batch of loads in flight, then their sums
             double cv[LB];
 #pragma unroll
