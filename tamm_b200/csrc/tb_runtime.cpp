@@ -875,6 +875,7 @@ void Sched::run(Op& op) {
   op.plan->nslices    = ctx->nslices;
   op.plan->tile_n     = 0;
   op.plan->store      = op.store;
+  op.plan->energy     = nullptr; // (plans are shared by signature: nothing of an earlier op stays)
   if(op.energy) { // the energy epilogue keeps the context's precision (no autotuning)
     if(!op.espec) op.espec = build_energy(op, op.plan->lc, ctx);
     op.plan->energy       = &op.espec->args;
