@@ -104,11 +104,12 @@ int tb_axpby(double alpha, const double* x, double beta, double* y, int64_t n, v
  * TB_ERR_INVALID and a message giving the size.  Labels as in tb_block_multiply
  * (plain contractions only: no Hadamard or one-sided reduction labels); nslices 0
  * picks the digit count for a 1e-11 target, 3..8 forces it.  The first call on a
- * device looks up the array's device address for that device, once; make that first
- * call before any stream capture on the device.  Every call reuses the same array and leaves its contents
- * behind; each call resets what it needs to start from a known value, and calls
- * that overlap on the GPU (other streams, other threads) race on the array.  The
- * call returns after the stream has drained. */
+ * device looks up the array's device address for that device, once.  Every call
+ * reuses the same array and leaves its contents behind; each call resets what it
+ * needs to start from a known value, and calls that overlap on the GPU (other
+ * streams, other threads) race on the array.  The call reads its status back and
+ * returns after the stream has drained, so it cannot be captured into a CUDA graph
+ * (a call on a capturing stream returns TB_ERR_INVALID before enqueuing anything). */
 int tb_block_multiply_int8_noalloc(double alpha, const double* a, const int64_t* adims,
                                    const int* alabels, int na, const double* b,
                                    const int64_t* bdims, const int* blabels, int nb, double* c,

@@ -2015,6 +2015,14 @@ extern "C" int tb_block_multiply_int8_noalloc(double alpha, const double* a, con
     TB_EXPECTS((na == 0 || (adims && alabels)) && (nb == 0 || (bdims && blabels)) && (nc == 0 || (cdims && clabels)),
                "dims/labels arrays must be given for every non-scalar operand");
     TB_EXPECTS(nslices == 0 || (nslices >= 3 && nslices <= 8), "nslices must be 0 (target 1e-11) or 3..8");
+    {
+      // the call drains the stream to read its status back: refused before any work
+      // is enqueued while the stream is capturing, so the capture itself stays valid
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      TB_CUDA(cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs));
+      TB_EXPECTS(cs == cudaStreamCaptureStatusNone,
+                 "tb_block_multiply_int8_noalloc cannot be captured into a CUDA graph (it synchronises its stream)");
+    }
     const LabelClasses lc = classify(clabels, nc, alabels, na, blabels, nb);
     if(lc.nbatch > 0 || lc.nar > 0 || lc.nbr > 0 || lc.nk == 0)
       fail(TB_ERR_NOT_IMPLEMENTED, "the allocation-free split-INT8 entry point takes plain contractions only "

@@ -106,3 +106,25 @@ def test_no_alloc_rejects_triples_beyond_the_static_scratch():
                                           None)
     assert rc == A.TB_ERR_INVALID
     assert "64 MiB" in A.last_error()
+
+
+def test_no_alloc_refuses_a_capturing_stream():
+    # the call drains its stream, so under capture it must refuse before enqueuing
+    # anything: the capture stays valid and C is left as it was
+    a, b, c0, al, bl, cl = _case(dict(a=24, b=31, c=29, d=37, i=20, j=20), ("abij", "abcd", "cdij"), 44)
+    (da, db, dc), k = _args(a, al, b, bl, c0, cl)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rc = A.lib().tb_block_multiply_int8_noalloc(
+            0.75, da.data_ptr(), k[0].ctypes.data_as(A.i64p), k[1].ctypes.data_as(A.ip), a.ndim, db.data_ptr(),
+            k[2].ctypes.data_as(A.i64p), k[3].ctypes.data_as(A.ip), b.ndim, dc.data_ptr(),
+            k[4].ctypes.data_as(A.i64p), k[5].ctypes.data_as(A.ip), c0.ndim, 0,
+            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        dc.add_(0.0)  # the capture holds one node of its own
+    assert rc == A.TB_ERR_INVALID
+    assert "cannot be captured" in A.last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(dc.cpu().numpy().reshape(c0.shape), c0)
+    del g
