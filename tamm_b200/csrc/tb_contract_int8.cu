@@ -47,7 +47,7 @@ using namespace sm100;
 constexpr int MT = 128; // UMMA M: output rows of a tile
 constexpr int KC = 32;  // bytes of K per pipeline stage (one INT8 MMA k-step)
 constexpr int kMaxSmem = 227 * 1024; // dynamic shared memory per CTA on sm_100
-constexpr int NEPI     = 256;           // epilogue threads (warps 2-9)
+constexpr int NEPI     = 256;           // epilogue threads of the default kernel (warps 2-9)
 constexpr int NTHREADS = 64 + NEPI;     // warp 0 producer, warp 1 MMA issuer, warps 2-9 epilogue
 
 // One operand block to split into digit slices.
@@ -650,11 +650,12 @@ __host__ __device__ constexpr int stages() {
   return (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) < 6 ? (int) ((kMaxSmem - kTail) / stage_bytes<S, NT>()) : 6;
 }
 
-// Epilogue transpose buffer behind the tail, where it fits: per epilogue warp kXCols
-// columns x 32 rows of doubles, rows kXStride apart (34: the transposed reads of a half
-// warp, 8 columns x 2 rows, fall on 16 distinct bank pairs).
-constexpr int kXCols = 8, kXStride = 34;
-constexpr int kXBytes = (NEPI / 32) * kXCols * kXStride * 8;
+// Epilogue transpose buffer behind the tail, where it fits: per epilogue warp XC (8 or
+// 4) columns x 32 rows of doubles, rows kXStride apart (34: the transposed reads of a half
+// warp, 8 columns x 2 rows, fall on 16 distinct bank pairs), 64 columns in all: eight
+// warps of 8 columns, or sixteen of 4.
+constexpr int kXStride = 34;
+constexpr int kXBytes = 64 * kXStride * 8;
 template<int S, int NT>
 __host__ __device__ constexpr bool xpose_fits() {
   return (size_t) stages<S, NT>() * stage_bytes<S, NT>() + kTail + kXBytes <= kMaxSmem;
@@ -669,9 +670,14 @@ constexpr size_t smem_bytes() {
 // diagonals carry the same power of two, 2^(e_row + e_col)).
 // EN: the energy epilogue (p.energy) instead of the C update, in instantiations of its
 // own so that the plain kernels' code is unchanged.
-template<int S, int NT, bool BF, bool EN = false>
-__global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
+// EW: epilogue warps, 8 or 16 (four per TMEM lane quarter, each a quarter of the tile's
+// columns: for contractions whose tiles have little K, where the epilogue bounds the
+// kernel; the threads then get at most 96 registers each).
+template<int S, int NT, bool BF, bool EN = false, int EW = 8>
+__global__ void __launch_bounds__(64 + 32 * EW, 1) k_contract_i8(const I8Params p) {
   static_assert(S * NT <= 512, "TMEM holds 512 columns");
+  static_assert(EW == 8 || (EW == 16 && !EN && !BF), "sixteen epilogue warps: the plain INT8 C update only");
+  constexpr int NE = 32 * EW; // epilogue threads
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr uint32_t A_BYTES = S * MT * KC, B_BYTES = S * NT * KC, STAGE = A_BYTES + B_BYTES;
   constexpr int      kStack  = 256 / NT; // B digits per MMA (UMMA N <= 256)
@@ -704,10 +710,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    for(int d = 0; d < S; d++) mbar_init(&tempty[d], NEPI);
+    for(int d = 0; d < S; d++) mbar_init(&tempty[d], NE);
     for(int i = 0; i < kQueue; i++) {
       mbar_init(&qfull[i], 1);
-      mbar_init(&qempty[i], 1 + NEPI); // the MMA issuer and every epilogue thread
+      mbar_init(&qempty[i], 1 + NE); // the MMA issuer and every epilogue thread
     }
     fence_mbarrier_init();
   }
@@ -896,9 +902,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
   }
   else {
     // ---------------- epilogue: FP64 recombination of the diagonals ----------------
-    // Eight warps: warp w reads TMEM lanes 32 * (w % 4) (its rows) and one half of the
-    // tile's columns, so two warps share every lane quarter.
-    constexpr int NH = NT / 2;
+    // EW warps: warp w reads TMEM lanes 32 * (w % 4) (its rows) and one of EW / 4 equal
+    // column ranges of the tile, so EW / 4 warps share every lane quarter.
+    constexpr int NH = NT / (EW / 4);
+    // transpose width: 8 columns where the buffer holds 8 per warp, else 4
+    constexpr int XC = (NH % 8 == 0 && EW * 8 <= 64) ? 8 : 4;
+    static_assert(EW * XC <= 64 && NH % XC == 0, "transpose buffer");
     const int     q = warp & 3, row = q * 32 + lane, col0 = ((warp - 2) >> 2) * NH;
     const int     et = threadIdx.x - 64; // column whose scale this thread loads
     uint32_t      tphase = 0, tcount = 0, icount = 0;
@@ -914,7 +923,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
                      "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
                      : "=r"(anyfail)
-                     : "r"((uint32_t) got), "n"(NEPI)
+                     : "r"((uint32_t) got), "n"(NE)
                      : "memory");
         if(anyfail) break;
         it    = qitem[qslot];
@@ -960,11 +969,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       if constexpr(EN) {
         // the tile's C values go to L2 while its MMAs run (the energy epilogue reads them
         // once they are done): the epilogue warps publish the column offsets first
-        asm volatile("bar.sync 1, %0;\n" ::"n"(NEPI) : "memory");
+        asm volatile("bar.sync 1, %0;\n" ::"n"(NE) : "memory");
         if(rowoff >= 0) {
           const double* crow = p.C + rowoff;
 #pragma unroll
-          for(int x = 0; x < NH; x += (p.xpose ? kXCols : 1)) { // xpose: a row's columns are contiguous
+          for(int x = 0; x < NH; x += (p.xpose ? XC : 1)) { // xpose: a row's columns are contiguous
             const int o = nof[col0 + x];
             if(o >= 0) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(crow + o));
           }
@@ -988,7 +997,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         asm volatile("{\n\t.reg .pred p, q;\n\tsetp.eq.u32 p, %1, 0;\n\t"
                      "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
                      : "=r"(anyfail)
-                     : "r"((uint32_t) waited), "n"(NEPI)
+                     : "r"((uint32_t) waited), "n"(NE)
                      : "memory");
         if(anyfail) {
           ok = false;
@@ -1028,7 +1037,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
           }
         }
         else {
-          constexpr int  CH = NH >= 24 ? NH / 2 : NH; // columns per TMEM load round
+          // columns per TMEM load round (sixteen warps: narrower rounds, as their threads
+          // hold at most 96 registers: five of the eighteen warps share one sub-partition)
+          constexpr int  CH = EW == 8 ? (NH >= 24 ? NH / 2 : NH) : (NH <= 12 ? NH : NH % 8 == 0 ? 8 : 4);
           static_assert(NH % CH == 0 && CH % 4 == 0, "drain chunking");
           const uint32_t tq = tmem + ((uint32_t) (q * 32) << 16) + col0;
 #pragma unroll
@@ -1082,25 +1093,25 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         // a fixed shuffle tree), so the total does not depend on which CTA took a tile.
         double e = 0.0;
         if constexpr(xpose_fits<S, NT>()) {
-          if(p.xpose) { // C contiguous along the columns: each load covers 4 rows x 8 columns
-            double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * kXCols * kXStride;
-            const int rsub = lane / kXCols, csub = lane % kXCols;
+          if(p.xpose) { // C contiguous along the columns: each load covers 32 / XC rows x XC columns
+            double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * XC * kXStride;
+            const int rsub = lane / XC, csub = lane % XC;
 #pragma unroll 1
-            for(int x0 = 0; x0 < NH; x0 += kXCols) {
+            for(int x0 = 0; x0 < NH; x0 += XC) {
 #pragma unroll
-              for(int j = 0; j < kXCols; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
+              for(int j = 0; j < XC; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
               __syncwarp();
               const int    o  = nof[col0 + x0 + csub];
               const double dc = dco[col0 + x0 + csub];
-              double       cv[kXCols];
+              double       cv[XC];
 #pragma unroll
-              for(int rr = 0; rr < kXCols; rr++) { // the loads first, all in flight
-                const int64_t ro = __shfl_sync(0xffffffffu, rowoff, rr * (32 / kXCols) + rsub);
+              for(int rr = 0; rr < XC; rr++) { // the loads first, all in flight
+                const int64_t ro = __shfl_sync(0xffffffffu, rowoff, rr * (32 / XC) + rsub);
                 cv[rr]           = (ro >= 0 && o >= 0) ? __ldcs(p.C + ro + o) : 0.0;
               }
 #pragma unroll
-              for(int rr = 0; rr < kXCols; rr++) {
-                const int     r  = rr * (32 / kXCols) + rsub;
+              for(int rr = 0; rr < XC; rr++) {
+                const int     r  = rr * (32 / XC) + rsub;
                 const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
                 const double  dr = __shfl_sync(0xffffffffu, drow, r);
                 if(ro >= 0 && o >= 0) {
@@ -1134,7 +1145,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
         }
 #pragma unroll
         for(int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-        if(lane == 0) p.en.part[(int64_t) it * (NEPI / 32) + (warp - 2)] = e;
+        if(lane == 0) p.en.part[(int64_t) it * EW + (warp - 2)] = e;
         continue;
       }
       // C (+)= alpha * result: one reduction per element (c + alpha * r, rounded once,
@@ -1142,22 +1153,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_contract_i8(const I8Params p) {
       // tile), performed at L2, so the epilogue does not wait for C's memory; a plain
       // store for an assignment (p.store).
       // A thread holds one row of the tile; when C is contiguous along the columns
-      // instead, the warp passes its values through shared memory kXCols columns at a
-      // time so that each reduction instruction covers 4 rows x 8 adjacent columns.
+      // instead, the warp passes its values through shared memory XC columns at a
+      // time so that each reduction instruction covers 32 / XC rows x XC adjacent columns.
       if constexpr(xpose_fits<S, NT>()) {
         if(p.xpose) {
-          static_assert(NH % kXCols == 0, "tile half width must be a multiple of the transpose width");
-          double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * kXCols * kXStride;
-          const int rsub = lane / kXCols, csub = lane % kXCols;
+          static_assert(NH % XC == 0, "a warp's columns must be a multiple of the transpose width");
+          double*   xb   = reinterpret_cast<double*>(smem + STAGES * STAGE + kTail) + (warp - 2) * XC * kXStride;
+          const int rsub = lane / XC, csub = lane % XC;
 #pragma unroll
-          for(int x0 = 0; x0 < NH; x0 += kXCols) {
+          for(int x0 = 0; x0 < NH; x0 += XC) {
 #pragma unroll
-            for(int j = 0; j < kXCols; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
+            for(int j = 0; j < XC; j++) xb[j * kXStride + lane] = p.alpha * racc[x0 + j];
             __syncwarp();
             const int o = nof[col0 + x0 + csub];
 #pragma unroll
-            for(int it = 0; it < kXCols; it++) { // rows it * 4 + rsub
-              const int     r  = it * (32 / kXCols) + rsub;
+            for(int it = 0; it < XC; it++) { // rows it * (32 / XC) + rsub
+              const int     r  = it * (32 / XC) + rsub;
               const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
               if(ro >= 0 && o >= 0) {
                 if(p.store) p.C[ro + o] = xb[csub * kXStride + r];
@@ -1255,6 +1266,7 @@ struct I8Layout {
   int64_t                 slice_bytes = 0, a_bytes = 0;
   int64_t                 nexp = 0, a_nexp = 0;
   double                  int8_ops = 0;
+  double                  kc_per_item = 0; // mean 32-byte K steps of an output tile (all its tasks)
   SplitBlock*             d_ablocks = nullptr;
   SplitBlock*             d_bblocks = nullptr;
   int32_t*                d_acbegin = nullptr;
@@ -1518,9 +1530,11 @@ std::shared_ptr<I8Layout> build_layout(const LabelClasses& lc, const WorkList& w
       int64_t gm = 0, gn = 0;
       tiles_of(order[r].group, gm, gn);
       L->int8_ops += 2.0 * MT * L->NT * kstep * order[r].work * (S * (S + 1) / 2) * (double) (gm * gn);
+      L->kc_per_item += (double) order[r].work * (double) (gm * gn);
     }
     r0 = r1;
   }
+  if(!L->items.empty()) L->kc_per_item /= (double) L->items.size();
   TB_CUDA(cudaGetDevice(&L->device));
   auto up = [](auto*& dptr, const auto& vec) {
     using T = std::remove_reference_t<decltype(vec[0])>;
@@ -1620,6 +1634,14 @@ void launch_split(const I8Layout& L, const WorkList& wl, const double* A, const 
   TB_CUDA(cudaGetLastError());
 }
 
+// Output tiles with at most this many 32-byte K steps on average (all their tasks) take
+// the kernel with sixteen epilogue warps: the triples' contractions over one virtual
+// index (one task of K = 250: 8 steps) or one occupied index (tasks of K = 40 and 10: 3
+// steps) measured 6 % faster with them; the ladder's (tens of tasks of 18-72 steps)
+// keep eight, and so does the energy gradient, which ran 1.5x slower when its
+// contractions of up to 32 steps per tile took sixteen.
+constexpr double kShortKSteps = 8.0;
+
 template<int S, int NT, bool BF>
 void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, double alpha,
                  const uint8_t* slices, const int32_t* exps, double* C, const Plan& plan, cudaStream_t st) {
@@ -1648,18 +1670,29 @@ void launch_gemm(const I8Layout& L, const WorkList& wl, const LabelClasses& lc, 
   }
   TB_CUDA(cudaMemsetAsync(L.d_ctr, 0, sizeof(int), st));
   const size_t smem = smem_bytes<S, NT>();
-  static bool  configured[64][2] = {};
+  static bool  configured[64][3] = {};
   int          dev            = 0;
   TB_CUDA(cudaGetDevice(&dev));
-  const int e = plan.energy ? 1 : 0;
+  // kernel: 0 the default, 1 the energy epilogue, 2 sixteen epilogue warps (a C update
+  // whose tiles have little K: the epilogue, not the tensor pipe, bounds them)
+  const int e = plan.energy ? 1 : (!BF && L.kc_per_item <= kShortKSteps) ? 2 : 0;
   if(dev < 64 && !configured[dev][e]) {
-    if(e) TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int) smem));
+    if(e == 1)
+      TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int) smem));
+    else if(e == 2) {
+      if constexpr(!BF)
+        TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, false, false, 16>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    }
     else TB_CUDA(cudaFuncSetAttribute(k_contract_i8<S, NT, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     configured[dev][e] = true;
   }
   const int grid = (int) std::min<int64_t>((int64_t) L.items.size(), sm_count());
-  if(e) k_contract_i8<S, NT, BF, true><<<grid, NTHREADS, smem, st>>>(p);
+  if(e == 1) k_contract_i8<S, NT, BF, true><<<grid, NTHREADS, smem, st>>>(p);
+  else if(e == 2) {
+    if constexpr(!BF) k_contract_i8<S, NT, false, false, 16><<<grid, 64 + 32 * 16, smem, st>>>(p);
+  }
   else k_contract_i8<S, NT, BF><<<grid, NTHREADS, smem, st>>>(p);
   TB_CUDA(cudaGetLastError());
   if(plan.energy)
